@@ -1,0 +1,208 @@
+/*
+ * sph_gpu.h — C ABI of the B200 (sm_100a) spectral shallow-water library
+ * (libsphgpu.so).
+ *
+ * Drop-in boundary for the hot path of schreiberx/sph_swe.  Every entry point
+ * replaces one call the reference makes into SHTNS 2.6.6 (spherical-harmonic
+ * transforms), LAPACK 3.6.1 (zgbsv) or one of its own spectral-space loops;
+ * the replaced interface is cited beside each declaration (paths relative to
+ * the reference's src/ directory).
+ *
+ * Conventions (identical to the reference):
+ *   grid            double[nphi*nlat], index i_lon*nlat + j_lat, j = 0 nearest
+ *                   the north pole, mu_j = sin(latitude) decreasing
+ *                   (SHT_THETA_CONTIGUOUS, SPHConfig.hpp:344,390);
+ *                   longitude lambda_i = 2*pi*i/nphi.
+ *   real spectral   complex (double2) packed m-major, n contiguous:
+ *                   index (m*(2L-m+1))/2 + n, m = 0..L, n = m..L
+ *                   (SPHConfig::getArrayIndexByModes, SPHConfig.hpp:106-116).
+ *   complex spectral index n*n + n + m, m = -n..n
+ *                   (getArrayIndexByModes_Complex, SPHConfig.hpp:120-130).
+ *   normalisation   orthonormal spherical harmonics with Condon-Shortley
+ *                   phase (sht_orthonormal, SPHConfig.hpp:338); real fields
+ *                   f = sum_l Q_l0 Y_l0 + 2 Re sum_{m>0} Q_lm Y_lm; complex
+ *                   fields use Y_l^{-m} = (-1)^m conj(Y_l^m).
+ *
+ * All pointers passed to compute entry points are DEVICE pointers; all work
+ * is ordered on the given stream (cudaStream_t passed as void*; NULL = the
+ * legacy default stream).  Every function returns SPH_OK (0) or an error
+ * code; sph_last_error() describes the last failure of the calling process.
+ * Handles are not thread safe: use one handle per host thread.
+ * The library has no CPU fallback: if no sm_100 device is present, every
+ * compute entry point fails with SPH_ERR_CUDA.
+ */
+#ifndef SPH_GPU_H_
+#define SPH_GPU_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum sph_status {
+    SPH_OK = 0,
+    SPH_ERR_ARG = 1,       /* invalid argument (sizes, layouts, null pointers) */
+    SPH_ERR_CUDA = 2,      /* CUDA runtime error or no usable device           */
+    SPH_ERR_SINGULAR = 3,  /* zero pivot in a banded solve (zgbsv INFO > 0)    */
+    SPH_ERR_NAN = 4,       /* non-finite value detected in the state           */
+    SPH_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up               */
+    SPH_ERR_NOMEM = 6      /* device allocation failed                         */
+};
+
+/* precision forms (flags of sph_create) */
+enum sph_precision {
+    SPH_PREC_FP64 = 0,     /* plain method: FP64 everywhere                      */
+    SPH_PREC_MIXED = 1     /* Legendre GEMMs on tcgen05 (split-bf16, FP32 acc.)  */
+};
+
+typedef struct sph_handle sph_handle;
+typedef struct sph_rexi sph_rexi;
+
+/* ---------------------------------------------------------------- setup */
+
+/* Create a transform handle for triangular truncation lmax == mmax on an
+ * nlat x nphi Gauss-Legendre grid.  nlat <= 0 or nphi <= 0 chooses the grid by
+ * the quadratic (3/2) rule: nphi = smallest 7-smooth integer >= 3*mmax+1,
+ * nlat = 3*lmax/2+1 rounded up to even.  Gauss nodes, weights and the P_l^m
+ * table are computed on the device in FP64.
+ * Replaces shtns_create + shtns_set_grid (SPHConfig::setup, SPHConfig.hpp:324-352)
+ * and shtns_set_grid_auto (SPHConfig::setupAutoPhysicalSpace, SPHConfig.hpp:366-399). */
+int sph_create(int lmax, int mmax, int nlat, int nphi, int flags, sph_handle** out);
+
+/* Release a handle (shtns_destroy, SPHConfig::shutdown, SPHConfig.hpp:421-446). */
+int sph_destroy(sph_handle* h);
+
+/* Sizes: lmax, nlat, nphi, nlm = (L+1)(L+2)/2, ncplx = (L+1)^2 (any may be NULL).
+ * Replaces the shtns_cfg fields read in SPHConfig::setup_data (SPHConfig.hpp:160-168). */
+int sph_info(const sph_handle* h, int* lmax, int* nlat, int* nphi, int* nlm, int* ncplx);
+
+/* Host copies of mu_j (sin latitude, = SHTNS ct), cos(latitude) (= SHTNS st),
+ * Gauss weights and latitude angles, nlat each (any may be NULL).
+ * Replaces lat_gaussian / lat_cogaussian / lat (SPHConfig.hpp:303-319). */
+int sph_grid(const sph_handle* h, double* mu, double* cosphi, double* w, double* lat);
+
+/* ---------------------------------------------------------------- transforms */
+
+/* Real analysis, batch fields: spat[b*ld_spat + .] -> spec[b*ld_spec + .]
+ * (strides in doubles / double2; <= 0 means dense).
+ * Replaces spat_to_SH(shtns, double* Vr, cplx* Qlm) (SPHData.hpp:201,509,527). */
+int sph_spat_to_SH(sph_handle* h, const double* spat, double* spec, int batch, long long ld_spat,
+                   long long ld_spec, void* stream);
+
+/* Real synthesis.  Replaces SH_to_spat(shtns, cplx* Qlm, double* Vr)
+ * (SPHData.hpp:221,510,526). */
+int sph_SH_to_spat(sph_handle* h, const double* spec, double* spat, int batch, long long ld_spec,
+                   long long ld_spat, void* stream);
+
+/* Complex analysis / synthesis on complex grids (double2[nphi*nlat]) and
+ * (L+1)^2 complex coefficients.  Replace spat_cplx_to_SH / SH_to_spat_cplx
+ * (SPHDataComplex.hpp:190,210,469-470,486-487). */
+int sph_cplx_spat_to_SH(sph_handle* h, const double* spat, double* spec, int batch, long long ld_spat,
+                        long long ld_spec, void* stream);
+int sph_cplx_SH_to_spat(sph_handle* h, const double* spec, double* spat, int batch, long long ld_spec,
+                        long long ld_spat, void* stream);
+
+/* Vector pair: vorticity/divergence spectra (real layout, unit sphere)
+ * -> velocity grids u (eastward), v (northward):
+ *   psi = lap^-1 vort, chi = lap^-1 div,
+ *   u*cos(phi) = d chi/d lambda - (1-mu^2) d psi/d mu,
+ *   v*cos(phi) = d psi/d lambda + (1-mu^2) d chi/d mu,
+ * with the exact (degree L+1 retained) meridional derivative.  robert != 0
+ * returns (u cos phi, v cos phi).  The reference has no inverse vector
+ * transform; the forward direction replaces SPHOperators::vort/div
+ * (SPHOperators.hpp:507-529) applied to (u, v). */
+int sph_vec_SH_to_spat(sph_handle* h, const double* vort, const double* div, double* u, double* v, int batch,
+                       int robert, void* stream);
+int sph_vec_spat_to_SH(sph_handle* h, const double* u, const double* v, double* vort, double* div, int batch,
+                       int robert, void* stream);
+
+/* ---------------------------------------------------------------- spectral operators */
+
+enum sph_spec_op_id {
+    SPH_OP_DIFF_LON = 0,   /* x i m                          SPHOperators::diff_lon (SPHOperators.hpp:30-54) */
+    SPH_OP_D1MU2 = 1,      /* truncated (1-mu^2) d/dmu       spec_one_minus_mu_squared_diff_lat_mu (:234-260) */
+    SPH_OP_MU = 2,         /* mu x (Galerkin)                SPHOperators::mu (:268-297)          */
+    SPH_OP_MU2 = 3,        /* mu^2 x (Galerkin)              SPHOperators::mu2 (:303-333)         */
+    SPH_OP_LAPLACE = 4,    /* -n(n+1) x                      SPHOperators::laplace (:482-498)     */
+    SPH_OP_HELMHOLTZ = 5,  /* x / (a + (-(b/r^2) n(n+1)));  args a, b (complex) and r in b.y? see below */
+    SPH_OP_SCALE = 6,      /* a x                            SPHData operator*(double/complex)    */
+    SPH_OP_AXPY = 7        /* out = out + a x                SPHData operator+= with scaling      */
+};
+
+/* Apply a spectral-space operator to batch fields.  cplx = 0: real packed
+ * layout (nlm entries), cplx = 1: complex layout ((L+1)^2 entries).
+ * a = (a_re, a_im), b = (b_re, b_im) are operator arguments: SCALE/AXPY use a;
+ * HELMHOLTZ computes x / (a - b*n(n+1)) (the caller folds r^2 into b), as
+ * SPHData::spec_solve_helmholtz (SPHData.hpp:475-497) and
+ * SPHDataComplex::spec_solve_helmholtz (SPHDataComplex.hpp:523-545).
+ * in == out is allowed for the pointwise operators (DIFF_LON, LAPLACE,
+ * HELMHOLTZ, SCALE, AXPY) but not for the recurrences (D1MU2, MU, MU2). */
+int sph_spec_op(sph_handle* h, int op, const double* in, double* out, double a_re, double a_im, double b_re,
+                double b_im, int batch, int cplx, void* stream);
+
+/* ---------------------------------------------------------------- SWE */
+
+typedef struct sph_swe_params {
+    double radius;     /* a     (SimVars::earth_radius)     */
+    double gravity;    /* g     (SimVars::gravitation)      */
+    double omega;      /* Omega (SimVars::coriolis_omega)   */
+    double h0;         /* mean depth (SimVars::h0)          */
+    double viscosity;  /* nu    (SimVars::viscosity2)       */
+    double dt;         /* time step (current_timestep_size) */
+    int nonlinear;     /* SimVars::use_nonlinear_equations  */
+    int robert;        /* SimVars::use_robert_functions     */
+} sph_swe_params;
+
+/* One SWE tendency evaluation: state = [h | u | v] spectral (3*nlm complex,
+ * contiguous) -> tend = [h_t | u_t | v_t].  Follows the projection points of
+ * AppSWE::p_run_euler_timestep_update (AppSWE.hpp:738-823). */
+int sph_swe_tendency(sph_handle* h, const sph_swe_params* p, const double* state, double* tend, void* stream);
+
+/* nsteps classical RK4 steps in place on state = [h | u | v] (3*nlm complex),
+ * as TimesteppingRK::run_rk_timestep order 4 (TimesteppingRK.hpp:310-392)
+ * driven by AppSWE::run (AppSWE.hpp:457-499).  The step is captured once in a
+ * CUDA graph and replayed.  Returns SPH_ERR_NAN if h became non-finite
+ * (AppSWE.hpp:486-491). */
+int sph_swe_rk4(sph_handle* h, const sph_swe_params* p, double* state, int nsteps, void* stream);
+
+/* Batched ensemble: nmem independent members, state of member k at
+ * state + 3*nlm*k (complex), all with the same handle and parameters except
+ * dt_k = dts[k] (host array, may be NULL = p->dt). */
+int sph_swe_rk4_batched(sph_handle* h, const sph_swe_params* p, const double* dts, double* state, int nmem,
+                        int nsteps, void* stream);
+
+/* ---------------------------------------------------------------- REXI */
+
+typedef struct sph_rexi_params {
+    double radius, gravity, omega, h0, viscosity, tau;
+    int robert;        /* SWERexiSPHRobert (1) or SWERexiSPH (0)            */
+    int coriolis;      /* include_coriolis_effect                           */
+    int fix_z5robert;  /* 0: reproduce SPHSolverComplex.hpp:305-309 as written */
+    int precision;     /* SPH_PREC_FP64 direct, SPH_PREC_MIXED (complex FP32
+                          factor/solve + FP64 iterative refinement)          */
+} sph_rexi_params;
+
+/* Prepare a REXI integrator for npoles poles alpha[k], beta[k] (host arrays of
+ * interleaved complex).  Replaces the per-pole SWERexiSPH[Robert]::setup loop
+ * (AppSWE.hpp:517-577, SWERexiSPHRobert.hpp:68-132). */
+int sph_rexi_create(sph_handle* h, const double* alpha, const double* beta, int npoles, const sph_rexi_params* p,
+                    sph_rexi** out);
+int sph_rexi_destroy(sph_rexi* r);
+
+/* nsteps REXI steps in place on state = [h | u | v] (3*nlm complex): all poles
+ * x all m x both l-parities are solved in one launch per step; replaces the
+ * serial pole loop of AppSWE::run (AppSWE.hpp:580-729) with
+ * SWERexiSPH[Robert]::solve (SWERexiSPHRobert.hpp:139-258) and
+ * SPHSolverComplex::solve -> zgbsv (SPHSolverComplex.hpp:462-511,
+ * BandedMatrixSolver.hpp:416-427). */
+int sph_rexi_step(sph_rexi* r, double* state, int nsteps, void* stream);
+
+/* ---------------------------------------------------------------- errors */
+
+/* Copy the message of the last error into buf (NUL terminated); returns its length. */
+int sph_last_error(char* buf, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPH_GPU_H_ */

@@ -1,0 +1,223 @@
+// Legendre stage of the spherical-harmonic transforms in FP64 (the plain
+// method): per zonal wavenumber m a dense contraction between the table
+// P_l^m(mu_j) (northern rings only, equatorial symmetry) and the batch of
+// fields, tiled as a small GEMM on the FP64 pipe.
+//
+//   synthesis  E_j = sum_{l-m even} Q_l P_l(mu_j),  O_j = sum_{l-m odd} Q_l P_l(mu_j)
+//              F(mu_j) = E_j + O_j,  F(-mu_j) = E_j - O_j
+//   analysis   Q_l = sum_{j<nh} w_j P_l(mu_j) (F(mu_j) +/- F(-mu_j))   (+ for l-m even)
+//
+// Real fields use m = 0..min(lmax, L) and the packed layout of degree lmax
+// (lmax = L, or L+1 for the vector transforms); complex fields use
+// m = -L..L, layout n*n+n+m and P_l^{-m} = (-1)^m P_l^m.
+// Columns of the GEMM are (field, re/im) pairs.
+#include "common.cuh"
+
+namespace sphgpu {
+
+namespace {
+constexpr int TJ = 64;   // latitudes per CTA tile (synthesis)
+constexpr int TLT = 64;  // degrees per CTA tile (analysis)
+constexpr int TC = 32;   // real columns per tile (16 complex fields)
+constexpr int TK = 16;   // contraction chunk
+constexpr int NT = 256;  // threads
+}  // namespace
+
+struct SpecMap {
+    int cplx;      // 0 real packed(lmax), 1 complex n*n+n+m
+    int lmax;
+    int L;
+    long long ld;  // per-field stride (double2)
+};
+
+__device__ __forceinline__ long long spec_index(const SpecMap& s, int l, int m) {
+    return s.cplx ? (long long)cidx(l, m) : (long long)pidx(s.lmax, l, m);
+}
+
+// grid: x = j tile, y = column tile, z = m slot (real: m, complex: m + L)
+__global__ void __launch_bounds__(NT) k_legendre_synthesis(const double* __restrict__ plm, const long long* __restrict__ poff,
+                                                           int nh, int nlat, const double2* __restrict__ spec, SpecMap sm,
+                                                           double2* __restrict__ F, long long ldF, int batch) {
+    __shared__ double As[TK][TJ];
+    __shared__ double Bs[TK][TC + 1];
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int j0 = blockIdx.x * TJ;
+    const int f0 = blockIdx.y * (TC / 2);
+    const int tid = threadIdx.x;
+    const int tx = tid & 15;   // field within tile
+    const int ty = tid >> 4;   // 4 latitudes: ty*4 .. ty*4+3
+    const double* P = plm + poff[am];
+
+    double eR[4] = {0, 0, 0, 0}, eI[4] = {0, 0, 0, 0}, oR[4] = {0, 0, 0, 0}, oI[4] = {0, 0, 0, 0};
+
+    for (int l0 = am; l0 <= lmax; l0 += TK) {
+        // A tile: P rows l0..l0+TK-1, latitudes j0..j0+TJ-1
+        for (int idx = tid; idx < TK * TJ; idx += NT) {
+            const int kk = idx / TJ, jj = idx - kk * TJ;
+            const int l = l0 + kk, j = j0 + jj;
+            As[kk][jj] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
+        }
+        // B tile: coefficients of 16 fields, degrees l0..l0+TK-1
+        {
+            const int kk = tid & 15, ff = tid >> 4;
+            const int l = l0 + kk, f = f0 + ff;
+            double2 q = make_double2(0, 0);
+            if (l <= lmax && f < batch) q = spec[(long long)f * sm.ld + spec_index(sm, l, m)];
+            Bs[kk][2 * ff] = q.x;
+            Bs[kk][2 * ff + 1] = q.y;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; kk += 2) {
+            const double br0 = Bs[kk][2 * tx], bi0 = Bs[kk][2 * tx + 1];
+            const double br1 = Bs[kk + 1][2 * tx], bi1 = Bs[kk + 1][2 * tx + 1];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const double a0 = As[kk][ty * 4 + r], a1 = As[kk + 1][ty * 4 + r];
+                eR[r] = fma(a0, br0, eR[r]);
+                eI[r] = fma(a0, bi0, eI[r]);
+                oR[r] = fma(a1, br1, oR[r]);
+                oI[r] = fma(a1, bi1, oI[r]);
+            }
+        }
+        __syncthreads();
+    }
+    const int f = f0 + tx;
+    if (f >= batch) return;
+    double2* out = F + (long long)f * ldF + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int j = j0 + ty * 4 + r;
+        if (j >= nh) continue;
+        out[j] = make_double2(eR[r] + oR[r], eI[r] + oI[r]);
+        out[nlat - 1 - j] = make_double2(eR[r] - oR[r], eI[r] - oI[r]);
+    }
+}
+
+// grid: x = degree tile, y = column tile, z = m slot
+__global__ void __launch_bounds__(NT) k_legendre_analysis(const double* __restrict__ plm, const long long* __restrict__ poff,
+                                                          int nh, int nlat, const double* __restrict__ w,
+                                                          const double2* __restrict__ F, long long ldF,
+                                                          double2* __restrict__ spec, SpecMap sm, int batch) {
+    __shared__ double Ps[TK][TLT + 1];
+    __shared__ double Ss[TK][TC + 1];
+    __shared__ double Ds[TK][TC + 1];
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int lbase = am + blockIdx.x * TLT;
+    if (lbase > lmax) return;
+    const int f0 = blockIdx.y * (TC / 2);
+    const int tid = threadIdx.x;
+    const int tx = tid & 15;
+    const int ty = tid >> 4;  // degrees lbase + ty + 16 r, r = 0..3 (same parity)
+    const double* P = plm + poff[am];
+    const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+    const bool odd = ((lbase + ty - am) & 1) != 0;
+
+    double aR[4] = {0, 0, 0, 0}, aI[4] = {0, 0, 0, 0};
+    for (int j0 = 0; j0 < nh; j0 += TK) {
+        for (int idx = tid; idx < TK * TLT; idx += NT) {
+            const int ll = idx / TK, kk = idx - ll * TK;
+            const int l = lbase + ll, j = j0 + kk;
+            Ps[kk][ll] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
+        }
+        {
+            const int kk = tid & 15, ff = tid >> 4;
+            const int j = j0 + kk, f = f0 + ff;
+            double2 s = make_double2(0, 0), d = make_double2(0, 0);
+            if (j < nh && f < batch) {
+                const double2* Ff = Fm + (long long)f * ldF;
+                const double2 n = Ff[j], so = Ff[nlat - 1 - j];
+                const double wj = w[j];
+                s = make_double2(wj * (n.x + so.x), wj * (n.y + so.y));
+                d = make_double2(wj * (n.x - so.x), wj * (n.y - so.y));
+            }
+            Ss[kk][2 * ff] = s.x;
+            Ss[kk][2 * ff + 1] = s.y;
+            Ds[kk][2 * ff] = d.x;
+            Ds[kk][2 * ff + 1] = d.y;
+        }
+        __syncthreads();
+        const double(*G)[TC + 1] = odd ? Ds : Ss;
+#pragma unroll
+        for (int kk = 0; kk < TK; kk++) {
+            const double gr = G[kk][2 * tx], gi = G[kk][2 * tx + 1];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const double p = Ps[kk][ty + 16 * r];
+                aR[r] = fma(p, gr, aR[r]);
+                aI[r] = fma(p, gi, aI[r]);
+            }
+        }
+        __syncthreads();
+    }
+    const int f = f0 + tx;
+    if (f >= batch) return;
+    double2* out = spec + (long long)f * sm.ld;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int l = lbase + ty + 16 * r;
+        if (l <= lmax) out[spec_index(sm, l, m)] = make_double2(aR[r], aI[r]);
+    }
+}
+
+// zero the m = L+1 column of a degree-(L+1) packed spectrum (no wavenumber L+1 exists)
+__global__ void k_zero_top(double2* spec, long long ld, int lmax, int batch) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < batch) spec[(long long)f * ld + pidx(lmax, lmax, lmax)] = make_double2(0, 0);
+}
+
+static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double2* F, long long ldF, int batch,
+                        cudaStream_t s) {
+    if (batch <= 0) return SPH_OK;
+    const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
+    dim3 grid((h->nh + TJ - 1) / TJ, (batch + TC / 2 - 1) / (TC / 2), nm);
+    k_legendre_synthesis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+static int launch_anal(const Handle* h, const double2* F, long long ldF, double2* spec, SpecMap sm, int batch,
+                       cudaStream_t s) {
+    if (batch <= 0) return SPH_OK;
+    const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
+    dim3 grid((sm.lmax + 1 + TLT - 1) / TLT, (batch + TC / 2 - 1) / (TC / 2), nm);
+    k_legendre_analysis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, h->w, F, ldF, spec, sm, batch);
+    SPH_CUDA_TRY(cudaGetLastError());
+    if (!sm.cplx && sm.lmax > h->L) {
+        k_zero_top<<<(batch + 127) / 128, 128, 0, s>>>(spec, sm.ld, sm.lmax, batch);
+        SPH_CUDA_TRY(cudaGetLastError());
+    }
+    return SPH_OK;
+}
+
+int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
+                            long long ldF, int batch, cudaStream_t s) {
+    SpecMap sm{0, lmax, h->L, ld_spec};
+    return launch_synth(h, spec, sm, F, ldF, batch, s);
+}
+
+int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
+                           int lmax, int batch, cudaStream_t s) {
+    SpecMap sm{0, lmax, h->L, ld_spec};
+    return launch_anal(h, F, ldF, spec, sm, batch, s);
+}
+
+int legendre_synthesis_cplx(const Handle* h, const double2* spec, long long ld_spec, double2* F, long long ldF,
+                            int batch, cudaStream_t s) {
+    SpecMap sm{1, h->L, h->L, ld_spec};
+    return launch_synth(h, spec, sm, F, ldF, batch, s);
+}
+
+int legendre_analysis_cplx(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
+                           int batch, cudaStream_t s) {
+    SpecMap sm{1, h->L, h->L, ld_spec};
+    return launch_anal(h, F, ldF, spec, sm, batch, s);
+}
+
+}  // namespace sphgpu

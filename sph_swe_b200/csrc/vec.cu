@@ -1,0 +1,164 @@
+// Vector transforms: vorticity/divergence spectra <-> velocity grids on the
+// unit sphere, built from the scalar Legendre/FFT stages with the meridional
+// derivative kept exact (degree L+1 retained, Legendre range lmax = L+1):
+//
+//   synthesis  psi = lap^-1 vort, chi = lap^-1 div
+//              U = u c = d chi/d lambda - (1-mu^2) d psi/d mu
+//              V = v c = d psi/d lambda + (1-mu^2) d chi/d mu
+//   analysis   with U' = U/c^2, V' = V/c^2 and a_l(.) the degree-(L+1) analysis,
+//              vort_l = i m a_l(V') + (l+1) e_l a_{l-1}(U') - l e_{l+1} a_{l+1}(U')
+//              div_l  = i m a_l(U') - (l+1) e_l a_{l-1}(V') + l e_{l+1} a_{l+1}(V')
+//              (integration by parts of d/dmu; exact by Gauss quadrature)
+// with (1-mu^2) dP_l/dmu = (l+1) e_l P_{l-1} - l e_{l+1} P_{l+1},
+// e_l = R(l-1, m), e_{l+1} = S(l+1, m) of SPHIdentities.hpp:52-86.
+// The reference has no vector transform; its scalar operators grad/div/vort
+// (SPHOperators.hpp:100-119, 339-529) are the truncated counterparts.
+#include "common.cuh"
+#include "identities.cuh"
+
+namespace sphgpu {
+
+// vort/div (degree L) -> [U, V] spectra of degree L+1
+__global__ void k_vec_prep(const double2* __restrict__ vort, const double2* __restrict__ div, long long ld,
+                           double2* __restrict__ X, int L, int nlmp) {
+    const int m = blockIdx.y;  // 0..L+1
+    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
+    const int Lp = L + 1;
+    if (n > Lp) return;
+    const int b = blockIdx.z;
+    double2* U = X + (size_t)b * 2 * nlmp;
+    double2* V = U + nlmp;
+    const int k = pidx(Lp, n, m);
+    if (m > L) {
+        U[k] = make_double2(0, 0);
+        V[k] = make_double2(0, 0);
+        return;
+    }
+    const double2* z = vort + (size_t)b * ld;
+    const double2* d = div + (size_t)b * ld;
+    auto inv = [&](const double2* x, int nn) -> double2 {  // lap^-1 on degree nn
+        if (nn < m || nn > L || nn == 0) return make_double2(0, 0);
+        const double s = -1.0 / ((double)nn * (nn + 1.0));
+        const double2 v = x[pidx(L, nn, m)];
+        return make_double2(v.x * s, v.y * s);
+    };
+    const double dn = n, dm = m;
+    const double cl = (-dn + 1.0) * idR(dn - 1, dm), ch = (dn + 2.0) * idS(dn + 1, dm);
+    const double2 psi = inv(z, n), chi = inv(d, n);
+    const double2 psl = inv(z, n - 1), psh = inv(z, n + 1), chl = inv(d, n - 1), chh = inv(d, n + 1);
+    // U = i m chi - Dex psi ; V = i m psi + Dex chi
+    U[k] = make_double2(-dm * chi.y - (cl * psl.x + ch * psh.x), dm * chi.x - (cl * psl.y + ch * psh.y));
+    V[k] = make_double2(-dm * psi.y + (cl * chl.x + ch * chh.x), dm * psi.x + (cl * chl.y + ch * chh.y));
+}
+
+// F[f][m][j] *= c_j^(-p)
+__global__ void k_fourier_scale(double2* __restrict__ F, long long ldF, int mF, int nlat,
+                                const double* __restrict__ cosphi, int p) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long fou = (long long)mF * nlat;
+    if (idx >= fou) return;
+    const int j = (int)(idx % nlat);
+    const double c = cosphi[j];
+    const double s = p == 1 ? 1.0 / c : 1.0 / (c * c);
+    double2* f = F + (long long)blockIdx.y * ldF + idx;
+    const double2 v = *f;
+    *f = make_double2(v.x * s, v.y * s);
+}
+
+// a(U'), a(V') of degree L+1 -> vort, div of degree L
+__global__ void k_vec_post(const double2* __restrict__ A, int nlmp, double2* __restrict__ vort, double2* __restrict__ div,
+                           long long ld, int L) {
+    const int m = blockIdx.y;
+    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n > L) return;
+    const int b = blockIdx.z;
+    const int Lp = L + 1;
+    const double2* aU = A + (size_t)b * 2 * nlmp;
+    const double2* aV = aU + nlmp;
+    auto at = [&](const double2* x, int nn) -> double2 {
+        if (nn < m || nn > Lp) return make_double2(0, 0);
+        return x[pidx(Lp, nn, m)];
+    };
+    const double dn = n, dm = m;
+    const double el = (dn + 1.0) * idR(dn - 1, dm), eh = dn * idS(dn + 1, dm);
+    const double2 u0 = at(aU, n), ul = at(aU, n - 1), uh = at(aU, n + 1);
+    const double2 v0 = at(aV, n), vl = at(aV, n - 1), vh = at(aV, n + 1);
+    const int k = pidx(L, n, m);
+    vort[(size_t)b * ld + k] = make_double2(-dm * v0.y + el * ul.x - eh * uh.x, dm * v0.x + el * ul.y - eh * uh.y);
+    div[(size_t)b * ld + k] = make_double2(-dm * u0.y - el * vl.x + eh * vh.x, dm * u0.x - el * vl.y + eh * vh.y);
+}
+
+}  // namespace sphgpu
+
+using namespace sphgpu;
+
+extern "C" {
+
+int sph_vec_SH_to_spat(sph_handle* hh, const double* vort, const double* div, double* u, double* v, int batch,
+                       int robert, void* stream) {
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || batch < 0 || (batch > 0 && (!vort || !div || !u || !v))) {
+        set_error("sph_vec_SH_to_spat: bad arguments");
+        return SPH_ERR_ARG;
+    }
+    if (batch == 0) return SPH_OK;
+    if (batch > 32767) { set_error("sph_vec_SH_to_spat: batch too large"); return SPH_ERR_ARG; }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int L = h->L, Lp = L + 1, mF = L + 1;
+    const int nlmp = (Lp + 1) * (Lp + 2) / 2;
+    const long long ldF = (long long)mF * h->nlat;
+    const size_t xbytes = sizeof(double2) * 2 * (size_t)nlmp * batch;
+    const size_t fbytes = sizeof(double2) * 2 * (size_t)ldF * batch;
+    if (int rc = ensure_workspace(h, xbytes + fbytes)) return rc;
+    double2* X = static_cast<double2*>(h->ws);
+    double2* F = reinterpret_cast<double2*>(static_cast<char*>(h->ws) + xbytes);
+    k_vec_prep<<<dim3((Lp + 1 + 63) / 64, Lp + 1, batch), 64, 0, s>>>(reinterpret_cast<const double2*>(vort),
+                                                                     reinterpret_cast<const double2*>(div), h->nlm, X, L,
+                                                                     nlmp);
+    SPH_CUDA_TRY(cudaGetLastError());
+    if (int rc = legendre_synthesis_real(h, X, nlmp, Lp, F, ldF, 2 * batch, s)) return rc;
+    if (!robert) {
+        k_fourier_scale<<<dim3((unsigned)((ldF + 255) / 256), 2 * batch), 256, 0, s>>>(F, ldF, mF, h->nlat, h->cosphi, 1);
+        SPH_CUDA_TRY(cudaGetLastError());
+    }
+    // outputs: member b -> u (field 2b) and v (field 2b+1) written to separate arrays
+    for (int c = 0; c < 2; c++) {
+        const int srcs[1] = {c};
+        if (int rc = ring_synthesis_real(h, F, ldF, mF, c == 0 ? u : v, h->nspat, batch, srcs, nullptr, 1, 2, s))
+            return rc;
+    }
+    return SPH_OK;
+}
+
+int sph_vec_spat_to_SH(sph_handle* hh, const double* u, const double* v, double* vort, double* div, int batch,
+                       int robert, void* stream) {
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || batch < 0 || (batch > 0 && (!vort || !div || !u || !v))) {
+        set_error("sph_vec_spat_to_SH: bad arguments");
+        return SPH_ERR_ARG;
+    }
+    if (batch == 0) return SPH_OK;
+    if (batch > 32767) { set_error("sph_vec_spat_to_SH: batch too large"); return SPH_ERR_ARG; }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int L = h->L, Lp = L + 1, mF = L + 1;
+    const int nlmp = (Lp + 1) * (Lp + 2) / 2;
+    const long long ldF = (long long)mF * h->nlat;
+    const size_t xbytes = sizeof(double2) * 2 * (size_t)nlmp * batch;
+    const size_t fbytes = sizeof(double2) * 2 * (size_t)ldF * batch;
+    if (int rc = ensure_workspace(h, xbytes + fbytes)) return rc;
+    double2* A = static_cast<double2*>(h->ws);
+    double2* F = reinterpret_cast<double2*>(static_cast<char*>(h->ws) + xbytes);
+    // Fourier of u into fields 2b, of v into 2b+1
+    if (int rc = ring_analysis_real(h, u, h->nspat, F, 2 * ldF, mF, batch, s)) return rc;
+    if (int rc = ring_analysis_real(h, v, h->nspat, F + ldF, 2 * ldF, mF, batch, s)) return rc;
+    k_fourier_scale<<<dim3((unsigned)((ldF + 255) / 256), 2 * batch), 256, 0, s>>>(F, ldF, mF, h->nlat, h->cosphi,
+                                                                                    robert ? 2 : 1);
+    SPH_CUDA_TRY(cudaGetLastError());
+    if (int rc = legendre_analysis_real(h, F, ldF, A, nlmp, Lp, 2 * batch, s)) return rc;
+    k_vec_post<<<dim3((L + 1 + 63) / 64, L + 1, batch), 64, 0, s>>>(A, nlmp, reinterpret_cast<double2*>(vort),
+                                                                   reinterpret_cast<double2*>(div), h->nlm, L);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+"""Python host view of the C ABI, on torch CUDA tensors (device memory and
+streams only; all arithmetic runs in libsphgpu.so).
+
+Names mirror the reference's SPHConfig surface (SPHConfig.hpp): a ``Sph``
+object owns one transform handle for a triangular truncation on a Gauss grid.
+Grids are float64 tensors shaped ``(..., nphi, nlat)`` (index i_lon*nlat+j),
+spectra complex128 ``(..., nlm)`` (real layout) or ``(..., (L+1)**2)``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import capi
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: torch.Tensor):
+    if not t.is_cuda:
+        raise ValueError("device tensor required")
+    if not t.is_contiguous():
+        raise ValueError("contiguous tensor required")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Sph:
+    """One transform handle (replaces SPHConfig + its shtns_cfg)."""
+
+    def __init__(self, lmax: int, nlat: int = 0, nphi: int = 0, precision: int = capi.SPH_PREC_FP64):
+        torch.cuda.init()
+        h = ctypes.c_void_p()
+        capi.check(capi.lib().sph_create(lmax, lmax, nlat, nphi, precision, ctypes.byref(h)))
+        self.h = h
+        vals = [ctypes.c_int() for _ in range(5)]
+        capi.check(capi.lib().sph_info(self.h, *[ctypes.byref(v) for v in vals]))
+        self.L, self.nlat, self.nphi, self.nlm, self.ncplx = (v.value for v in vals)
+        self.mu = np.zeros(self.nlat)
+        self.cosphi = np.zeros(self.nlat)
+        self.w = np.zeros(self.nlat)
+        self.lat = np.zeros(self.nlat)
+        dp = ctypes.POINTER(ctypes.c_double)
+        capi.check(capi.lib().sph_grid(self.h, *[a.ctypes.data_as(dp) for a in (self.mu, self.cosphi, self.w, self.lat)]))
+        self.lon = np.arange(self.nphi) / self.nphi * 2.0 * np.pi
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "h", None):
+            capi.lib().sph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ transforms
+    def spat_to_SH(self, spat: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        batch = spat.numel() // (self.nlat * self.nphi)
+        if out is None:
+            out = torch.empty(spat.shape[:-2] + (self.nlm,), dtype=torch.complex128, device=spat.device)
+        capi.check(capi.lib().sph_spat_to_SH(self.h, _ptr(spat), _ptr(out), batch, 0, 0, _stream()))
+        return out
+
+    def SH_to_spat(self, spec: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        batch = spec.numel() // self.nlm
+        if out is None:
+            out = torch.empty(spec.shape[:-1] + (self.nphi, self.nlat), dtype=torch.float64, device=spec.device)
+        capi.check(capi.lib().sph_SH_to_spat(self.h, _ptr(spec), _ptr(out), batch, 0, 0, _stream()))
+        return out
+
+    def cplx_spat_to_SH(self, spat: torch.Tensor) -> torch.Tensor:
+        batch = spat.numel() // (self.nlat * self.nphi)
+        out = torch.empty(spat.shape[:-2] + (self.ncplx,), dtype=torch.complex128, device=spat.device)
+        capi.check(capi.lib().sph_cplx_spat_to_SH(self.h, _ptr(spat), _ptr(out), batch, 0, 0, _stream()))
+        return out
+
+    def cplx_SH_to_spat(self, spec: torch.Tensor) -> torch.Tensor:
+        batch = spec.numel() // self.ncplx
+        out = torch.empty(spec.shape[:-1] + (self.nphi, self.nlat), dtype=torch.complex128, device=spec.device)
+        capi.check(capi.lib().sph_cplx_SH_to_spat(self.h, _ptr(spec), _ptr(out), batch, 0, 0, _stream()))
+        return out
+
+    def vec_SH_to_spat(self, vort: torch.Tensor, div: torch.Tensor, robert: bool = False):
+        batch = vort.numel() // self.nlm
+        u = torch.empty(vort.shape[:-1] + (self.nphi, self.nlat), dtype=torch.float64, device=vort.device)
+        v = torch.empty_like(u)
+        capi.check(capi.lib().sph_vec_SH_to_spat(self.h, _ptr(vort), _ptr(div), _ptr(u), _ptr(v), batch, int(robert),
+                                                 _stream()))
+        return u, v
+
+    def vec_spat_to_SH(self, u: torch.Tensor, v: torch.Tensor, robert: bool = False):
+        batch = u.numel() // (self.nlat * self.nphi)
+        vort = torch.empty(u.shape[:-2] + (self.nlm,), dtype=torch.complex128, device=u.device)
+        div = torch.empty_like(vort)
+        capi.check(capi.lib().sph_vec_spat_to_SH(self.h, _ptr(u), _ptr(v), _ptr(vort), _ptr(div), batch, int(robert),
+                                                 _stream()))
+        return vort, div
+
+    # ------------------------------------------------------------ operators
+    def spec_op(self, op, x: torch.Tensor, a: complex = 0.0, b: complex = 0.0, cplx: bool = False,
+                out: torch.Tensor | None = None) -> torch.Tensor:
+        n = self.ncplx if cplx else self.nlm
+        batch = x.numel() // n
+        if out is None:
+            out = torch.zeros_like(x) if op in ("axpy", capi.OPS["axpy"]) else torch.empty_like(x)
+        op_id = capi.OPS[op] if isinstance(op, str) else int(op)
+        a, b = complex(a), complex(b)
+        capi.check(capi.lib().sph_spec_op(self.h, op_id, _ptr(x), _ptr(out), a.real, a.imag, b.real, b.imag, batch,
+                                          int(cplx), _stream()))
+        return out
+
+    # ------------------------------------------------------------ SWE
+    @staticmethod
+    def swe_params(radius=6.37122e6, gravity=9.80616, omega=7.292e-5, h0=1e4, viscosity=0.0, dt=120.0,
+                   nonlinear=1, robert=0) -> capi.SWEParams:
+        return capi.SWEParams(radius, gravity, omega, h0, viscosity, dt, nonlinear, robert)
+
+    def swe_tendency(self, p: capi.SWEParams, state: torch.Tensor) -> torch.Tensor:
+        tend = torch.empty_like(state)
+        capi.check(capi.lib().sph_swe_tendency(self.h, ctypes.byref(p), _ptr(state), _ptr(tend), _stream()))
+        return tend
+
+    def swe_rk4(self, p: capi.SWEParams, state: torch.Tensor, nsteps: int) -> torch.Tensor:
+        """In place on state (3, nlm) complex128 = [h, u, v]."""
+        capi.check(capi.lib().sph_swe_rk4(self.h, ctypes.byref(p), _ptr(state), nsteps, _stream()))
+        return state
+
+    def swe_rk4_batched(self, p: capi.SWEParams, state: torch.Tensor, nsteps: int, dts=None) -> torch.Tensor:
+        nmem = state.numel() // (3 * self.nlm)
+        arr = None
+        if dts is not None:
+            arr = np.ascontiguousarray(dts, np.float64)
+            arr_p = arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        else:
+            arr_p = None
+        capi.check(capi.lib().sph_swe_rk4_batched(self.h, ctypes.byref(p), arr_p, _ptr(state), nmem, nsteps,
+                                                  _stream()))
+        return state
+
+    # ------------------------------------------------------------ helpers
+    def grid_from(self, f) -> np.ndarray:
+        LON, MU = np.meshgrid(self.lon, self.mu, indexing="ij")
+        return np.ascontiguousarray(f(LON, MU))
