@@ -1,0 +1,427 @@
+"""Benchmark of the spectral shallow-water hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--quick]
+
+Headline workload (one "step"): the transform-throughput configuration,
+T255 on the 384 x 768 Gauss grid, 64 scalar fields plus 32 vorticity/divergence
+pairs, inverse and forward transform of every field.  Metric: SHT GFLOP/s with
+the algorithmic flop count 2*nlm*nlat per field per direction per Legendre
+contraction (384 contractions) plus 2.5*nphi*log2(nphi)*nlat per field FFT
+(256 field-FFTs): 11.51 GFLOP per step.
+
+Inputs are synthetic (seeded complex N(0,1) spectra scaled by (l+1)^-1.5,
+Im = 0 at m = 0) and larger than L2 (>= 270 MB per step), so no L2 flush is
+needed between steps.  Also reported (not the headline): nonlinear RK4 steps/s
+at T255 and T63 (plain-method configuration) on the FP64 path.
+
+--impl reference times the CPU restatement of the same algorithm (the oracle;
+the reference's SHTNS/FFTW/LAPACK build is unavailable on this machine) on the
+host cores, on a bounded sample of the same workload.
+
+Multi-GPU: the transform batch is independent per field, so N ranks each run
+the full per-GPU workload (weak scaling, no collective in the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L_CFG1 = 255
+N_SCALAR = 64
+N_PAIRS = 32
+METRIC = "SWE steps/s & SHT GFLOP/s at T255/T127 REXI: mixed vs FP64-GPU at relL2<=1e-6"
+
+
+def cfg1_flops(L=L_CFG1, nlat=384, nphi=768):
+    nlm = (L + 1) * (L + 2) // 2
+    per_contraction = 2.0 * nlm * nlat
+    n_contr = N_SCALAR * 2 + N_PAIRS * 4 * 2
+    fft_per_field = 2.5 * nphi * math.log2(nphi) * nlat
+    n_fft = N_SCALAR * 2 + N_PAIRS * 2 * 2
+    return per_contraction * n_contr, fft_per_field * n_fft, per_contraction
+
+
+def random_spec(L, n, seed, zero_mean=False):
+    """complex N(0,1) * (l+1)^-1.5, Im = 0 at m = 0; zero_mean drops the (0,0)
+    coefficient (vorticity and divergence have no global mean)."""
+    rng = np.random.default_rng(seed)
+    nlm = (L + 1) * (L + 2) // 2
+    ls = np.concatenate([np.arange(m, L + 1) for m in range(L + 1)])
+    x = (rng.standard_normal((n, nlm)) + 1j * rng.standard_normal((n, nlm))) * (ls + 1.0) ** -1.5
+    x[:, : L + 1] = x[:, : L + 1].real
+    if zero_mean:
+        x[:, 0] = 0
+    return x
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and s[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world):
+    import torch
+
+    from sph_swe_b200 import build as b
+    b.build()
+    from sph_swe_b200.sph import Sph
+
+    dev = torch.device("cuda", rank % max(1, torch.cuda.device_count()))
+    torch.cuda.set_device(dev)
+    s = Sph(L_CFG1)
+    assert (s.nlat, s.nphi) == (384, 768)
+    gl, gf, per_contr = cfg1_flops()
+    flops_step = gl + gf
+
+    spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1 + rank)).to(dev)
+    vort = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 1001 + rank, zero_mean=True)).to(dev)
+    div = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 2001 + rank, zero_mean=True)).to(dev)
+    grid = torch.empty(N_SCALAR, s.nphi, s.nlat, dtype=torch.float64, device=dev)
+    spec_out = torch.empty_like(spec)
+    vo = torch.empty_like(vort)
+    do = torch.empty_like(div)
+
+    def step():
+        s.SH_to_spat(spec, out=grid)
+        s.spat_to_SH(grid, out=spec_out)
+        u, v = s.vec_SH_to_spat(vort, div)
+        z, d = s.vec_spat_to_SH(u, v)
+        return z, d
+
+    launches_per_step = 2 + 2 + 5 + 5
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # accuracy of this configuration: fwd(inv(x)) vs x, and inverse vs the oracle on one field
+    z, d = step()
+    torch.cuda.synchronize()
+    rt_scalar = float(torch.linalg.vector_norm(spec_out - spec) / torch.linalg.vector_norm(spec))
+    rt_vec = float(torch.linalg.vector_norm(z - vort) / torch.linalg.vector_norm(vort))
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = flops_step * world / (ms * 1e-3) / 1e9
+
+    # dominant kernel: the FP64 Legendre stage, timed alone on the same stream
+    four = torch.empty(N_SCALAR, L_CFG1 + 1, s.nlat, dtype=torch.complex128, device=dev)
+    for _ in range(3):
+        s.legendre_synthesis(spec, four)
+        s.legendre_analysis(four, spec_out)
+    torch.cuda.synchronize()
+    nrep = max(3, args.steps)
+    e2, e3, e4 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e2.record(st)
+    for _ in range(nrep):
+        s.legendre_synthesis(spec, four)
+    e3.record(st)
+    for _ in range(nrep):
+        s.legendre_analysis(four, spec_out)
+    e4.record(st)
+    torch.cuda.synchronize()
+    t_syn = e2.elapsed_time(e3) / nrep * 1e-3
+    t_ana = e3.elapsed_time(e4) / nrep * 1e-3
+    leg_flops = per_contr * N_SCALAR
+    # FP64 peak for the roofline: cuBLAS DGEMM measured in this run
+    a = torch.randn(4096, 4096, dtype=torch.float64, device=dev)
+    bm = torch.randn(4096, 4096, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, bm)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e5, e6 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e5.record(st)
+        torch.matmul(a, bm)
+        e6.record(st)
+        torch.cuda.synchronize()
+        best = min(best, e5.elapsed_time(e6) * 1e-3)
+    fp64_peak = 2.0 * 4096 ** 3 / best / 1e12
+    del a, bm
+    achieved = leg_flops / t_ana / 1e12
+    roofline = {"bound": "tensor", "kernel": "k_legendre_analysis (FP64, 64 fields, T255)", "achieved": achieved,
+                "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                "peak_source": "FP64 dense: cuBLAS DGEMM 4096^3 measured in this run (no FP64 figure in "
+                               "MEASURED_PEAKS.json)",
+                "legendre_synthesis_tflops": leg_flops / t_syn / 1e12}
+    if args.traffic is not None:
+        roofline["traffic"] = args.traffic
+
+    # end-to-end through the C ABI with host buffers: H2D of the input spectra,
+    # the step, D2H of the output spectra
+    h_spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1 + rank)).pin_memory()
+    h_vort = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 1001 + rank, zero_mean=True)).pin_memory()
+    h_div = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 2001 + rank, zero_mean=True)).pin_memory()
+    o_spec = torch.empty_like(h_spec).pin_memory()
+    o_vort = torch.empty_like(h_vort).pin_memory()
+    o_div = torch.empty_like(h_div).pin_memory()
+    h2d = (h_spec.numel() + h_vort.numel() + h_div.numel()) * 16
+    d2h = h2d
+
+    def e2e_step():
+        spec.copy_(h_spec, non_blocking=True)
+        vort.copy_(h_vort, non_blocking=True)
+        div.copy_(h_div, non_blocking=True)
+        z, d = step()
+        o_spec.copy_(spec_out, non_blocking=True)
+        o_vort.copy_(z, non_blocking=True)
+        o_div.copy_(d, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e7, e8 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e7.record(st)
+    for _ in range(args.steps):
+        e2e_step()
+    e8.record(st)
+    torch.cuda.synchronize()
+    ms_e2e = e7.elapsed_time(e8) / args.steps
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = flops_step * world / (ms_e2e * 1e-3) / 1e9
+    del spec, vort, div, grid, four
+    torch.cuda.empty_cache()
+
+    extra = {}
+    if not args.quick:
+        extra["rk4"] = rk4_rates(dev, args)
+    return dict(value=value, ms=ms, roofline=roofline, clocks=clk.summary(),
+                e2e={"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                     "ms_per_step": ms_e2e},
+                launches=launches_per_step * args.steps, accuracy={"scalar_roundtrip_rel_l2": rt_scalar,
+                                                                   "vector_roundtrip_rel_l2": rt_vec},
+                extra=extra)
+
+
+def rk4_rates(dev, args):
+    """Nonlinear RK4 steps/s (FP64 path) at T255 and at the T63 plain-method configuration."""
+    import torch
+
+    from sph_swe_b200.sph import Sph
+
+    # T255: the reference's non-Robert advective form is unstable at dt = 30 s
+    # (the oracle diverges within 60 steps); dt = 10 s with the reference's
+    # default viscosity 1e5 runs stably.  T63: the plain-method configuration.
+    out = {}
+    for L, dt, a, visc in ((255, 10.0, 6.371e6, 1e5), (63, 120.0, 6.371e6, 0.0)):
+        s = Sph(L)
+        lat0, lon0 = np.deg2rad(30.0), np.deg2rad(60.0)
+
+        def bump(lon, mu):
+            p = np.arcsin(mu)
+            c = np.sin(p) * np.sin(lat0) + np.cos(p) * np.cos(lat0) * np.cos(lon - lon0)
+            return 1e4 + 500.0 * np.exp(-(np.arccos(np.clip(c, -1, 1)) / 0.1) ** 2)
+
+        hgrid = torch.from_numpy(s.grid_from(bump)).to(dev)
+        st = torch.zeros(3, s.nlm, dtype=torch.complex128, device=dev)
+        st[0] = s.spat_to_SH(hgrid)
+        p = Sph.swe_params(radius=a, dt=dt, viscosity=visc)
+        s.swe_rk4(p, st, 3)
+        torch.cuda.synchronize()
+        n = 50 if L == 255 else 200
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.swe_rk4(p, st, n)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        out[f"T{L}"] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms, "nsteps": n, "dt": dt, "viscosity": visc,
+                        "kernel_launches_per_step": 4 * 11 + 1}
+        s.close()
+    return out
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle port)
+def cpu_baseline(min_seconds=10.0, max_reps=50):
+    """Oracle restatement of the same transforms on the host cores: repeated
+    inverse + forward of the 64 scalar T255 fields until >= min_seconds."""
+    from oracle import oracle as O
+
+    g = O.Grid(L_CFG1)
+    spec = random_spec(L_CFG1, N_SCALAR, 7)
+    _, _, per_contr = cfg1_flops()
+    fft_per_field = 2.5 * g.nphi * math.log2(g.nphi) * g.nlat
+    g.spat_to_SH(g.SH_to_spat(spec[:2]))
+    reps = 0
+    t0 = time.perf_counter()
+    while reps < max_reps:
+        g.spat_to_SH(g.SH_to_spat(spec))
+        reps += 1
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    flops = reps * N_SCALAR * 2 * (per_contr + fft_per_field)
+    return {"value": flops / dt / 1e9, "unit": "GFLOP/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{reps} x (inverse + forward) of the {N_SCALAR} scalar T255 fields "
+                      f"(oracle C++/OpenMP FP64, {dt:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    """CPU arm: the oracle (C++/OpenMP FP64 restatement; the reference's own
+    SHTNS/FFTW/LAPACK build is unavailable on this machine) on all host cores.
+    One step: inverse + forward of 128 scalar T255 fields (the 64 scalar fields
+    and the 32 vector pairs counted as two scalar fields each)."""
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+
+    O.build()
+    g = O.Grid(L_CFG1)
+    spec = random_spec(L_CFG1, N_SCALAR + 2 * N_PAIRS, 7)
+    _, _, per_contr = cfg1_flops()
+    fft_per_field = 2.5 * g.nphi * math.log2(g.nphi) * g.nlat
+    for _ in range(args.warmup):
+        g.spat_to_SH(g.SH_to_spat(spec[:4]))
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        g.spat_to_SH(g.SH_to_spat(spec))
+        ts.append(time.perf_counter() - t0)
+    dt = float(np.mean(ts))
+    flops = spec.shape[0] * 2 * (per_contr + fft_per_field)
+    value = flops / dt / 1e9
+    sample = (f"per step inverse + forward of {spec.shape[0]} scalar T255 fields (oracle C++/OpenMP FP64; the "
+              "reference's SHTNS/FFTW/LAPACK build is unavailable on this machine)")
+    return {"metric": METRIC, "value": value, "unit": "GFLOP/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "SHT throughput: T255 384x768 Gauss grid, 64 scalar fields + 32 vort/div pairs, "
+                                   "inverse + forward per step", "lmax": L_CFG1, "nlat": 384, "nphi": 768},
+            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="skip the RK4 side measurements")
+    ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the dominant kernel")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res))
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+        return
+
+    r = run_ours(args, rank, world)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": r["value"], "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "SHT throughput: T255 384x768 Gauss grid, 64 scalar fields + 32 vort/div pairs, "
+                                   "inverse + forward per step (FP64 plain method)",
+                       "lmax": L_CFG1, "nlat": 384, "nphi": 768, "fields": N_SCALAR, "vector_pairs": N_PAIRS,
+                       "gflop_per_step": sum(cfg1_flops()[:2]) / 1e9,
+                       "l2": "inputs larger than L2 (>= 270 MB touched per step); no flush"},
+            "roofline": r["roofline"], "clocks": r["clocks"], "e2e": r["e2e"], "gpu_launches": r["launches"],
+            "accuracy": r["accuracy"],
+        }
+        if not args.quick:
+            line["cpu_baseline"] = cpu_baseline()
+        line.update(r["extra"])
+        print(json.dumps(line))
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -115,6 +115,17 @@ int sph_vec_SH_to_spat(sph_handle* h, const double* vort, const double* div, dou
 int sph_vec_spat_to_SH(sph_handle* h, const double* u, const double* v, double* vort, double* div, int batch,
                        int robert, void* stream);
 
+/* Legendre stage alone (per-m contraction with P_l^m at the Gauss nodes), for
+ * callers that run their own longitude stage or profile the stages apart.
+ * Fourier buffer four: double2[batch][L+1][nlat], F_m(mu_j) at
+ * four[b*(L+1)*nlat + m*nlat + j], with the analysis convention
+ * F_m = (2 pi / nphi) sum_i f(lambda_i) e^{-i m lambda_i}; the synthesis writes
+ * F_m without that factor, so that f = sum_m (2 - delta_m0) Re(F_m e^{i m lambda}).
+ * These are the Legendre halves of SHTNS spat_to_SH / SH_to_spat
+ * (SPHData.hpp:201,221). */
+int sph_legendre_synthesis(sph_handle* h, const double* spec, double* four, int batch, void* stream);
+int sph_legendre_analysis(sph_handle* h, const double* four, double* spec, int batch, void* stream);
+
 /* ---------------------------------------------------------------- spectral operators */
 
 enum sph_spec_op_id {

@@ -215,6 +215,22 @@ int sph_cplx_SH_to_spat(sph_handle* h, const double* spec, double* spat, int bat
     return ring_synthesis_cplx(h, F, ldF, reinterpret_cast<double2*>(spat), ld_spat, batch, S(stream));
 }
 
+int sph_legendre_synthesis(sph_handle* h, const double* spec, double* four, int batch, void* stream) {
+    CHECK_H("sph_legendre_synthesis");
+    if (batch < 0 || (batch > 0 && (!spec || !four))) { set_error("sph_legendre_synthesis: bad arguments"); return SPH_ERR_ARG; }
+    const long long ldF = (long long)(h->L + 1) * h->nlat;
+    return legendre_synthesis_real(h, reinterpret_cast<const double2*>(spec), h->nlm, h->L,
+                                   reinterpret_cast<double2*>(four), ldF, batch, S(stream));
+}
+
+int sph_legendre_analysis(sph_handle* h, const double* four, double* spec, int batch, void* stream) {
+    CHECK_H("sph_legendre_analysis");
+    if (batch < 0 || (batch > 0 && (!spec || !four))) { set_error("sph_legendre_analysis: bad arguments"); return SPH_ERR_ARG; }
+    const long long ldF = (long long)(h->L + 1) * h->nlat;
+    return legendre_analysis_real(h, reinterpret_cast<const double2*>(four), ldF, reinterpret_cast<double2*>(spec), h->nlm,
+                                  h->L, batch, S(stream));
+}
+
 int sph_spec_op(sph_handle* h, int op, const double* in, double* out, double a_re, double a_im, double b_re,
                 double b_im, int batch, int cplx, void* stream) {
     CHECK_H("sph_spec_op");

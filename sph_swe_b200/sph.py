@@ -102,6 +102,16 @@ class Sph:
                                                  _stream()))
         return vort, div
 
+    def legendre_synthesis(self, spec: torch.Tensor, four: torch.Tensor) -> torch.Tensor:
+        batch = spec.numel() // self.nlm
+        capi.check(capi.lib().sph_legendre_synthesis(self.h, _ptr(spec), _ptr(four), batch, _stream()))
+        return four
+
+    def legendre_analysis(self, four: torch.Tensor, spec: torch.Tensor) -> torch.Tensor:
+        batch = spec.numel() // self.nlm
+        capi.check(capi.lib().sph_legendre_analysis(self.h, _ptr(four), _ptr(spec), batch, _stream()))
+        return spec
+
     # ------------------------------------------------------------ operators
     def spec_op(self, op, x: torch.Tensor, a: complex = 0.0, b: complex = 0.0, cplx: bool = False,
                 out: torch.Tensor | None = None) -> torch.Tensor:

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-@pytest.fixture(scope="module", params=[31, 63, 127])
+@pytest.fixture(scope="module", params=[31, 63, 127, 255])
 def pair(request, gpu, oracle_mod):
     from sph_swe_b200.sph import Sph
 
