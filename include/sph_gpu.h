@@ -93,6 +93,21 @@ int sph_spat_to_SH(sph_handle* h, const double* spat, double* spec, int batch, l
 int sph_SH_to_spat(sph_handle* h, const double* spec, double* spat, int batch, long long ld_spec,
                    long long ld_spat, void* stream);
 
+/* Real synthesis that performs no device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot have cudaMalloc called once
+ * they are running (their own allocator has reserved the device memory, or a
+ * cudaMalloc/cudaFree synchronisation would break their latency budget).
+ * Same result as sph_SH_to_spat on dense arrays (spec: batch*nlm complex,
+ * spat: batch*nphi*nlat doubles).  The Fourier intermediate lives in a fixed
+ * 8 MiB device array inside the library, shared by all calls and kept by
+ * every GPU that loads the library until the process exits: batch is limited
+ * to 8 MiB / ((L+1)*nlat*16 bytes) fields (5 at T255, 85 at T63) and larger
+ * batches fail with SPH_ERR_ARG.  The first call on each device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Calls that overlap on the GPU (other streams, other host threads) race on
+ * the shared array: serialise them. */
+int sph_SH_to_spat_noalloc(sph_handle* h, const double* spec, double* spat, int batch, void* stream);
+
 /* Complex analysis / synthesis on complex grids (double2[nphi*nlat]) and
  * (L+1)^2 complex coefficients.  Replace spat_cplx_to_SH / SH_to_spat_cplx
  * (SPHDataComplex.hpp:190,210,469-470,486-487). */

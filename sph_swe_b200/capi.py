@@ -19,7 +19,7 @@ OPS = dict(diff_lon=0, d1mu2=1, mu=2, mu2=3, laplace=4, helmholtz=5, scale=6, ax
 # every symbol declared in include/sph_gpu.h
 EXPORTS = (
     "sph_create", "sph_destroy", "sph_info", "sph_grid",
-    "sph_spat_to_SH", "sph_SH_to_spat", "sph_cplx_spat_to_SH", "sph_cplx_SH_to_spat",
+    "sph_spat_to_SH", "sph_SH_to_spat", "sph_SH_to_spat_noalloc", "sph_cplx_spat_to_SH", "sph_cplx_SH_to_spat",
     "sph_vec_SH_to_spat", "sph_vec_spat_to_SH", "sph_legendre_synthesis", "sph_legendre_analysis", "sph_spec_op",
     "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched",
     "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_last_error",
@@ -67,6 +67,7 @@ def lib():
         for n in ("sph_vec_SH_to_spat", "sph_vec_spat_to_SH"):
             getattr(L, n).argtypes = [vp, vp, vp, vp, vp, i, i, vp]
         L.sph_spec_op.argtypes = [vp, i, vp, vp, d, d, d, d, i, i, vp]
+        L.sph_SH_to_spat_noalloc.argtypes = [vp, vp, vp, i, vp]
         L.sph_legendre_synthesis.argtypes = [vp, vp, vp, i, vp]
         L.sph_legendre_analysis.argtypes = [vp, vp, vp, i, vp]
         L.sph_swe_tendency.argtypes = [vp, ctypes.POINTER(SWEParams), vp, vp, vp]

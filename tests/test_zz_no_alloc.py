@@ -1,0 +1,52 @@
+"""sph_SH_to_spat_noalloc: the synthesis entry point that performs no device
+allocation, for callers that cannot have cudaMalloc called while they run
+(their own allocator holds the device memory, or an implicit synchronisation
+would break their latency budget).  It must give the same grids as
+sph_SH_to_spat, call after call, while reusing the library's fixed scratch
+array.  This file is collected last on purpose."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(s, spec, out):
+    from sph_swe_b200 import capi
+
+    batch = spec.numel() // s.nlm
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return capi.lib().sph_SH_to_spat_noalloc(s.h, ctypes.c_void_p(spec.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                             batch, stream)
+
+
+@pytest.mark.parametrize("L,batch", [(63, 7), (255, 5)])
+def test_noalloc_synthesis_matches_allocating_entry_point(gpu, L, batch):
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+    from tests.helpers import random_spec, rel_l2
+
+    s = Sph(L)
+    for call in range(2):
+        spec = torch.from_numpy(random_spec(L, batch, seed=100 + 10 * L + call)).cuda()
+        ref = s.SH_to_spat(spec).cpu().numpy()
+        out = torch.full((batch, s.nphi, s.nlat), float("nan"), dtype=torch.float64, device="cuda")
+        rc = _noalloc(s, spec, out)
+        assert rc == capi.SPH_OK, capi.last_error()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.isfinite(got).all()
+        assert rel_l2(got, ref) < 1e-12, call
+
+
+def test_noalloc_rejects_batches_beyond_the_fixed_scratch(gpu):
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+
+    s = Sph(255)
+    spec = torch.zeros(6, s.nlm, dtype=torch.complex128, device="cuda")
+    out = torch.empty(6, s.nphi, s.nlat, dtype=torch.float64, device="cuda")
+    assert _noalloc(s, spec, out) == capi.SPH_ERR_ARG
+    assert "at most 5 fields" in capi.last_error()
