@@ -63,6 +63,7 @@ def lib():
         L.orc_swe_run.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]
         L.orc_rexi_run.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]
+        L.orc_rexi_pole.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_dp] * 8
         L.orc_auto_grid.argtypes = [ctypes.c_int, _ip, _ip]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_num_threads.restype = ctypes.c_int
@@ -251,6 +252,20 @@ class Grid:
         if rc not in (0, 3):
             raise RuntimeError(f"orc_swe_run rc={rc}")
         return hs, us, vs, rc
+
+    def rexi_pole(self, params, alpha, beta, phi0, u, v, robert=1, coriolis=1, fix_z5robert=False):
+        """One pole of SWERexiSPH[Robert]::setup+solve; returns the real spectra of Re(I(beta x))."""
+        p = np.array(params, np.float64)
+        al = np.array([complex(alpha).real, complex(alpha).imag])
+        be = np.array([complex(beta).real, complex(beta).imag])
+        ins = [np.ascontiguousarray(a, np.complex128) for a in (phi0, u, v)]
+        outs = [np.zeros(self.nlm, np.complex128) for _ in range(3)]
+        rc = lib().orc_rexi_pole(self.h, _p(p), robert, coriolis, int(fix_z5robert), _p(al), _p(be),
+                                 *[a.view(np.float64).ctypes.data_as(_dp) for a in ins],
+                                 *[a.view(np.float64).ctypes.data_as(_dp) for a in outs])
+        if rc:
+            raise RuntimeError(f"orc_rexi_pole rc={rc}")
+        return outs
 
     def rexi_run(self, params, h, u, v, nsteps, rexi_h=0.2, rexi_M=256, half=False, robert=1, coriolis=1,
                  fix_z5robert=False):

@@ -334,6 +334,30 @@ int orc_swe_run(const void* gp, const double* p, int nonlinear, int robert, doub
     }
 }
 
+// One pole of SWERexiSPH[Robert]::setup + solve: inputs phi0 = g h, u, v (real
+// spectral), outputs the real spectra of Re(I_c(beta * x)).  alpha, beta are
+// the raw pole coefficients (divided by tau inside setup).
+int orc_rexi_pole(const void* gp, const double* p, int robert, int coriolis, int fix_z5, const double* alpha,
+                  const double* beta, const double* phi0, const double* u, const double* v, double* ophi, double* ou,
+                  double* ov) {
+    const Grid* g = static_cast<const Grid*>(gp);
+    try {
+        RexiSWE s;
+        s.setup(g, cplx(alpha[0], alpha[1]), cplx(beta[0], beta[1]), p[0], p[2], p[3] * p[1], p[5],
+                coriolis != 0 && p[2] != 0, robert != 0, fix_z5 != 0);
+        Field P = real_from_spec(g, phi0), U = real_from_spec(g, u), V = real_from_spec(g, v);
+        Field a(g), b(g), c(g);
+        s.solve(P, U, V, a, b, c);
+        a.request_spec(); b.request_spec(); c.request_spec();
+        std::memcpy(ophi, (const void*)a.spec.data(), sizeof(cplx) * g->nlm);
+        std::memcpy(ou, (const void*)b.spec.data(), sizeof(cplx) * g->nlm);
+        std::memcpy(ov, (const void*)c.spec.data(), sizeof(cplx) * g->nlm);
+        return 0;
+    } catch (...) {
+        return 2;
+    }
+}
+
 // nsteps REXI steps (AppSWE::run REXI branch, extended modes off); state h,u,v
 // spectral in/out.  p as orc_swe_run (p[5] = tau).  Returns number of poles
 // used (>0) or <0 on error.

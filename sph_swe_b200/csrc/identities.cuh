@@ -6,6 +6,14 @@
 // matrices match it coefficient for coefficient.
 #pragma once
 
+#include <cmath>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+using std::sqrt;
+#endif
+
 namespace sphgpu {
 
 __host__ __device__ inline double idR(double k, double m) {

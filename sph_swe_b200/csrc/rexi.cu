@@ -1,21 +1,433 @@
-// REXI integrator (batched banded solves) — entry points.
+// REXI time integrator for the linear shallow-water equations, Robert
+// formulation (SWERexiSPHRobert.hpp), FP64 direct.
+//
+// Reference per step (AppSWE.hpp:580-729): for every pole (alpha_k, beta_k)
+// SWERexiSPHRobert::solve (SWERexiSPHRobert.hpp:139-258) promotes phi0 = g h,
+// u0, v0 to complex fields, builds a right-hand side from mu / mu^2 / (1-mu^2)d/dmu
+// recurrences, solves one banded system per zonal wavenumber m for phi
+// (9 diagonals, SPHSolverComplex + zgbsv), recovers u, v with two 5-diagonal
+// solves, scales by beta and accumulates Re(.) of the result.
+//
+// Here every part that does not depend on the pole is computed once per step
+// (the complex promotions, the divergence through one real synthesis /
+// analysis pair, eta0, and the mu / mu^2 images), so that the right-hand side
+// of a pole is a linear combination of 10 pole-independent vectors with
+// alpha-dependent weights, and the Phi matrix is
+//      A(alpha) = alpha^4 I + alpha^2 C2 + alpha C1 + alpha^-1 Cm1 + C0
+// with pole-independent band matrices C (the reference's z1..z8 components,
+// SPHSolverComplex.hpp:88-420, grouped by power of alpha).  All offsets are
+// even, so each m-block splits into two l-parities: pentadiagonal (Phi) and
+// tridiagonal (velocity) systems.  One warp handles one m-block for 32 poles
+// (one pole per lane): assembly, LU with partial pivoting (LAPACK zgbtf2 pivot
+// rule, |re|+|im|), back substitution, velocity recovery, beta scaling and a
+// warp reduction over its poles.  A final kernel sums the pole groups and takes
+// Re(.) spectrally: Q_lm = (A_lm + (-1)^m conj(A_l,-m)) / 2.
+// The complex grid product of the Coriolis term is applied as the full-grid
+// product (the reference multiplies only the first (L+1)^2 grid points,
+// SPHDataComplex.hpp:333): Proj[(1-mu^2) G] = G - mu2(G).
 #include "common.cuh"
+#include "identities.cuh"
+#include "rexi_tables.h"
+#include "rexi_lane.h"
+
+#include <cmath>
+#include <complex>
+#include <cstring>
+
+struct sph_rexi;
+
+namespace sphgpu {
+
+struct RexiPlan {
+    Handle* h = nullptr;
+    sph_rexi_params p{};
+    int npoles = 0, ngroups = 0;
+    double2* alpha = nullptr;   // alpha_k / tau
+    double2* beta = nullptr;    // beta_k / tau
+    double2* Cphi = nullptr;    // [4][ncplx][5]  (C2, C1, Cm1, C0), block (N-compact) rows
+    double2* Cvel = nullptr;    // [ncplx][3]
+    double* coef = nullptr;     // [ncplx][4]: R(n-1,m), S(n+1,m), (1-n)R(n-1,m), (n+2)S(n+1,m)
+    double2* V = nullptr;       // [18][ncplx] block layout
+    double2* part = nullptr;    // [ngroups][3][ncplx]
+    double2* X = nullptr;       // nlm (real layout)
+    double2* Xr = nullptr;      // nlm
+    double2* F = nullptr;       // (L+1)*nlat
+    int* flag = nullptr;        // bit0 non-finite h, bit1 singular pivot
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double* state = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+template <int MAXN>
+__global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int L = d.L;
+    const int nblk = 2 * L + 1;
+    if (warp >= nblk * d.ngroups) return;
+    const int g = warp % d.ngroups, kk = warp / d.ngroups;
+    const int m = (kk & 1) ? -((kk + 1) >> 1) : (kk >> 1);  // 0, -1, 1, -2, 2, ...: largest blocks first
+    const int N = L + 1 - (m < 0 ? -m : m);
+    const int base = block_off(L, m);
+    const int nc = d.ncplx;
+    const int pole = g * 32 + lane;
+    const bool valid = pole < d.npoles;
+    const double2 a = d.alpha[valid ? pole : 0];
+    const double2 bt = valid ? d.beta[pole] : make_double2(0, 0);
+    double2 phi[MAXN], ra[MAXN], rb[MAXN];
+    const bool ok = rexi_lane<MAXN>(d, m, a, phi, ra, rb);
+    if (!ok && valid) atomicOr(d.flag, 2);
+    // beta scaling and reduction over the 32 poles of this warp
+    double2* outp = d.part + (size_t)g * 3 * nc;
+    for (int i = 0; i < N; i++) {
+        double2 v0 = c_mul(bt, phi[i]), v1 = c_mul(bt, ra[i]), v2 = c_mul(bt, rb[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v0.x += __shfl_down_sync(0xffffffffu, v0.x, o);
+            v0.y += __shfl_down_sync(0xffffffffu, v0.y, o);
+            v1.x += __shfl_down_sync(0xffffffffu, v1.x, o);
+            v1.y += __shfl_down_sync(0xffffffffu, v1.y, o);
+            v2.x += __shfl_down_sync(0xffffffffu, v2.x, o);
+            v2.y += __shfl_down_sync(0xffffffffu, v2.y, o);
+        }
+        if (lane == 0) {
+            const int row = base + i;
+            outp[row] = v0;
+            outp[(size_t)nc + row] = v1;
+            outp[(size_t)2 * nc + row] = v2;
+        }
+    }
+}
+
+// ------------------------------------------------------------ pole-independent prep
+// real packed (degree L) -> complex block layout, times s:
+// c(n,m) = s x(n,m) for m >= 0, s (-1)^m conj(x(n,|m|)) for m < 0
+__global__ void k_rx_complexify(const double2* __restrict__ x, double s, double2* __restrict__ out, int L) {
+    const int m = (int)blockIdx.y - L;
+    const int am = m < 0 ? -m : m;
+    const int n = am + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n > L) return;
+    double2 v = x[pidx(L, n, am)];
+    if (m < 0) v = make_double2((am & 1) ? -v.x : v.x, (am & 1) ? v.y : -v.y);
+    out[brow(L, n, m)] = make_double2(v.x * s, v.y * s);
+}
+
+// block-layout operators: 0 mu, 1 mu2, 2 eta = ir (i m V - D U) (in = U, in2 = V),
+// 3 lincomb out = x - y (in, in2)
+__global__ void k_rx_block_op(int op, const double2* __restrict__ in, const double2* __restrict__ in2,
+                              double2* __restrict__ out, int L, double ir) {
+    const int m = (int)blockIdx.y - L;
+    const int am = m < 0 ? -m : m;
+    const int n = am + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n > L) return;
+    const int base = block_off(L, m);
+    auto at = [&](const double2* p, int nn) -> double2 {
+        if (nn < am || nn > L) return make_double2(0, 0);
+        return p[base + nn - am];
+    };
+    const double dn = n, dm = m;
+    double2 r;
+    if (op == 0) {
+        const double cl = idR(dn - 1, dm), ch = idS(dn + 1, dm);
+        const double2 lo = at(in, n - 1), hi = at(in, n + 1);
+        r = make_double2(cl * lo.x + ch * hi.x, cl * lo.y + ch * hi.y);
+    } else if (op == 1) {
+        const double ca = idA(dn - 2, dm), cb = idB(dn, dm), cc = idC(dn + 2, dm);
+        const double2 lo = at(in, n - 2), mid = at(in, n), hi = at(in, n + 2);
+        r = make_double2(ca * lo.x + cb * mid.x + cc * hi.x, ca * lo.y + cb * mid.y + cc * hi.y);
+    } else if (op == 2) {
+        const double cl = (-dn + 1.0) * idR(dn - 1, dm), ch = (dn + 2.0) * idS(dn + 1, dm);
+        const double2 ul = at(in, n - 1), uh = at(in, n + 1), v = at(in2, n);
+        const double2 du = make_double2(cl * ul.x + ch * uh.x, cl * ul.y + ch * uh.y);
+        r = make_double2(ir * (-dm * v.y - du.x), ir * (dm * v.x - du.y));
+    } else {
+        const double2 x = at(in, n), y = at(in2, n);
+        r = make_double2(x.x - y.x, x.y - y.y);
+    }
+    out[base + n - am] = r;
+}
+
+// X = i m u + D v (real packed layout) from the state
+__global__ void k_rx_divsrc(const double2* __restrict__ u, const double2* __restrict__ v, double2* __restrict__ X, int L) {
+    const int m = blockIdx.y;
+    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n > L) return;
+    const double dn = n, dm = m;
+    const double cl = (-dn + 1.0) * idR(dn - 1, dm), ch = (dn + 2.0) * idS(dn + 1, dm);
+    const double2 lo = n - 1 >= m ? v[pidx(L, n - 1, m)] : make_double2(0, 0);
+    const double2 hi = n + 1 <= L ? v[pidx(L, n + 1, m)] : make_double2(0, 0);
+    const double2 uu = u[pidx(L, n, m)];
+    X[pidx(L, n, m)] = make_double2(-dm * uu.y + cl * lo.x + ch * hi.x, dm * uu.x + cl * lo.y + ch * hi.y);
+}
+
+// Fourier-space F *= 2 pi / c^2 (synthesis -> analysis convention, / cos^2 phi)
+__global__ void k_rx_fscale(double2* __restrict__ F, int nlat, int mF, const double* __restrict__ cosphi) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= mF * nlat) return;
+    const double c = cosphi[idx % nlat];
+    const double s = 2.0 * kPi / (c * c);
+    F[idx] = make_double2(F[idx].x * s, F[idx].y * s);
+}
+
+// sum the pole groups, take Re(.) spectrally and write the real state:
+// h = Re(phi)/g, u, v; optional implicit viscosity x / (1 + nu tau n(n+1)/r^2)
+__global__ void k_rx_finish(const double2* __restrict__ part, int ngroups, int ncplx, double2* __restrict__ state,
+                            int L, int nlm, double inv_g, double visc_fac, int* __restrict__ flag) {
+    const int m = blockIdx.y;
+    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n > L) return;
+    const int rp = brow(L, n, m), rm = brow(L, n, -m);
+    const double dn = n;
+    const double vf = 1.0 / (1.0 + visc_fac * dn * (dn + 1.0));
+    for (int f = 0; f < 3; f++) {
+        double2 ap = make_double2(0, 0), amn = make_double2(0, 0);
+        for (int g = 0; g < ngroups; g++) {
+            const double2* p = part + ((size_t)g * 3 + f) * ncplx;
+            ap = c_add(ap, p[rp]);
+            amn = c_add(amn, p[rm]);
+        }
+        // (A(n,m) + (-1)^m conj(A(n,-m))) / 2
+        const double sg = (m & 1) ? -1.0 : 1.0;
+        double2 q = make_double2(0.5 * (ap.x + sg * amn.x), 0.5 * (ap.y - sg * amn.y));
+        if (f == 0) q = make_double2(q.x * inv_g, q.y * inv_g);
+        q = make_double2(q.x * vf, q.y * vf);
+        if (f == 0 && !(isfinite(q.x) && isfinite(q.y))) atomicOr(flag, 1);
+        state[(size_t)f * nlm + pidx(L, n, m)] = q;
+    }
+}
+
+static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
+    Handle* h = R->h;
+    const int L = h->L, nlm = h->nlm, nc = h->ncplx, nlat = h->nlat, mF = L + 1;
+    const double g = R->p.gravity, ir = 1.0 / R->p.radius;
+    const double2* hh = state;
+    const double2* uu = state + nlm;
+    const double2* vv = state + 2 * (size_t)nlm;
+    const dim3 gc((L + 1 + 63) / 64, 2 * L + 1), gr((L + 1 + 63) / 64, L + 1);
+    double2* V = R->V;
+    auto Vs = [&](int k) { return V + (size_t)k * nc; };
+    // divergence of the Robert velocities: F(I(i m u + D v)/c^2), real transforms
+    k_rx_divsrc<<<gr, 64, 0, s>>>(uu, vv, R->X, L);
+    if (int rc = legendre_synthesis_real(h, R->X, nlm, L, R->F, (long long)mF * nlat, 1, s)) return rc;
+    k_rx_fscale<<<(mF * nlat + 255) / 256, 256, 0, s>>>(R->F, nlat, mF, h->cosphi);
+    if (int rc = legendre_analysis_real(h, R->F, (long long)mF * nlat, R->Xr, nlm, L, 1, s)) return rc;
+    // complex promotions: 0 div0 = ir div, 2 phi0 = g h, 10 u0, 11 v0
+    k_rx_complexify<<<gc, 64, 0, s>>>(R->Xr, ir, Vs(0), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(hh, g, Vs(2), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(uu, 1.0, Vs(10), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(vv, 1.0, Vs(11), L);
+    // 14 eta0, 1 mu(eta0), 3 mu2(phi0), 4 mu2(div0), 5 mu2(mu eta0), 6 mu2 mu2 phi0
+    k_rx_block_op<<<gc, 64, 0, s>>>(2, Vs(10), Vs(11), Vs(14), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(0, Vs(14), nullptr, Vs(1), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(2), nullptr, Vs(3), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(0), nullptr, Vs(4), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(1), nullptr, Vs(5), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(3), nullptr, Vs(6), L, ir);
+    // 15 mu2 u0, 16 mu2 mu2 u0, 12 mu v0, 17 mu2 mu v0, 13 mu u0
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(10), nullptr, Vs(15), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(15), nullptr, Vs(16), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(0, Vs(11), nullptr, Vs(12), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(12), nullptr, Vs(17), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(0, Vs(10), nullptr, Vs(13), L, ir);
+    // 7 W1 = u0 - mu2 u0, 8 W2 = mu2 u0 - mu2 mu2 u0, 9 W3 = mu v0 - mu2 mu v0
+    k_rx_block_op<<<gc, 64, 0, s>>>(3, Vs(10), Vs(15), Vs(7), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(3, Vs(15), Vs(16), Vs(8), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(3, Vs(12), Vs(17), Vs(9), L, ir);
+    SPH_CUDA_TRY(cudaGetLastError());
+    // all poles x all m x both parities
+    RexiDev d;
+    d.L = L;
+    d.npoles = R->npoles;
+    d.ngroups = R->ngroups;
+    d.ncplx = nc;
+    d.coriolis = (R->p.coriolis && R->p.omega != 0.0) ? 1 : 0;
+    d.r = R->p.radius;
+    d.ir = ir;
+    d.T = 2.0 * R->p.omega;
+    d.P = R->p.h0 * R->p.gravity;
+    d.alpha = R->alpha;
+    d.beta = R->beta;
+    d.Cphi = R->Cphi;
+    d.Cvel = R->Cvel;
+    d.coef = R->coef;
+    d.V = R->V;
+    d.part = R->part;
+    d.flag = R->flag;
+    const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
+    const unsigned nb = (unsigned)((nthreads + 63) / 64);
+    if (L + 1 <= 64) k_rexi_solve<64><<<nb, 64, 0, s>>>(d);
+    else if (L + 1 <= 128) k_rexi_solve<128><<<nb, 64, 0, s>>>(d);
+    else k_rexi_solve<256><<<nb, 64, 0, s>>>(d);
+    SPH_CUDA_TRY(cudaGetLastError());
+    const double visc_fac = R->p.viscosity * R->p.tau / (R->p.radius * R->p.radius);
+    k_rx_finish<<<gr, 64, 0, s>>>(R->part, R->ngroups, nc, state, L, nlm, 1.0 / g, visc_fac, R->flag);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+static void rexi_free(RexiPlan* R) {
+    if (!R) return;
+    if (R->exec) cudaGraphExecDestroy(R->exec);
+    if (R->graph) cudaGraphDestroy(R->graph);
+    void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V, R->part, R->X, R->Xr, R->F, R->flag};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    delete R;
+}
+
+}  // namespace sphgpu
 
 using namespace sphgpu;
 
+struct sph_rexi : public RexiPlan {};
+
 extern "C" {
 
-int sph_rexi_create(sph_handle*, const double*, const double*, int, const sph_rexi_params*, sph_rexi** out) {
+int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int npoles, const sph_rexi_params* p,
+                    sph_rexi** out) {
     if (out) *out = nullptr;
-    set_error("sph_rexi_create: not available in this build");
-    return SPH_ERR_ARG;
+    Handle* h = reinterpret_cast<Handle*>(hh);
+    if (!h || !alpha || !beta || npoles <= 0 || !p || !out || p->tau == 0.0 || p->radius <= 0.0) {
+        set_error("sph_rexi_create: bad arguments");
+        return SPH_ERR_ARG;
+    }
+    if (!p->robert) {
+        set_error("sph_rexi_create: only the Robert formulation (SWERexiSPHRobert) runs on the GPU path");
+        return SPH_ERR_ARG;
+    }
+    if (p->precision != SPH_PREC_FP64) {
+        set_error("sph_rexi_create: precision must be SPH_PREC_FP64 in this build");
+        return SPH_ERR_ARG;
+    }
+    if (h->L > 255) {
+        set_error("sph_rexi_create: truncations above T255 are not supported by the REXI solver");
+        return SPH_ERR_ARG;
+    }
+    sph_rexi* R = new sph_rexi();
+    R->h = h;
+    R->p = *p;
+    R->npoles = npoles;
+    R->ngroups = (npoles + 31) / 32;
+    const int L = h->L, nc = h->ncplx;
+    // pole scalars alpha/tau, beta/tau (SWERexiSPHRobert.hpp:84-85)
+    std::vector<double2> al(npoles), be(npoles);
+    for (int k = 0; k < npoles; k++) {
+        al[k] = make_double2(alpha[2 * k] / p->tau, alpha[2 * k + 1] / p->tau);
+        be[k] = make_double2(beta[2 * k] / p->tau, beta[2 * k + 1] / p->tau);
+    }
+    // pole-independent band matrices, grouped by power of alpha
+    const double r = p->radius, T = 2.0 * p->omega, P = p->h0 * p->gravity;
+    BandTable C2(L), C1(L), Cm1(L), C0(L), Cv(L);
+    const bool cor = p->coriolis && p->omega != 0.0;
+    comp_z7(C2, cd(-P), r);
+    if (cor) {
+        comp_z2(C2, cd(2.0 * T * T));
+        comp_z3(C0, cd(T * T * T * T));
+        comp_z4robert(C1, cd(-P * T), r);
+        comp_z5robert(Cm1, cd(P * T * T * T), r, p->fix_z5robert != 0);
+        comp_z6robert(C0, cd(P * 2.0 * T * T), r);
+        comp_z8(C0, cd(-P * T * T), r);
+        comp_z2(Cv, cd(T * T));
+    }
+    std::vector<double2> cphi((size_t)4 * nc * 5), cvel((size_t)nc * 3);
+    const BandTable* tabs[4] = {&C2, &C1, &Cm1, &C0};
+    for (int q = 0; q < 4; q++)
+        for (size_t i = 0; i < (size_t)nc * 5; i++)
+            cphi[(size_t)q * nc * 5 + i] = make_double2(tabs[q]->a[i].real(), tabs[q]->a[i].imag());
+    for (int row = 0; row < nc; row++)
+        for (int dd = 0; dd < 3; dd++) {
+            const cd v = Cv.a[(size_t)row * 5 + dd + 1];
+            cvel[(size_t)row * 3 + dd] = make_double2(v.real(), v.imag());
+        }
+    std::vector<double> coef((size_t)nc * 4);
+    for (int m = -L; m <= L; m++)
+        for (int n = std::abs(m); n <= L; n++) {
+            const int row = brow(L, n, m);
+            coef[(size_t)row * 4 + 0] = idR(n - 1, m);
+            coef[(size_t)row * 4 + 1] = idS(n + 1, m);
+            coef[(size_t)row * 4 + 2] = (-(double)n + 1.0) * idR(n - 1, m);
+            coef[(size_t)row * 4 + 3] = ((double)n + 2.0) * idS(n + 1, m);
+        }
+    auto fail = [&](int rc) {
+        rexi_free(R);
+        return rc;
+    };
+#define RX_TRY(x)                                                               \
+    do {                                                                        \
+        cudaError_t e_ = (x);                                                   \
+        if (e_ != cudaSuccess) {                                                \
+            set_error(std::string("sph_rexi_create: ") + cudaGetErrorString(e_)); \
+            return fail(SPH_ERR_CUDA);                                          \
+        }                                                                       \
+    } while (0)
+    RX_TRY(cudaMalloc(&R->alpha, sizeof(double2) * npoles));
+    RX_TRY(cudaMalloc(&R->beta, sizeof(double2) * npoles));
+    RX_TRY(cudaMalloc(&R->Cphi, sizeof(double2) * cphi.size()));
+    RX_TRY(cudaMalloc(&R->Cvel, sizeof(double2) * cvel.size()));
+    RX_TRY(cudaMalloc(&R->coef, sizeof(double) * coef.size()));
+    RX_TRY(cudaMalloc(&R->V, sizeof(double2) * 18 * (size_t)nc));
+    RX_TRY(cudaMalloc(&R->part, sizeof(double2) * 3 * (size_t)nc * R->ngroups));
+    RX_TRY(cudaMalloc(&R->X, sizeof(double2) * h->nlm));
+    RX_TRY(cudaMalloc(&R->Xr, sizeof(double2) * h->nlm));
+    RX_TRY(cudaMalloc(&R->F, sizeof(double2) * (size_t)(L + 1) * h->nlat));
+    RX_TRY(cudaMalloc(&R->flag, sizeof(int)));
+    RX_TRY(cudaMemcpy(R->alpha, al.data(), sizeof(double2) * npoles, cudaMemcpyHostToDevice));
+    RX_TRY(cudaMemcpy(R->beta, be.data(), sizeof(double2) * npoles, cudaMemcpyHostToDevice));
+    RX_TRY(cudaMemcpy(R->Cphi, cphi.data(), sizeof(double2) * cphi.size(), cudaMemcpyHostToDevice));
+    RX_TRY(cudaMemcpy(R->Cvel, cvel.data(), sizeof(double2) * cvel.size(), cudaMemcpyHostToDevice));
+    RX_TRY(cudaMemcpy(R->coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice));
+    RX_TRY(cudaMemset(R->V, 0, sizeof(double2) * 18 * (size_t)nc));
+    RX_TRY(cudaMemset(R->flag, 0, sizeof(int)));
+#undef RX_TRY
+    *out = R;
+    return SPH_OK;
 }
 
-int sph_rexi_destroy(sph_rexi*) { return SPH_OK; }
+int sph_rexi_destroy(sph_rexi* r) {
+    if (!r) return SPH_OK;
+    cudaDeviceSynchronize();
+    rexi_free(r);
+    return SPH_OK;
+}
 
-int sph_rexi_step(sph_rexi*, double*, int, void*) {
-    set_error("sph_rexi_step: not available in this build");
-    return SPH_ERR_ARG;
+int sph_rexi_step(sph_rexi* R, double* state, int nsteps, void* stream) {
+    if (!R || !state || nsteps < 0) {
+        set_error("sph_rexi_step: bad arguments");
+        return SPH_ERR_ARG;
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!R->exec || R->state != state || R->stream != s) {
+        if (R->exec) { cudaGraphExecDestroy(R->exec); R->exec = nullptr; }
+        if (R->graph) { cudaGraphDestroy(R->graph); R->graph = nullptr; }
+        cudaStream_t cap;
+        SPH_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        SPH_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        int rc = rexi_step_launch(R, reinterpret_cast<double2*>(state), cap);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) { set_error(std::string("sph_rexi_step: capture: ") + cudaGetErrorString(e)); return SPH_ERR_CUDA; }
+        R->graph = g;
+        SPH_CUDA_TRY(cudaGraphInstantiate(&R->exec, g, 0));
+        R->state = state;
+        R->stream = s;
+    }
+    SPH_CUDA_TRY(cudaMemsetAsync(R->flag, 0, sizeof(int), s));
+    for (int i = 0; i < nsteps; i++) SPH_CUDA_TRY(cudaGraphLaunch(R->exec, s));
+    int flag = 0;
+    SPH_CUDA_TRY(cudaMemcpyAsync(&flag, R->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPH_CUDA_TRY(cudaStreamSynchronize(s));
+    if (flag & 2) {
+        set_error("sph_rexi_step: zero pivot in a banded solve (zgbsv INFO > 0)");
+        return SPH_ERR_SINGULAR;
+    }
+    if (flag & 1) {
+        set_error("sph_rexi_step: instability detected (non-finite value in h)");
+        return SPH_ERR_NAN;
+    }
+    return SPH_OK;
 }
 
 }  // extern "C"

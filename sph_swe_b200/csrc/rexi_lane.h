@@ -1,0 +1,281 @@
+// Per-pole arithmetic of the REXI solver (one thread = one pole x one m-block),
+// shared by the CUDA kernel in rexi.cu and its CPU unit test.
+#pragma once
+
+#include <cmath>
+#include <vector_types.h>
+#include <vector_functions.h>
+
+#include "rexi_tables.h"
+
+#ifdef __CUDA_ARCH__
+#define RX_LDG(p) __ldg(p)
+#else
+#define RX_LDG(p) (*(p))
+using std::fabs;
+#endif
+
+namespace sphgpu {
+
+struct RexiDev {
+    int L, npoles, ngroups, ncplx;
+    int coriolis;
+    double r, ir, T, P;  // radius, 1/radius, 2 Omega, average geopotential
+    const double2* alpha;
+    const double2* beta;
+    const double2* Cphi;
+    const double2* Cvel;
+    const double* coef;
+    const double2* V;
+    double2* part;
+    int* flag;
+};
+
+__host__ __device__ inline double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ inline double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ inline double2 c_mul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ inline double2 c_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ inline double2 c_div(double2 a, double2 b) {
+    const double d = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__host__ __device__ inline double c_abs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+__host__ __device__ inline double2 c_im(double2 a, double m) { return make_double2(-m * a.y, m * a.x); }  // a * i m
+__host__ __device__ inline double2 ld(const double2* p) { return RX_LDG(p); }
+
+// Banded LU with partial pivoting (kl = ku = H on the parity-reduced system of
+// Np rows) and solve for NR right-hand sides, one system per thread.
+// entry(k, d) gives A[k][k+d] for d = -H..H, rhs(k, r) right-hand side r.
+// Solutions are written through out(k, r, x).  Returns false on a zero pivot.
+// The pivot rule is LAPACK's (first maximum of |re|+|im| in the column).
+// U rows (2H+1 entries) and the eliminated right-hand sides live in the
+// thread-local arrays U / y.
+template <int H, int MAXR, int NR, class Entry, class Rhs, class Out>
+__host__ __device__ bool band_solve(int Np, Entry entry, Rhs rhs, Out out) {
+    constexpr int W = 2 * H + 1;
+    double2 U[MAXR][W];
+    double2 y[MAXR][NR];
+    double2 win[H + 1][W];  // rows k..k+H, columns k..k+2H
+    double2 wr[H + 1][NR];
+#pragma unroll
+    for (int i = 0; i <= H; i++) {
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - i;  // row i, column j
+            win[i][j] = (i < Np && d >= -H && d <= H && j < Np) ? entry(i, d) : make_double2(0, 0);
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) wr[i][r] = i < Np ? rhs(i, r) : make_double2(0, 0);
+    }
+    bool ok = true;
+    for (int k = 0; k < Np; k++) {
+        int p = 0;
+        double best = c_abs1(win[0][0]);
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const double v = (k + i < Np) ? c_abs1(win[i][0]) : -1.0;
+            if (v > best) {
+                best = v;
+                p = i;
+            }
+        }
+        if (best == 0.0) ok = false;
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < W; j++) {
+                const double2 t0 = win[0][j], ti = win[i][j];
+                win[0][j] = sw ? ti : t0;
+                win[i][j] = sw ? t0 : ti;
+            }
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const double2 t0 = wr[0][r], ti = wr[i][r];
+                wr[0][r] = sw ? ti : t0;
+                wr[i][r] = sw ? t0 : ti;
+            }
+        }
+        const double2 rp = best == 0.0 ? make_double2(0, 0) : c_div(make_double2(1, 0), win[0][0]);
+#pragma unroll
+        for (int j = 0; j < W; j++) U[k][j] = win[0][j];
+#pragma unroll
+        for (int r = 0; r < NR; r++) y[k][r] = wr[0][r];
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const double2 l = c_mul(win[i][0], rp);
+#pragma unroll
+            for (int j = 1; j < W; j++) win[i][j] = c_sub(win[i][j], c_mul(l, win[0][j]));
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[i][r] = c_sub(wr[i][r], c_mul(l, wr[0][r]));
+        }
+        // shift the window one row down / one column right, load row k+1+H
+#pragma unroll
+        for (int i = 0; i < H; i++) {
+#pragma unroll
+            for (int j = 0; j < W - 1; j++) win[i][j] = win[i + 1][j + 1];
+            win[i][W - 1] = make_double2(0, 0);
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[i][r] = wr[i + 1][r];
+        }
+        const int rn = k + 1 + H;
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - H;  // row rn at window row H, column j <-> matrix column k+1+j
+            win[H][j] = (rn < Np && k + 1 + j < Np) ? entry(rn, d) : make_double2(0, 0);
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) wr[H][r] = rn < Np ? rhs(rn, r) : make_double2(0, 0);
+    }
+    // back substitution with a sliding window of the last 2H solution values
+    double2 x[W][NR];
+#pragma unroll
+    for (int j = 0; j < W; j++)
+#pragma unroll
+        for (int r = 0; r < NR; r++) x[j][r] = make_double2(0, 0);
+    for (int k = Np - 1; k >= 0; k--) {
+        const double2 rd = c_div(make_double2(1, 0), U[k][0]);
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            double2 s = y[k][r];
+#pragma unroll
+            for (int j = 1; j < W; j++) s = c_sub(s, c_mul(U[k][j], x[j - 1][r]));
+            const double2 xk = c_mul(s, rd);
+#pragma unroll
+            for (int j = W - 1; j > 0; j--) x[j][r] = x[j - 1][r];
+            x[0][r] = xk;
+            out(k, r, xk);
+        }
+    }
+    return ok;
+}
+
+// One pole, one m-block: Phi solve (both l-parities), velocity right-hand
+// sides and the two velocity solves.  Writes the unscaled phi, u, v of the
+// block's N = L+1-|m| rows to phi / ra / rb; returns false on a zero pivot.
+template <int MAXN>
+__host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* phi, double2* ra, double2* rb) {
+    const int L = d.L;
+    const int am = m < 0 ? -m : m;
+    const int N = L + 1 - am;
+    const int base = block_off(L, m);
+    const double T = d.T, P = d.P, ir = d.ir;
+    const int nc = d.ncplx;
+    const double2* V = d.V;
+    const double2 a2 = c_mul(a, a), a3 = c_mul(a2, a), a4 = c_mul(a2, a2);
+    const double2 ainv = c_div(make_double2(1, 0), a);
+    const double dm = m;
+
+    bool ok = true;
+    if (d.coriolis) {
+        // right-hand side weights of the 10 pole-independent vectors
+        double2 s[10];
+        s[0] = c_scale(a2, P);                       // div0
+        s[1] = c_scale(a, -P * T);                    // mu(eta0)
+        s[2] = a3;                                    // phi0
+        s[3] = c_scale(a, 2.0 * T * T);               // mu2(phi0)
+        s[4] = make_double2(T * T * P, 0);            // mu2(div0)
+        s[5] = c_scale(ainv, -P * T * T * T);         // mu2(mu(eta0))
+        s[6] = c_scale(ainv, T * T * T * T);          // mu2(mu2(phi0))
+        s[7] = c_scale(a, -P * T * ir);               // W1 = u0 - mu2 u0
+        s[8] = c_scale(ainv, P * T * T * T * ir);     // W2 = mu2 u0 - mu2 mu2 u0
+        s[9] = make_double2(2.0 * P * T * T * ir, 0); // W3 = mu v0 - mu2 mu v0
+        for (int par = 0; par < 2; par++) {
+            const int Np = (N - par + 1) >> 1;
+            if (Np <= 0) continue;
+            auto entry = [&](int k, int dd) -> double2 {
+                const int row = base + par + 2 * k;
+                const double2* c = d.Cphi + (size_t)row * 5 + (dd + 2);
+                double2 v = c_mul(a2, ld(c));
+                v = c_add(v, c_mul(a, ld(c + (size_t)nc * 5)));
+                v = c_add(v, c_mul(ainv, ld(c + (size_t)2 * nc * 5)));
+                v = c_add(v, ld(c + (size_t)3 * nc * 5));
+                if (dd == 0) v = c_add(v, a4);
+                return v;
+            };
+            auto rhs = [&](int k, int) -> double2 {
+                const int row = base + par + 2 * k;
+                double2 v = make_double2(0, 0);
+#pragma unroll
+                for (int q = 0; q < 10; q++) v = c_add(v, c_mul(s[q], ld(&V[(size_t)q * nc + row])));
+                return v;
+            };
+            auto out = [&](int k, int, double2 x) { phi[par + 2 * k] = x; };
+            ok = band_solve<2, (MAXN + 1) / 2, 1>(Np, entry, rhs, out) && ok;
+        }
+        // rhsa = a u0 + a ir i m phi - T mu(v0) - T ir mu(D phi)
+        // rhsb = T mu(u0) + T ir mu(i m phi) + a v0 + a ir D phi
+        // D phi of every row, parked in ra until the right-hand sides are formed
+        for (int i = 0; i < N; i++) {
+            const double* cf = d.coef + (size_t)(base + i) * 4;
+            const double2 lo = i > 0 ? phi[i - 1] : make_double2(0, 0);
+            const double2 hi = i + 1 < N ? phi[i + 1] : make_double2(0, 0);
+            ra[i] = c_add(c_scale(lo, RX_LDG(cf + 2)), c_scale(hi, RX_LDG(cf + 3)));
+        }
+        double2 dprev = make_double2(0, 0);  // D phi of row i-1 (ra[i-1] is overwritten by then)
+        for (int i = 0; i < N; i++) {
+            const int row = base + i;
+            const double* cf = d.coef + (size_t)row * 4;
+            const double Rl = RX_LDG(cf), Sh = RX_LDG(cf + 1);
+            const double2 dcur = ra[i];
+            const double2 dnext = i + 1 < N ? ra[i + 1] : make_double2(0, 0);
+            const double2 plo = i > 0 ? phi[i - 1] : make_double2(0, 0);
+            const double2 phi_hi = i + 1 < N ? phi[i + 1] : make_double2(0, 0);
+            const double2 mud = c_add(c_scale(dprev, Rl), c_scale(dnext, Sh));  // mu(D phi)_i
+            const double2 mup = c_add(c_scale(plo, Rl), c_scale(phi_hi, Sh));   // mu(phi)_i
+            const double2 u0 = ld(&V[(size_t)10 * nc + row]), v0 = ld(&V[(size_t)11 * nc + row]);
+            const double2 mv = ld(&V[(size_t)12 * nc + row]), mu0 = ld(&V[(size_t)13 * nc + row]);
+            double2 xa = c_mul(a, u0);
+            xa = c_add(xa, c_mul(a, c_scale(c_im(phi[i], dm), ir)));
+            xa = c_sub(xa, c_scale(mv, T));
+            xa = c_sub(xa, c_scale(mud, T * ir));
+            double2 xb = c_scale(mu0, T);
+            xb = c_add(xb, c_scale(c_im(mup, dm), T * ir));
+            xb = c_add(xb, c_mul(a, v0));
+            xb = c_add(xb, c_mul(a, c_scale(dcur, ir)));
+            ra[i] = xa;
+            rb[i] = xb;
+            dprev = dcur;
+        }
+        for (int par = 0; par < 2; par++) {
+            const int Np = (N - par + 1) >> 1;
+            if (Np <= 0) continue;
+            auto entry = [&](int k, int dd) -> double2 {
+                const int row = base + par + 2 * k;
+                double2 v = ld(&d.Cvel[(size_t)row * 3 + dd + 1]);
+                if (dd == 0) v = c_add(v, a2);
+                return v;
+            };
+            // u and v share the matrix: one factorisation, two right-hand sides
+            auto rhs2 = [&](int k, int r) -> double2 { return r == 0 ? ra[par + 2 * k] : rb[par + 2 * k]; };
+            auto out2 = [&](int k, int r, double2 x) {
+                if (r == 0) ra[par + 2 * k] = x;
+                else rb[par + 2 * k] = x;
+            };
+            ok = band_solve<1, (MAXN + 1) / 2, 2>(Np, entry, rhs2, out2) && ok;
+        }
+    } else {
+        // phi = (P div0 + a phi0) / (a^2 + (P/r^2) n(n+1)); u = (u0 + ir i m phi)/a; v = (v0 + ir D phi)/a
+        for (int i = 0; i < N; i++) {
+            const int row = base + i;
+            const double n = am + i;
+            const double2 rhs = c_add(c_scale(ld(&V[row]), P), c_mul(a, ld(&V[(size_t)2 * nc + row])));
+            const double2 den = c_add(a2, make_double2(P / (d.r * d.r) * n * (n + 1.0), 0));
+            phi[i] = c_div(rhs, den);
+        }
+        for (int i = 0; i < N; i++) {
+            const int row = base + i;
+            const double* cf = d.coef + (size_t)row * 4;
+            const double2 lo = i > 0 ? phi[i - 1] : make_double2(0, 0);
+            const double2 hi = i + 1 < N ? phi[i + 1] : make_double2(0, 0);
+            const double2 dp = c_add(c_scale(lo, RX_LDG(cf + 2)), c_scale(hi, RX_LDG(cf + 3)));
+            ra[i] = c_mul(ainv, c_add(ld(&V[(size_t)10 * nc + row]), c_scale(c_im(phi[i], dm), ir)));
+            rb[i] = c_mul(ainv, c_add(ld(&V[(size_t)11 * nc + row]), c_scale(dp, ir)));
+        }
+    }
+    return ok;
+}
+
+}  // namespace sphgpu

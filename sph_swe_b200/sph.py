@@ -153,7 +153,44 @@ class Sph:
                                                   _stream()))
         return state
 
+    # ------------------------------------------------------------ REXI
+    def rexi(self, alpha, beta, radius=6.37122e6, gravity=9.80616, omega=7.292e-5, h0=1e4, viscosity=0.0,
+             tau=3600.0, robert=1, coriolis=1, fix_z5robert=0, precision=capi.SPH_PREC_FP64) -> "Rexi":
+        return Rexi(self, alpha, beta, capi.RexiParams(radius, gravity, omega, h0, viscosity, tau, robert, coriolis,
+                                                       fix_z5robert, precision))
+
     # ------------------------------------------------------------ helpers
     def grid_from(self, f) -> np.ndarray:
         LON, MU = np.meshgrid(self.lon, self.mu, indexing="ij")
         return np.ascontiguousarray(f(LON, MU))
+
+
+class Rexi:
+    """REXI integrator (replaces the per-pole SWERexiSPHRobert set of AppSWE::run)."""
+
+    def __init__(self, sph: Sph, alpha, beta, params: capi.RexiParams):
+        self.sph = sph
+        a = np.ascontiguousarray(np.asarray(alpha, np.complex128)).view(np.float64)
+        b = np.ascontiguousarray(np.asarray(beta, np.complex128)).view(np.float64)
+        dp = ctypes.POINTER(ctypes.c_double)
+        r = ctypes.c_void_p()
+        capi.check(capi.lib().sph_rexi_create(sph.h, a.ctypes.data_as(dp), b.ctypes.data_as(dp), len(a) // 2,
+                                              ctypes.byref(params), ctypes.byref(r)))
+        self.r = r
+        self.npoles = len(a) // 2
+
+    def step(self, state: torch.Tensor, nsteps: int = 1) -> torch.Tensor:
+        """In place on state (3, nlm) complex128 = [h, u, v] (Robert u cos(phi), v cos(phi))."""
+        capi.check(capi.lib().sph_rexi_step(self.r, _ptr(state), nsteps, _stream()))
+        return state
+
+    def close(self):
+        if getattr(self, "r", None):
+            capi.lib().sph_rexi_destroy(self.r)
+            self.r = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
