@@ -51,7 +51,8 @@ enum sph_status {
 /* precision forms (flags of sph_create) */
 enum sph_precision {
     SPH_PREC_FP64 = 0,     /* plain method: FP64 everywhere                      */
-    SPH_PREC_MIXED = 1     /* Legendre GEMMs on tcgen05 (split-bf16, FP32 acc.)  */
+    SPH_PREC_MIXED = 1     /* Legendre GEMMs on tcgen05 (split-TF32, FP32 chunk
+                              sums added in FP64); everything else FP64         */
 };
 
 typedef struct sph_handle sph_handle;
@@ -223,6 +224,11 @@ int sph_rexi_destroy(sph_rexi* r);
 int sph_rexi_step(sph_rexi* r, double* state, int nsteps, void* stream);
 
 /* ---------------------------------------------------------------- errors */
+
+/* Wait for the stream and report device-side failures of the handle's kernels
+ * (a bounded wait inside a tensor-core kernel that gave up: SPH_ERR_TIMEOUT).
+ * No counterpart in the reference, whose CPU path has no asynchronous errors. */
+int sph_sync(sph_handle* h, void* stream);
 
 /* Copy the message of the last error into buf (NUL terminated); returns its length. */
 int sph_last_error(char* buf, int n);

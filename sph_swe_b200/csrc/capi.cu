@@ -108,6 +108,10 @@ int sph_create(int lmax, int mmax, int nlat, int nphi, int flags, sph_handle** o
     int rc = fft_kernels_init();
     if (rc == SPH_OK) rc = fft_plan_init(&h->fft, nphi);
     if (rc == SPH_OK) rc = setup_tables(h);
+    if (rc == SPH_OK && (flags & SPH_PREC_MIXED)) {
+        rc = tc_kernels_init();
+        if (rc == SPH_OK) rc = tc_tables_build(h, lmax + 1);
+    }
     if (rc != SPH_OK) {
         sph_destroy(h);
         return rc;
@@ -120,6 +124,7 @@ int sph_destroy(sph_handle* h) {
     if (!h) return SPH_OK;
     cudaDeviceSynchronize();
     rk_free(h);
+    tc_tables_free(h);
     if (h->mu) cudaFree(h->mu);
     if (h->w) cudaFree(h->w);
     if (h->cosphi) cudaFree(h->cosphi);
@@ -154,6 +159,12 @@ int sph_grid(const sph_handle* h, double* mu, double* cosphi, double* w, double*
 
 #define CHECK_H(fn)                                                  \
     if (!h) { set_error(std::string(fn) + ": NULL handle"); return SPH_ERR_ARG; }
+
+int sph_sync(sph_handle* h, void* stream) {
+    CHECK_H("sph_sync");
+    SPH_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+    return tc_check(h);
+}
 
 int sph_spat_to_SH(sph_handle* h, const double* spat, double* spec, int batch, long long ld_spat, long long ld_spec,
                    void* stream) {

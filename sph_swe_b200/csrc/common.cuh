@@ -52,7 +52,7 @@ struct Handle {
     std::vector<long long> poff_h;
     long long* poff = nullptr;  // device copy, L+3 entries
     FFTPlan fft;
-    // mixed-precision Legendre tables (split bf16, built on demand)
+    // mixed-precision Legendre state (legendre_tc.cu): recurrence checkpoints, error flag
     void* mixed = nullptr;
     // RK4 buffers and captured step graph (swe.cu)
     void* rk = nullptr;
@@ -100,6 +100,16 @@ int legendre_synthesis_cplx(const Handle* h, const double2* spec, long long ld_s
                             int batch, cudaStream_t s);
 int legendre_analysis_cplx(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
                            int batch, cudaStream_t s);
+
+// Legendre stage of the mixed-precision form on tcgen05 (legendre_tc.cu), real layout only
+int tc_kernels_init();
+int tc_tables_build(Handle* h, int lmax);
+void tc_tables_free(Handle* h);
+int tc_check(const Handle* h);
+int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F, long long ldF,
+                          int batch, cudaStream_t s);
+int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec, int lmax,
+                         int batch, cudaStream_t s);
 
 // spectral operators (packed real or complex layout)
 int spec_op(const Handle* h, int op, const double2* in, long long ld_in, double2* out, long long ld_out, double2 a,

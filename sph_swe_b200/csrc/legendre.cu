@@ -198,12 +198,21 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
 
 int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
                             long long ldF, int batch, cudaStream_t s) {
+    if (h->flags & SPH_PREC_MIXED) return legendre_synthesis_tc(h, spec, ld_spec, lmax, F, ldF, batch, s);
     SpecMap sm{0, lmax, h->L, ld_spec};
     return launch_synth(h, spec, sm, F, ldF, batch, s);
 }
 
 int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
                            int lmax, int batch, cudaStream_t s) {
+    if (h->flags & SPH_PREC_MIXED) {
+        if (int rc = legendre_analysis_tc(h, F, ldF, spec, ld_spec, lmax, batch, s)) return rc;
+        if (lmax > h->L) {
+            k_zero_top<<<(batch + 127) / 128, 128, 0, s>>>(spec, ld_spec, lmax, batch);
+            SPH_CUDA_TRY(cudaGetLastError());
+        }
+        return SPH_OK;
+    }
     SpecMap sm{0, lmax, h->L, ld_spec};
     return launch_anal(h, F, ldF, spec, sm, batch, s);
 }

@@ -1,0 +1,115 @@
+"""Mixed-precision form (SPH_PREC_MIXED): Legendre stage on tcgen05 in
+split-TF32 with FP32 chunk sums folded into FP64, everything else FP64.
+
+Tolerances (relative L2 against the FP64 oracle / FP64 GPU path):
+  scalar synthesis and analysis           <= 1e-6  (measured 2e-7 .. 4e-7)
+  vector synthesis u, v                   <= 2e-6
+  vector round trip vort -> u,v -> vort   <= 5e-5  (the analysis of u, v divides
+      by l(l+1) and amplifies the split-TF32 error at high degree)
+  nonlinear RK4, T63, 200 steps: h <= 1e-6; u, v <= 5e-5 (measured 2e-5: the
+      tensor core accumulates in FP32, which bounds each transform near 2e-7,
+      and the 200-step map amplifies that by ~100 in the velocity, which
+      starts from rest)
+"""
+import numpy as np
+import pytest
+import torch
+
+from tests.helpers import ga_f, random_spec, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-6
+
+
+def _mixed(L):
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+
+    return Sph(L, precision=capi.SPH_PREC_MIXED)
+
+
+def _sync_ok(s):
+    from sph_swe_b200 import capi
+
+    assert capi.lib().sph_sync(s.h, None) == capi.SPH_OK, capi.last_error()
+
+
+# batch sizes exercise the 8-, 16- and 32-field column tiles and a ragged last tile
+@pytest.mark.parametrize("L,nb", [(31, 1), (31, 13), (63, 8), (63, 37), (127, 16), (127, 20), (255, 3), (255, 64)])
+def test_scalar_transforms_vs_oracle(gpu, oracle_mod, L, nb):
+    s = _mixed(L)
+    g = oracle_mod.Grid(L)
+    spec = random_spec(L, nb, seed=100 + L + nb)
+    ref = g.SH_to_spat(spec)
+    out = s.SH_to_spat(torch.from_numpy(spec).cuda()).cpu().numpy()
+    _sync_ok(s)
+    for b in range(nb):
+        assert rel_l2(out[b], ref[b]) < TOL
+    back = s.spat_to_SH(torch.from_numpy(ref).cuda()).cpu().numpy()
+    _sync_ok(s)
+    ana = g.spat_to_SH(ref)
+    for b in range(nb):
+        assert rel_l2(back[b], ana[b]) < TOL
+
+
+def test_analysis_of_non_bandlimited_field(gpu, oracle_mod):
+    s = _mixed(63)
+    g = oracle_mod.Grid(63)
+    f = g.grid_from(ga_f)
+    out = s.spat_to_SH(torch.from_numpy(f).cuda()).cpu().numpy()
+    _sync_ok(s)
+    assert rel_l2(out, g.spat_to_SH(f)) < TOL
+
+
+@pytest.mark.parametrize("L", [63, 255])
+def test_vector_pair_vs_fp64(gpu, L):
+    from sph_swe_b200.sph import Sph
+
+    s, s64 = _mixed(L), Sph(L)
+    vort = torch.from_numpy(random_spec(L, 2, seed=5)).cuda()
+    div = torch.from_numpy(random_spec(L, 2, seed=6)).cuda()
+    vort[:, 0] = 0
+    div[:, 0] = 0
+    for robert in (False, True):
+        u, v = s.vec_SH_to_spat(vort, div, robert=robert)
+        u64, v64 = s64.vec_SH_to_spat(vort, div, robert=robert)
+        assert rel_l2(u.cpu().numpy(), u64.cpu().numpy()) < 2e-6
+        assert rel_l2(v.cpu().numpy(), v64.cpu().numpy()) < 2e-6
+        z, d = s.vec_spat_to_SH(u, v, robert=robert)
+        assert rel_l2(z.cpu().numpy(), vort.cpu().numpy()) < 5e-5
+        assert rel_l2(d.cpu().numpy(), div.cpu().numpy()) < 5e-5
+    _sync_ok(s)
+
+
+def test_config0_rk4_vs_oracle(gpu, oracle_mod):
+    """Plain-method configuration (T63 96x192, nonlinear RK4, bump 500 m at
+    (30N, 60E), dt = 120 s, 200 steps) run in the mixed form: h, u, v within
+    the tolerances of the module docstring of the FP64 oracle."""
+    from tests.helpers import bump_state
+
+    L = 63
+    s = _mixed(L)
+    g = oracle_mod.Grid(L)
+    p = s.swe_params(radius=6.371e6, dt=120.0, nonlinear=1)
+    h = g.spat_to_SH(bump_state(g))
+    u = np.zeros(g.nlm, complex)
+    v = np.zeros(g.nlm, complex)
+    st = torch.from_numpy(np.stack([h, u, v])).cuda()
+    s.swe_rk4(p, st, 200)
+    _sync_ok(s)
+    out = st.cpu().numpy()
+    rh, ru, rv, rc = g.swe_run((p.radius, p.gravity, p.omega, p.h0, p.viscosity, p.dt), h, u, v, 200)
+    assert rc == 0
+    for q, (ref, tol) in enumerate(((rh, TOL), (ru, 5e-5), (rv, 5e-5))):
+        assert rel_l2(out[q], ref) < tol, q
+
+
+def test_reuse_and_sync_stay_clean(gpu):
+    s = _mixed(127)
+    x = torch.from_numpy(random_spec(127, 20, seed=7)).cuda()
+    first = s.SH_to_spat(x)
+    for _ in range(5):
+        again = s.SH_to_spat(x)
+    _sync_ok(s)
+    assert torch.equal(first, again)
