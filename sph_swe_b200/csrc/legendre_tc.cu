@@ -20,12 +20,13 @@
 // then added into an FP64 running sum kept in tensor memory, so FP32
 // rounding acts on short partial sums only.
 //
-// One persistent CTA of 16 warps per SM walks its tiles as one stream of
-// chunks.  Producers (warps 0-7) prefetch raw data NRAW-1 chunks ahead with
-// cp.async, regenerate P and stage B for a chunk into one of NSTAGE smem
-// stages; one producer thread issues the chunk's MMAs and commits them.
-// Consumers (warps 8-15) fold finished groups into the FP64 sums and write
-// finished tiles.  Producers and consumers are decoupled by mbarriers; all
+// One persistent CTA of 17 warps per SM walks its tiles as one stream of
+// chunks.  Producers (warps 0-11) prefetch a chunk's raw data NRAW-1 chunks
+// ahead with cp.async, then warps 0-7 regenerate P and warps 8-11 stage B
+// into one of NSTAGE smem stages; one thread of warp 16
+// issues each staged chunk's MMAs and commits them; consumers (warps 12-15)
+// fold finished groups into the FP64 sums and write finished tiles.  The
+// roles are decoupled by mbarriers; all
 // waits are bounded: on timeout the CTA raises an abort flag, waits (bounded)
 // for its last MMA, records the error in the handle's flag, frees its tensor
 // memory and returns.
@@ -41,7 +42,12 @@ namespace tc {
 constexpr int M = 128;            // tile rows (TMEM lanes)
 constexpr int KC = 16;            // K per chunk and parity (two MMA K-steps of 8)
 constexpr int SEG = 16;           // degrees per recurrence checkpoint
-constexpr int NT = 512;           // threads per CTA: 256 producers + 256 consumers
+constexpr int NGEN = 256;         // producer threads regenerating P (warps 0-7)
+constexpr int NBST = 128;         // producer threads staging B (warps 8-11)
+constexpr int NPROD = NGEN + NBST;
+constexpr int NCONS = 128;        // consumer threads (warps 12-15)
+constexpr int MMA_WARP = 16;
+constexpr int NT = 544;           // threads per CTA
 constexpr int ATILE = M * KC;     // floats per A part (8 KB)
 constexpr int NMAX = 64;          // max columns per CTA (32 complex fields)
 constexpr int BTILE = NMAX * KC;  // floats per B part (4 KB)
@@ -50,13 +56,27 @@ constexpr double BIG = 0x1p600, SMALL = 0x1p-600;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s limit of every wait
 }  // namespace tc
 
+// Recurrence coefficients of degree l (order m):
+//   P_l = a (mu P_{l-1} - b P_{l-2})                        (l >= m + 2)
+//   P_l = (alpha mu^2 + beta) P_{l-2} + gamma P_{l-4}       (l >= m + 4)
+// the second form is the first applied twice with P_{l-1}, P_{l-3} eliminated:
+//   alpha = a_l a_{l-1}, beta = -a_l (a_{l-1} b_{l-1} / a_{l-2} + b_l),
+//   gamma = -a_l a_{l-1} b_{l-1} b_{l-2}; it advances the even and the odd
+// degrees as two independent chains.
+struct TcCoef {
+    double2 ab;   // (a, b)
+    double2 ag;   // (alpha, beta)
+    double2 g;    // (gamma, 0)
+};
+
 struct MixedTables {
-    double2* ab = nullptr;        // recurrence coefficients (a_l, b_l) at ab[abo(m) + l - m], l >= m + 2
+    TcCoef* ab = nullptr;         // recurrence coefficients of (l, m) at ab[abo(m) + l - m]
     long long* abo = nullptr;     // [m]
-    double2* ck = nullptr;        // checkpoints (P_l, P_{l+1}), scaled, at ck[(cko(m) + c) * nh + j], l = m + SEG c
+    double2* ck = nullptr;        // checkpoints (P_l, P_{l+1}), scaled, at ck[(cko(m) + c) * nhp + j], l = m + SEG c
     int* ckx = nullptr;           // binary exponent of each checkpoint's scale (0, -600, ...)
     long long* cko = nullptr;     // [m]
     int lmax = 0;
+    int nhp = 0;                  // checkpoint row stride: nh rounded up to a multiple of 4 (16 B rows of ints)
     int* flag = nullptr;          // device error flag (bit 0: a wait gave up)
 };
 
@@ -254,16 +274,27 @@ __device__ __forceinline__ double plm_value(double p, int el) {
 }
 
 // thread per (l, m): recurrence coefficients
-__global__ void k_tc_ab(int lmax, int mm, double2* __restrict__ ab) {
+__global__ void k_tc_ab(int lmax, int mm, TcCoef* __restrict__ ab) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (m > mm || l < m || l > lmax) return;
-    ab[tc_abo(lmax, m) + (l - m)] = l >= m + 2 ? make_double2(plm_a(l, m), plm_b(l, m)) : make_double2(0.0, 0.0);
+    TcCoef c;
+    c.ab = l >= m + 2 ? make_double2(plm_a(l, m), plm_b(l, m)) : make_double2(0.0, 0.0);
+    c.ag = make_double2(0.0, 0.0);
+    c.g = make_double2(0.0, 0.0);
+    if (l >= m + 4) {
+        const double a0 = plm_a(l, m), b0 = plm_b(l, m);
+        const double a1 = plm_a(l - 1, m), b1 = plm_b(l - 1, m);
+        const double a2 = plm_a(l - 2, m), b2 = plm_b(l - 2, m);
+        c.ag = make_double2(a0 * a1, -a0 * (a1 * b1 / a2 + b0));
+        c.g = make_double2(-a0 * a1 * b1 * b2, 0.0);
+    }
+    ab[tc_abo(lmax, m) + (l - m)] = c;
 }
 
 // thread per (j, m): runs the recurrence over all degrees and stores a checkpoint every SEG degrees
-__global__ void k_tc_ck(int nh, int lmax, int mm, const double* __restrict__ x, const double2* __restrict__ ab,
-                        double2* __restrict__ ck, int* __restrict__ ckx) {
+__global__ void k_tc_ck(int nh, int nhp, int lmax, int mm, const double* __restrict__ x,
+                        const TcCoef* __restrict__ ab, double2* __restrict__ ck, int* __restrict__ ckx) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (j >= nh || m > mm) return;
@@ -280,24 +311,24 @@ __global__ void k_tc_ck(int nh, int lmax, int mm, const double* __restrict__ x, 
     }
     double p0 = pmm;
     double p1 = m + 1 <= lmax ? z * sqrt(2.0 * m + 3.0) * p0 : 0.0;
-    double2* ckm = ck + tc_cko(lmax, m) * nh + j;
-    int* ckxm = ckx + tc_cko(lmax, m) * nh + j;
+    double2* ckm = ck + tc_cko(lmax, m) * nhp + j;
+    int* ckxm = ckx + tc_cko(lmax, m) * nhp + j;
     ckm[0] = make_double2(p0, p1);
     ckxm[0] = el;
-    const double2* abm = ab + tc_abo(lmax, m);
+    const TcCoef* abm = ab + tc_abo(lmax, m);
     for (int l = m + 2; l <= lmax; l++) {
-        plm_step(z, abm[l - m], p0, p1, el);  // state (P_{l-1}, P_l)
+        plm_step(z, abm[l - m].ab, p0, p1, el);  // state (P_{l-1}, P_l)
         const int d = l - 1 - m;
         if (d % tc::SEG == 0) {
-            ckm[(size_t)(d / tc::SEG) * nh] = make_double2(p0, p1);
-            ckxm[(size_t)(d / tc::SEG) * nh] = el;
+            ckm[(size_t)(d / tc::SEG) * nhp] = make_double2(p0, p1);
+            ckxm[(size_t)(d / tc::SEG) * nhp] = el;
         }
     }
     // a checkpoint at l = lmax itself has no successor inside the range
     const int d = lmax - m;
     if (d > 0 && d % tc::SEG == 0) {
-        ckm[(size_t)(d / tc::SEG) * nh] = make_double2(p1, 0.0);
-        ckxm[(size_t)(d / tc::SEG) * nh] = el;
+        ckm[(size_t)(d / tc::SEG) * nhp] = make_double2(p1, 0.0);
+        ckxm[(size_t)(d / tc::SEG) * nhp] = el;
     }
 }
 
@@ -309,14 +340,16 @@ int tc_tables_build(Handle* h, int lmax) {
     T->lmax = lmax;
     const int mm = std::min(lmax, h->L);
     const long long na = tc_abo(lmax, mm + 1), nc = tc_cko(lmax, mm + 1);
-    SPH_CUDA_TRY(cudaMalloc(&T->ab, sizeof(double2) * na));
-    SPH_CUDA_TRY(cudaMalloc(&T->ck, sizeof(double2) * nc * nh));
-    SPH_CUDA_TRY(cudaMalloc(&T->ckx, sizeof(int) * nc * nh));
+    SPH_CUDA_TRY(cudaMalloc(&T->ab, sizeof(TcCoef) * na));
+    T->nhp = (nh + 3) & ~3;
+    SPH_CUDA_TRY(cudaMalloc(&T->ck, sizeof(double2) * nc * T->nhp));
+    SPH_CUDA_TRY(cudaMalloc(&T->ckx, sizeof(int) * nc * T->nhp));
+    SPH_CUDA_TRY(cudaMemset(T->ckx, 0, sizeof(int) * nc * T->nhp));
     SPH_CUDA_TRY(cudaMalloc(&T->flag, sizeof(int)));
     SPH_CUDA_TRY(cudaMemset(T->flag, 0, sizeof(int)));
     k_tc_ab<<<dim3((lmax + 128) / 128, mm + 1), 128>>>(lmax, mm, T->ab);
     SPH_CUDA_TRY(cudaGetLastError());
-    k_tc_ck<<<dim3((nh + 127) / 128, mm + 1), 128>>>(nh, lmax, mm, h->mu, T->ab, T->ck, T->ckx);
+    k_tc_ck<<<dim3((nh + 127) / 128, mm + 1), 128>>>(nh, T->nhp, lmax, mm, h->mu, T->ab, T->ck, T->ckx);
     SPH_CUDA_TRY(cudaGetLastError());
     SPH_CUDA_TRY(cudaDeviceSynchronize());
     return SPH_OK;
@@ -334,14 +367,14 @@ void tc_tables_free(Handle* h) {
 
 // ------------------------------------------------------------------ kernels
 struct TcArgs {
-    const double2* ab;
+    const TcCoef* ab;
     const double2* ck;
     const int* ckx;
     const double* mu;
     const double* w;
     int tlmax;      // degree of the coefficient / checkpoint tables
     int lmax;       // degree of this call's packed layout (<= tlmax)
-    int nh, nlat;
+    int nh, nhp, nlat;
     int batch;      // fields
     int nct, nrt;   // column tiles, row tiles (latitude tiles or degree tiles)
     int ntiles;     // nct * nrt * (number of m)
@@ -352,24 +385,32 @@ struct TcArgs {
 };
 
 // Shared-memory map: NSTAGE operand stages, NRAW raw prefetch buffers (the
-// producers prefetch NRAW-1 chunks ahead), barriers.  A raw buffer holds the
-// generators' checkpoints, mu and scale exponents, the recurrence
-// coefficients of the chunk's degrees, and the B-operand data.
+// producers prefetch NRAW-1 chunks ahead with cp.async), barriers.  A raw
+// buffer holds the generators' checkpoints, mu and scale exponents, the
+// recurrence coefficients of the chunk's degrees (segment h at row 17 h), and
+// the B-operand data.
 namespace tcs {
 constexpr int NSTAGE = 2;
-constexpr int NRAW = 4;
+constexpr int NRAW = 3;
 constexpr int STAGE_B = 4 * tc::STAGE_F;                  // 48 KB
 constexpr int R_CK = 0;                                   // double2[256]
 constexpr int R_MU = R_CK + 256 * 16;                     // double[256]
 constexpr int R_EX = R_MU + 256 * 8;                      // int[256]
-constexpr int R_AB = R_EX + 256 * 4;                      // double2[16][17] (segment stride 17)
-constexpr int R_B = R_AB + 16 * 17 * 16;                  // double2[32][NF + 4], then double[16]
-constexpr int RAW_B = R_B + 32 * (32 + 4) * 16 + 16 * 8;  // 29.4 KB
+constexpr int R_AB = R_EX + 256 * 4;                      // TcCoef[16][17]
+constexpr int R_B = R_AB + 16 * 17 * 48;                  // double2[32][NF + 4], then double[16]
+constexpr int RAW_B = R_B + 32 * (32 + 4) * 16 + 16 * 8;  // 38 KB
 constexpr int OFF_RAW = NSTAGE * STAGE_B;
 constexpr int OFF_BAR = OFF_RAW + NRAW * RAW_B;
 constexpr int BYTES = OFF_BAR + 256;
 }  // namespace tcs
 constexpr size_t tc_smem_bytes() { return (size_t)tcs::BYTES; }
+
+// position of a chunk in the CTA's sequence of tiles
+struct TcPos {
+    int t;    // tile index (>= ntiles: none)
+    int m, rt, ct;
+    int kc, nk;
+};
 
 __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes, bool valid) {
     const uint32_t d = smem_u32(dst);
@@ -389,55 +430,60 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 __device__ __forceinline__ bool producers_and(bool v) {
     uint32_t r;
     asm volatile(
-        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, 1, 256, p;\n\t"
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, 1, 384, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}\n"
         : "=r"(r)
         : "r"((uint32_t)v)
         : "memory");
     return r != 0;
 }
-__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, 384;" ::: "memory"); }
 
 // raw prefetch slots of one buffer
 struct Raw {
     double2* ck;
     double* mu;
     int* ex;
-    double2* ab;
+    TcCoef* ab;
     double2* b;  // [32][NF + 4]: spectral (parity 16 + k) or Fourier (hemisphere 16 + k) rows
 };
 __device__ __forceinline__ Raw raw_buf(unsigned char* smem, int buf) {
     unsigned char* p = smem + tcs::OFF_RAW + buf * tcs::RAW_B;
     return Raw{reinterpret_cast<double2*>(p + tcs::R_CK), reinterpret_cast<double*>(p + tcs::R_MU),
-               reinterpret_cast<int*>(p + tcs::R_EX), reinterpret_cast<double2*>(p + tcs::R_AB),
+               reinterpret_cast<int*>(p + tcs::R_EX), reinterpret_cast<TcCoef*>(p + tcs::R_AB),
                reinterpret_cast<double2*>(p + tcs::R_B)};
 }
 
 // The SEG values P_l(mu), l = l0 .. l0+SEG-1 (zero above lmax), from the
 // checkpoint at l0 and the coefficients abl[t] of degree l0 + t (shared
 // memory), handed to emit(t, hi, lo) with t = l - l0 a compile-time constant.
-// Unscaled full segments (the common case) take a branch-free path.
+// Unscaled full segments (the common case) take the branch-free path: two
+// ordinary steps, then the even and odd degrees as two independent chains of
+// the mu^2 form, one dependent FMA per step.
 template <typename Emit>
-__device__ __forceinline__ void plm_segment(double z, double2 c, int el, const double2* abl, int l0, int lmax,
+__device__ __forceinline__ void plm_segment(double z, double2 c, int el, const TcCoef* abl, int l0, int lmax,
                                             Emit&& emit) {
-    double p0 = c.x, p1 = c.y;
     float hi, lo;
     if (el == 0 && l0 + tc::SEG - 1 <= lmax) {
-        split_tf32(p0, hi, lo);
-        emit(0, hi, lo);
-        split_tf32(p1, hi, lo);
-        emit(1, hi, lo);
+        double v[tc::SEG];
+        v[0] = c.x;
+        v[1] = c.y;
+        v[2] = abl[2].ab.x * (z * v[1] - abl[2].ab.y * v[0]);
+        v[3] = abl[3].ab.x * (z * v[2] - abl[3].ab.y * v[1]);
+        const double z2 = z * z;
 #pragma unroll
-        for (int t = 2; t < tc::SEG; t++) {
-            const double2 ab = abl[t];
-            const double p2 = ab.x * (z * p1 - ab.y * p0);
-            p0 = p1;
-            p1 = p2;
-            split_tf32(p2, hi, lo);
+        for (int t = 4; t < tc::SEG; t++) {
+            const double2 ag = abl[t].ag;
+            v[t] = fma(fma(ag.x, z2, ag.y), v[t - 2], abl[t].g.x * v[t - 4]);
+        }
+#pragma unroll
+        for (int t = 0; t < tc::SEG; t++) {
+            split_tf32(v[t], hi, lo);
             emit(t, hi, lo);
         }
         return;
     }
+    double p0 = c.x, p1 = c.y;
     split_tf32(l0 <= lmax ? plm_value(p0, el) : 0.0, hi, lo);
     emit(0, hi, lo);
     split_tf32(l0 + 1 <= lmax ? plm_value(p1, el) : 0.0, hi, lo);
@@ -447,7 +493,7 @@ __device__ __forceinline__ void plm_segment(double z, double2 c, int el, const d
         const int l = l0 + t;
         double v = 0.0;
         if (l <= lmax) {
-            plm_step(z, abl[t], p0, p1, el);
+            plm_step(z, abl[t].ab, p0, p1, el);
             v = plm_value(p1, el);
         }
         split_tf32(v, hi, lo);
@@ -457,21 +503,25 @@ __device__ __forceinline__ void plm_segment(double z, double2 c, int el, const d
 
 // Issue the split-TF32 products of one staged chunk for both parities (one
 // thread) into the accumulator buffer (E at column 0, O at NC); the first
-// product starts from zero unless `acc`.
+// product starts from zero unless `acc`.  Descriptors differ only in their
+// start-address field, so each is the stage's base descriptor plus a
+// compile-time offset (in 16 B units).
 template <int NC>
 __device__ __forceinline__ void tc_issue_chunk(const float* As, const float* Bs, uint32_t tacc, bool acc) {
     constexpr uint32_t idesc = idesc_tf32(tc::M, NC);
+    const uint64_t dA = sdesc(smem_u32(As)), dB = sdesc(smem_u32(Bs));
 #pragma unroll
-    for (int par = 0; par < 2; par++) {
-        const uint32_t ah = smem_u32(As + par * 2 * tc::ATILE), al = ah + tc::ATILE * 4;
-        const uint32_t bh = smem_u32(Bs + par * 2 * tc::BTILE), bl = bh + tc::BTILE * 4;
-        const uint32_t d = tacc + par * NC;
+    for (int s = 0; s < tc::KC / 8; s++) {
 #pragma unroll
-        for (int s = 0; s < tc::KC / 8; s++) {
-            const uint32_t ao = s * tc::M * 32, bo = s * NC * 32;
-            mma_tf32(d, sdesc(ah + ao), sdesc(bh + bo), idesc, (s > 0 || acc) ? 1u : 0u);
-            mma_tf32(d, sdesc(ah + ao), sdesc(bl + bo), idesc, 1u);
-            mma_tf32(d, sdesc(al + ao), sdesc(bh + bo), idesc, 1u);
+        for (int par = 0; par < 2; par++) {
+            const uint64_t ah = dA + (uint64_t)((par * 2 * tc::ATILE * 4 + s * tc::M * 32) >> 4);
+            const uint64_t al = ah + (uint64_t)((tc::ATILE * 4) >> 4);
+            const uint64_t bh = dB + (uint64_t)((par * 2 * tc::BTILE * 4 + s * NC * 32) >> 4);
+            const uint64_t bl = bh + (uint64_t)((tc::BTILE * 4) >> 4);
+            const uint32_t d = tacc + par * NC;
+            mma_tf32(d, ah, bh, idesc, (s > 0 || acc) ? 1u : 0u);
+            mma_tf32(d, ah, bl, idesc, 1u);
+            mma_tf32(d, al, bh, idesc, 1u);
         }
     }
 }
@@ -487,27 +537,21 @@ struct TcCfg {
     static constexpr uint32_t NCOLS = USED <= 32 ? 32u : USED <= 64 ? 64u : USED <= 128 ? 128u : USED <= 256 ? 256u : 512u;
 };
 
-// position of a chunk in the CTA's sequence of tiles
-struct TcPos {
-    int t;    // tile index (>= ntiles: none)
-    int m, rt, ct;
-    int kc, nk;
-};
 
 // B-operand item decomposition: lanes cover (re/im, k & 3, f & 3) so that the
 // scalar stores into the K-major tile hit 32 distinct banks.  k depends on the
-// thread only (idx = tid + 256 it).
+// B thread only (idx = bt + 128 it).
 __device__ __forceinline__ int item_ri(int idx) { return idx & 1; }
 __device__ __forceinline__ int item_k(int idx) { return ((idx >> 1) & 3) | (((idx >> 5) & 3) << 2); }
 
 // Synthesis: tile = (column tile, latitude tile of 128, m); chunk k = degrees
-// l = m + 32k .. m + 32k + 31 (16 per parity = K of the chunk).  Producer
-// thread t: P row t & 127, half h = t >> 7 (degrees 16h .. 16h+15), and
-// NC/8 coefficient items.
+// l = m + 32k .. m + 32k + 31 (16 per parity = K of the chunk).  Generator
+// thread t < 256: P row t & 127, half h = t >> 7 (degrees 16h .. 16h+15);
+// B thread bt = t - 256: NC/4 coefficient items.
 template <int NC>
 struct SynDir {
     static constexpr int NF = NC / 2;
-    static constexpr int BIT = NC * 2 * tc::KC / 256;  // B items per producer
+    static constexpr int BIT = NC * 2 * tc::KC / tc::NBST;  // B items per B thread
     __device__ static int nchunks(const TcArgs& a, int m, int) { return (a.lmax - m) / (2 * tc::KC) + 1; }
     __device__ static int item_f(int idx) { return ((idx >> 3) & 3) | ((idx >> 7) % (NF / 4)) * 4; }
     __device__ static int item_par(int idx) { return (idx >> 7) / (NF / 4); }
@@ -517,30 +561,37 @@ struct SynDir {
         const int tid = threadIdx.x;
         const int l0 = p.m + 2 * tc::KC * p.kc;
         const Raw r = raw_buf(smem, buf);
+        if (tid >= tc::NGEN) {
+            // coefficients (f, l0 + d), d = 0..31: consecutive threads read consecutive degrees
+            const int bt = tid - tc::NGEN;
+#pragma unroll
+            for (int it = 0; it < NF * 32 / tc::NBST; it++) {
+                const int idx = bt + tc::NBST * it;
+                const int d = idx & 31, fl = idx >> 5;
+                const int l = l0 + d, f = p.ct * NF + fl;
+                const bool v = l <= a.lmax && f < a.batch;
+                cp_async(&r.b[((d & 1) * 16 + (d >> 1)) * (NF + 4) + fl],
+                         v ? (const void*)(spec + (long long)f * a.ld_spec + pidx(a.lmax, l, p.m)) : (const void*)spec,
+                         16, v);
+            }
+            return;
+        }
         {
             const int gr = tid & (tc::M - 1), gh = tid >> 7;
             const int gj = p.rt * tc::M + gr;
             const bool v = gj < a.nh && l0 + tc::SEG * gh <= a.lmax;
-            const long long ci = (tc_cko(a.tlmax, p.m) + 2 * p.kc + gh) * (long long)a.nh + gj;
+            const long long ci = (tc_cko(a.tlmax, p.m) + 2 * p.kc + gh) * (long long)a.nhp + gj;
             cp_async(&r.ck[tid], v ? (const void*)(a.ck + ci) : (const void*)a.ck, 16, v);
             cp_async(&r.ex[tid], v ? (const void*)(a.ckx + ci) : (const void*)a.ckx, 4, v);
             cp_async(&r.mu[tid], v ? (const void*)(a.mu + gj) : (const void*)a.mu, 8, v);
         }
-        if (tid < 2 * tc::KC) {  // coefficients of degrees l0 .. l0+31 (segment h at 17 h)
-            const int l = l0 + tid;
+        if (tid < 3 * 2 * tc::KC) {  // coefficients of degrees l0 .. l0+31 (segment h at 17 h), 3 x 16 B each
+            const int e = tid / 3, part = tid % 3;
+            const int l = l0 + e;
             const bool v = l <= a.lmax;
-            cp_async(&r.ab[(tid >> 4) * 17 + (tid & 15)],
-                     v ? (const void*)(a.ab + tc_abo(a.tlmax, p.m) + (l - p.m)) : (const void*)a.ab, 16, v);
-        }
-        // coefficients (f, l0 + d), d = 0..31: consecutive threads read consecutive degrees
-#pragma unroll
-        for (int it = 0; it < NF * 32 / 256; it++) {
-            const int idx = tid + 256 * it;
-            const int d = idx & 31, fl = idx >> 5;
-            const int l = l0 + d, f = p.ct * NF + fl;
-            const bool v = l <= a.lmax && f < a.batch;
-            cp_async(&r.b[((d & 1) * 16 + (d >> 1)) * (NF + 4) + fl],
-                     v ? (const void*)(spec + (long long)f * a.ld_spec + pidx(a.lmax, l, p.m)) : (const void*)spec, 16, v);
+            const double2* src = reinterpret_cast<const double2*>(a.ab + tc_abo(a.tlmax, p.m) + (l - p.m)) + part;
+            cp_async(reinterpret_cast<double2*>(&r.ab[(e >> 4) * 17 + (e & 15)]) + part,
+                     v ? (const void*)src : (const void*)a.ab, 16, v);
         }
     }
 
@@ -548,41 +599,43 @@ struct SynDir {
         const int tid = threadIdx.x;
         const int l0 = p.m + 2 * tc::KC * p.kc;
         const Raw r = raw_buf(smem, buf);
-        {
-            const int gr = tid & (tc::M - 1), gh = tid >> 7;
-            const int gj = p.rt * tc::M + gr;
-            float h[8], g[8];
-            auto emit = [&](int t, float hi, float lo) {
-                h[t & 7] = hi;
-                g[t & 7] = lo;
-                if ((t & 7) == 7) {
-                    const int k0 = 8 * gh + (t >> 3) * 4;
+        if (tid >= tc::NGEN) {
+            const int bt = tid - tc::NGEN;
 #pragma unroll
-                    for (int par = 0; par < 2; par++) {
-                        float* ap = As + par * 2 * tc::ATILE + tile_off(gr, k0, tc::M);
-                        *reinterpret_cast<float4*>(ap) = make_float4(h[par], h[par + 2], h[par + 4], h[par + 6]);
-                        *reinterpret_cast<float4*>(ap + tc::ATILE) =
-                            make_float4(g[par], g[par + 2], g[par + 4], g[par + 6]);
-                    }
-                }
-            };
-            const int lseg = l0 + tc::SEG * gh;
-            if (gj < a.nh && lseg <= a.lmax) {
-                plm_segment(r.mu[tid], r.ck[tid], r.ex[tid], r.ab + 17 * gh, lseg, a.lmax, emit);
-            } else {
-#pragma unroll
-                for (int t = 0; t < tc::SEG; t++) emit(t, 0.f, 0.f);
+            for (int it = 0; it < BIT; it++) {
+                const int idx = bt + tc::NBST * it;
+                const double2 q = r.b[(item_par(idx) * 16 + item_k(idx)) * (NF + 4) + item_f(idx)];
+                float hi, lo;
+                split_tf32(item_ri(idx) ? q.y : q.x, hi, lo);
+                float* bp =
+                    Bs + item_par(idx) * 2 * tc::BTILE + tile_off(2 * item_f(idx) + item_ri(idx), item_k(idx), NC);
+                bp[0] = hi;
+                bp[tc::BTILE] = lo;
             }
+            return;
         }
+        const int gr = tid & (tc::M - 1), gh = tid >> 7;
+        const int gj = p.rt * tc::M + gr;
+        float h[8], g[8];
+        auto emit = [&](int t, float hi, float lo) {
+            h[t & 7] = hi;
+            g[t & 7] = lo;
+            if ((t & 7) == 7) {
+                const int k0 = 8 * gh + (t >> 3) * 4;
 #pragma unroll
-        for (int it = 0; it < BIT; it++) {
-            const int idx = tid + 256 * it;
-            const double2 q = r.b[(item_par(idx) * 16 + item_k(idx)) * (NF + 4) + item_f(idx)];
-            float hi, lo;
-            split_tf32(item_ri(idx) ? q.y : q.x, hi, lo);
-            float* bp = Bs + item_par(idx) * 2 * tc::BTILE + tile_off(2 * item_f(idx) + item_ri(idx), item_k(idx), NC);
-            bp[0] = hi;
-            bp[tc::BTILE] = lo;
+                for (int par = 0; par < 2; par++) {
+                    float* ap = As + par * 2 * tc::ATILE + tile_off(gr, k0, tc::M);
+                    *reinterpret_cast<float4*>(ap) = make_float4(h[par], h[par + 2], h[par + 4], h[par + 6]);
+                    *reinterpret_cast<float4*>(ap + tc::ATILE) = make_float4(g[par], g[par + 2], g[par + 4], g[par + 6]);
+                }
+            }
+        };
+        const int lseg = l0 + tc::SEG * gh;
+        if (gj < a.nh && lseg <= a.lmax) {
+            plm_segment(r.mu[tid], r.ck[tid], r.ex[tid], r.ab + 17 * gh, lseg, a.lmax, emit);
+        } else {
+#pragma unroll
+            for (int t = 0; t < tc::SEG; t++) emit(t, 0.f, 0.f);
         }
     }
 
@@ -605,14 +658,14 @@ struct SynDir {
 };
 
 // Analysis: tile = (column tile, degree tile of 256 = 128 rows per parity, m);
-// chunk k = latitudes j = 16k .. 16k+15.  Producer thread (s, jj), s, jj = 0..15,
+// chunk k = latitudes j = 16k .. 16k+15.  Generator thread (s, jj), s, jj = 0..15,
 // regenerates degrees l = lbase + 16 s + t at latitude 16k + jj; the i-th degree
 // of parity p of segment s sits in row 8 s + ((i + s) & 7), a rotation that keeps
 // the scalar shared-memory stores free of bank conflicts.
 template <int NC>
 struct AnaDir {
     static constexpr int NF = NC / 2;
-    static constexpr int BIT = NC * tc::KC / 256;  // B items per producer
+    static constexpr int BIT = NC * tc::KC / tc::NBST;  // B items per B thread
     __device__ static int nchunks(const TcArgs& a, int m, int rt) {
         return m + 2 * tc::M * rt > a.lmax ? 0 : (a.nh + tc::KC - 1) / tc::KC;
     }
@@ -625,74 +678,84 @@ struct AnaDir {
         const int tid = threadIdx.x;
         const int lbase = p.m + 2 * tc::M * p.rt;
         const Raw r = raw_buf(smem, buf);
+        if (tid >= tc::NGEN) {
+            // Fourier data (f, hemisphere, j0 + k): consecutive threads read consecutive latitudes
+            const int bt = tid - tc::NGEN;
+            const int j0 = p.kc * tc::KC;
+#pragma unroll
+            for (int it = 0; it < NF * 32 / tc::NBST; it++) {
+                const int idx = bt + tc::NBST * it;
+                const int k = idx & 15, hs = (idx >> 4) & 1, fl = idx >> 5;
+                const int j = j0 + k, f = p.ct * NF + fl;
+                const bool v = j < a.nh && f < a.batch;
+                const double2* src = F + (long long)f * a.ldF + (long long)p.m * a.nlat + (hs ? a.nlat - 1 - j : j);
+                cp_async(&r.b[(hs * 16 + k) * (NF + 4) + fl], v ? (const void*)src : (const void*)F, 16, v);
+            }
+            if (bt < tc::KC) {
+                double* wr = reinterpret_cast<double*>(r.b + 32 * (NF + 4));
+                cp_async(&wr[bt], j0 + bt < a.nh ? (const void*)(a.w + j0 + bt) : (const void*)a.w, 8, j0 + bt < a.nh);
+            }
+            return;
+        }
         {
             const int s = gs();
             const int j = p.kc * tc::KC + gjj();
             const bool v = j < a.nh && lbase + tc::SEG * s <= a.lmax;
-            const long long ci = (tc_cko(a.tlmax, p.m) + (2 * tc::M / tc::SEG) * p.rt + s) * (long long)a.nh + j;
+            const long long ci = (tc_cko(a.tlmax, p.m) + (2 * tc::M / tc::SEG) * p.rt + s) * (long long)a.nhp + j;
             cp_async(&r.ck[tid], v ? (const void*)(a.ck + ci) : (const void*)a.ck, 16, v);
             cp_async(&r.ex[tid], v ? (const void*)(a.ckx + ci) : (const void*)a.ckx, 4, v);
             cp_async(&r.mu[tid], v ? (const void*)(a.mu + j) : (const void*)a.mu, 8, v);
         }
-        {  // coefficients of the tile's 256 degrees, segment s at 17 s
-            const int l = lbase + tid;
-            const bool v = l <= a.lmax;
-            cp_async(&r.ab[(tid >> 4) * 17 + (tid & 15)],
-                     v ? (const void*)(a.ab + tc_abo(a.tlmax, p.m) + (l - p.m)) : (const void*)a.ab, 16, v);
-        }
-        // Fourier data (f, hemisphere, j0 + k): consecutive threads read consecutive latitudes
-        const int j0 = p.kc * tc::KC;
 #pragma unroll
-        for (int it = 0; it < NF * 32 / 256; it++) {
-            const int idx = tid + 256 * it;
-            const int k = idx & 15, hs = (idx >> 4) & 1, fl = idx >> 5;
-            const int j = j0 + k, f = p.ct * NF + fl;
-            const bool v = j < a.nh && f < a.batch;
-            const double2* src = F + (long long)f * a.ldF + (long long)p.m * a.nlat + (hs ? a.nlat - 1 - j : j);
-            cp_async(&r.b[(hs * 16 + k) * (NF + 4) + fl], v ? (const void*)src : (const void*)F, 16, v);
-        }
-        if (tid < tc::KC) {
-            double* wr = reinterpret_cast<double*>(r.b + 32 * (NF + 4));
-            cp_async(&wr[tid], j0 + tid < a.nh ? (const void*)(a.w + j0 + tid) : (const void*)a.w, 8, j0 + tid < a.nh);
+        for (int it = 0; it < 3; it++) {  // coefficients of the tile's 256 degrees, segment s at 17 s, 3 x 16 B each
+            const int idx = tid + tc::NGEN * it;
+            const int e = idx / 3, part = idx % 3;
+            const int l = lbase + e;
+            const bool v = l <= a.lmax;
+            const double2* src = reinterpret_cast<const double2*>(a.ab + tc_abo(a.tlmax, p.m) + (l - p.m)) + part;
+            cp_async(reinterpret_cast<double2*>(&r.ab[(e >> 4) * 17 + (e & 15)]) + part,
+                     v ? (const void*)src : (const void*)a.ab, 16, v);
         }
     }
 
     __device__ static void fill(const TcArgs& a, const TcPos& p, float* As, float* Bs, unsigned char* smem, int buf) {
         const int tid = threadIdx.x;
         const Raw r = raw_buf(smem, buf);
-        {
-            const int s = gs(), jj = gjj();
-            const int j = p.kc * tc::KC + jj;
-            const int l0 = p.m + 2 * tc::M * p.rt + tc::SEG * s;
-            auto emit = [&](int t, float hi, float lo) {
-                const int par = t & 1, i = t >> 1;
-                float* ap = As + par * 2 * tc::ATILE + tile_off(8 * s + ((i + s) & 7), jj, tc::M);
-                ap[0] = hi;
-                ap[tc::ATILE] = lo;
-            };
-            if (j < a.nh && l0 <= a.lmax) {
-                plm_segment(r.mu[tid], r.ck[tid], r.ex[tid], r.ab + 17 * s, l0, a.lmax, emit);
-            } else {
+        if (tid >= tc::NGEN) {
+            // G_S = w (F_j + F_mirror) (even parity), G_A = w (F_j - F_mirror) (odd), K = latitude
+            const int bt = tid - tc::NGEN;
+            const int k = item_k(bt), ri = item_ri(bt);
+            const double wj = reinterpret_cast<const double*>(r.b + 32 * (NF + 4))[k];
 #pragma unroll
-                for (int t = 0; t < tc::SEG; t++) emit(t, 0.f, 0.f);
+            for (int it = 0; it < BIT; it++) {
+                const int idx = bt + tc::NBST * it;
+                const double2 qn = r.b[k * (NF + 4) + item_f(idx)], qs = r.b[(16 + k) * (NF + 4) + item_f(idx)];
+                const double n = ri ? qn.y : qn.x, sv = ri ? qs.y : qs.x;
+                float hi, lo;
+                const int o = tile_off(2 * item_f(idx) + ri, k, NC);
+                split_tf32(wj * (n + sv), hi, lo);
+                Bs[o] = hi;
+                Bs[tc::BTILE + o] = lo;
+                split_tf32(wj * (n - sv), hi, lo);
+                Bs[2 * tc::BTILE + o] = hi;
+                Bs[3 * tc::BTILE + o] = lo;
             }
+            return;
         }
-        // G_S = w (F_j + F_mirror) (even parity), G_A = w (F_j - F_mirror) (odd), K = latitude
-        const int k = item_k(tid), ri = item_ri(tid);
-        const double wj = reinterpret_cast<const double*>(r.b + 32 * (NF + 4))[k];
+        const int s = gs(), jj = gjj();
+        const int j = p.kc * tc::KC + jj;
+        const int l0 = p.m + 2 * tc::M * p.rt + tc::SEG * s;
+        auto emit = [&](int t, float hi, float lo) {
+            const int par = t & 1, i = t >> 1;
+            float* ap = As + par * 2 * tc::ATILE + tile_off(8 * s + ((i + s) & 7), jj, tc::M);
+            ap[0] = hi;
+            ap[tc::ATILE] = lo;
+        };
+        if (j < a.nh && l0 <= a.lmax) {
+            plm_segment(r.mu[tid], r.ck[tid], r.ex[tid], r.ab + 17 * s, l0, a.lmax, emit);
+        } else {
 #pragma unroll
-        for (int it = 0; it < BIT; it++) {
-            const int idx = tid + 256 * it;
-            const double2 qn = r.b[k * (NF + 4) + item_f(idx)], qs = r.b[(16 + k) * (NF + 4) + item_f(idx)];
-            const double n = ri ? qn.y : qn.x, s = ri ? qs.y : qs.x;
-            float hi, lo;
-            const int o = tile_off(2 * item_f(idx) + ri, k, NC);
-            split_tf32(wj * (n + s), hi, lo);
-            Bs[o] = hi;
-            Bs[tc::BTILE + o] = lo;
-            split_tf32(wj * (n - s), hi, lo);
-            Bs[2 * tc::BTILE + o] = hi;
-            Bs[3 * tc::BTILE + o] = lo;
+            for (int t = 0; t < tc::SEG; t++) emit(t, 0.f, 0.f);
         }
     }
 
@@ -716,16 +779,16 @@ struct AnaDir {
     }
 };
 
-// Consumer warp cw (0..7): TMEM lanes 32 (cw & 3) .. +31, columns [h NC/2, (h+1) NC/2)
-// of E and of O with h = cw >> 2, in pieces of 8.  The group's FP32 partial sums
+// Consumer warp cw (0..3): TMEM lanes 32 cw .. +31, all NC columns of E and of O,
+// in pieces of 8.  The group's FP32 partial sums
 // are added to the FP64 running sums kept in TMEM; the tile's first group starts
 // them, its last group hands the totals to the epilogue instead of storing them.
 template <class Dir, int NC>
 __device__ __forceinline__ void tc_consume(const TcArgs& a, const TcPos& p, uint32_t tmem, int b, int cw, bool first,
                                            bool last, double2* __restrict__ out) {
-    constexpr int H = NC / 2;
+    constexpr int H = NC;
     const uint32_t lane = (uint32_t)((cw & 3) * 32) << 16;
-    const int col0 = (cw >> 2) * H;
+    const int col0 = 0;
     const uint32_t part = tmem + lane + (uint32_t)(b * 2 * NC + col0);
     const uint32_t sum = tmem + lane + TcCfg<NC>::ACC64 + (uint32_t)(2 * col0);
 #pragma unroll
@@ -795,9 +858,10 @@ __device__ __forceinline__ TcPos tc_next(const TcArgs& a, TcPos p) {
 // blockIdx.x + gridDim.x, ... as one stream of chunks q.
 //   producers (warps 0-7): prefetch the raw data of chunk q + NRAW - 1
 //     (cp.async), wait for stage q % NSTAGE to be free, regenerate P and stage B
-//     for chunk q; thread 0 then issues the chunk's MMAs into the accumulator
-//     buffer of its group (after that buffer was drained) and commits
-//     stage-free / group-ready;
+//     for chunk q and mark the stage full;
+//   MMA warp (warp 16, one thread): wait for the stage and, at a group's first
+//     chunk, for its accumulator buffer to be drained; issue the chunk's MMAs
+//     and commit stage-free / group-ready;
 //   consumers (warps 8-15): per group, wait until ready, fold the accumulator
 //     into the FP64 sums, release the buffer, and write a finished tile out.
 template <class Dir, int NC>
@@ -808,7 +872,8 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
     extern __shared__ __align__(1024) unsigned char smem[];
     float* stages = reinterpret_cast<float*>(smem);
     unsigned long long* empty = reinterpret_cast<unsigned long long*>(smem + tcs::OFF_BAR);  // [NSTAGE]
-    unsigned long long* accfull = empty + tcs::NSTAGE;                                        // [NACC]
+    unsigned long long* full = empty + tcs::NSTAGE;                                           // [NSTAGE]
+    unsigned long long* accfull = full + tcs::NSTAGE;                                         // [NACC]
     unsigned long long* accempty = accfull + NACC;                                            // [NACC]
     volatile int* abort = reinterpret_cast<volatile int*>(accempty + NACC);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(accempty + NACC) + 1;
@@ -819,10 +884,13 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
 
     if (warp == 0) tmem_alloc(smem_u32(tslot), NCOLS);
     if (tid == 0) {
-        for (int i = 0; i < tcs::NSTAGE; i++) mbar_init(smem_u32(&empty[i]), 1);
+        for (int i = 0; i < tcs::NSTAGE; i++) {
+            mbar_init(smem_u32(&empty[i]), 1);
+            mbar_init(smem_u32(&full[i]), 1);
+        }
         for (int i = 0; i < NACC; i++) {
             mbar_init(smem_u32(&accfull[i]), 1);
-            mbar_init(smem_u32(&accempty[i]), 256);
+            mbar_init(smem_u32(&accempty[i]), tc::NCONS);
         }
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -832,8 +900,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
     const uint32_t tmem = *tslot;
     int issued = -1;
 
-    if (tid < 256) {
-        asm volatile("setmaxnreg.inc.sync.aligned.u32 152;" ::: "memory");
+    if (tid < tc::NPROD) {
         TcPos cur = first, pf = first;
 #pragma unroll
         for (int i = 0; i < tcs::NRAW - 1; i++) {
@@ -843,8 +910,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
             }
             cp_async_commit();
         }
-        int q = 0, gq = -1;
-        bool go = true;
+        int q = 0;
         while (cur.t < a.ntiles) {
             if (pf.t < a.ntiles) {
                 Dir::prefetch(a, in, pf, smem, (q + tcs::NRAW - 1) % tcs::NRAW);
@@ -853,8 +919,8 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
             cp_async_commit();
             cp_async_wait<tcs::NRAW - 1>();
             const int s = q % tcs::NSTAGE;
-            bool v = go;
-            if (tid == 0 && v && q >= tcs::NSTAGE)
+            bool v = true;
+            if (tid == 0 && q >= tcs::NSTAGE)
                 v = mbar_wait_abort(smem_u32(&empty[s]), (uint32_t)((q / tcs::NSTAGE - 1) & 1), abort);
             if (!producers_and(v)) break;  // also publishes every producer's prefetched data
             float* As = stages + s * tc::STAGE_F;
@@ -862,28 +928,39 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
             Dir::fill(a, cur, As, Bs, smem, q % tcs::NRAW);
             fence_async_smem();
             producers_sync();
-            const bool gfirst = cur.kc % a.group == 0;
-            const bool glast = cur.kc % a.group == a.group - 1 || cur.kc == cur.nk - 1;
-            if (gfirst) gq++;
-            if (tid == 0) {
-                const int b = gq % NACC;
-                if (gfirst && gq >= NACC)
-                    go = mbar_wait_abort(smem_u32(&accempty[b]), (uint32_t)(((gq - NACC) / NACC) & 1), abort);
-                if (go) {
-                    tc_fence_after();
-                    tc_issue_chunk<NC>(As, Bs, tmem + b * 2 * NC, !gfirst);
-                    mma_commit(smem_u32(&empty[s]));
-                    if (glast) mma_commit(smem_u32(&accfull[b]));
-                    issued = q;
-                }
-            }
+            if (tid == 0) mbar_arrive(smem_u32(&full[s]));
             q++;
             cur = tc_next<Dir>(a, cur);
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp == tc::MMA_WARP) {
+        // MMA warp: lane 0 issues each staged chunk once the producers filled it
+        if (tid == tc::MMA_WARP * 32) {
+            TcPos cur = first;
+            int q = 0, gq = -1;
+            while (cur.t < a.ntiles) {
+                const int s = q % tcs::NSTAGE;
+                const bool gfirst = cur.kc % a.group == 0;
+                const bool glast = cur.kc % a.group == a.group - 1 || cur.kc == cur.nk - 1;
+                if (gfirst) gq++;
+                const int b = gq % NACC;
+                if (!mbar_wait_abort(smem_u32(&full[s]), (uint32_t)((q / tcs::NSTAGE) & 1), abort)) break;
+                if (gfirst && gq >= NACC &&
+                    !mbar_wait_abort(smem_u32(&accempty[b]), (uint32_t)(((gq - NACC) / NACC) & 1), abort))
+                    break;
+                tc_fence_after();
+                float* As = stages + s * tc::STAGE_F;
+                tc_issue_chunk<NC>(As, As + 4 * tc::ATILE, tmem + b * 2 * NC, !gfirst);
+                mma_commit(smem_u32(&empty[s]));
+                if (glast) mma_commit(smem_u32(&accfull[b]));
+                issued = q;
+                q++;
+                cur = tc_next<Dir>(a, cur);
+            }
+        }
+        __syncwarp();
     } else {
-        asm volatile("setmaxnreg.dec.sync.aligned.u32 104;" ::: "memory");
-        const int cw = warp - 8;
+        const int cw = warp - tc::NPROD / 32;
         TcPos cur = first;
         int g = -1;
         while (cur.t < a.ntiles) {
@@ -906,7 +983,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
     __syncthreads();
     if (*abort) {
         // let the last issued chunk finish before its tensor memory is freed
-        if (tid == 0) {
+        if (tid == tc::MMA_WARP * 32) {
             if (issued >= 0) {
                 const uint32_t bar = smem_u32(&empty[issued % tcs::NSTAGE]);
                 const uint32_t ph = (uint32_t)((issued / tcs::NSTAGE) & 1);
@@ -957,6 +1034,7 @@ static TcArgs make_args(const Handle* h, const MixedTables* T, int lmax, int bat
     a.tlmax = T->lmax;
     a.lmax = lmax;
     a.nh = h->nh;
+    a.nhp = T->nhp;
     a.nlat = h->nlat;
     a.batch = batch;
     a.nct = a.nrt = a.ntiles = 0;
