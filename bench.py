@@ -2,7 +2,9 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--quick]
 
-Headline workload (one "step"): the transform-throughput configuration,
+Headline workload (one "step"), run in the mixed-precision form (Legendre
+stage on tcgen05, split-TF32) with the FP64 form measured beside it: the
+transform-throughput configuration,
 T255 on the 384 x 768 Gauss grid, 64 scalar fields plus 32 vorticity/divergence
 pairs, inverse and forward transform of every field.  Metric: SHT GFLOP/s with
 the algorithmic flop count 2*nlm*nlat per field per direction per Legendre
@@ -11,8 +13,10 @@ contraction (384 contractions) plus 2.5*nphi*log2(nphi)*nlat per field FFT
 
 Inputs are synthetic (seeded complex N(0,1) spectra scaled by (l+1)^-1.5,
 Im = 0 at m = 0) and larger than L2 (>= 270 MB per step), so no L2 flush is
-needed between steps.  Also reported (not the headline): nonlinear RK4 steps/s
-at T255 and T63 (plain-method configuration) on the FP64 path.
+needed between steps.  Also reported (not the headline): the FP64 form of the
+same step, the per-field relative L2 of the mixed form against the FP64 path,
+nonlinear RK4 steps/s at T255 and T63 (plain-method configuration) in both
+forms, and REXI steps/s at T127 (M = 256, 535 poles, FP64 direct solves).
 
 --impl reference times the CPU restatement of the same algorithm (the oracle;
 the reference's SHTNS/FFTW/LAPACK build is unavailable on this machine) on the
@@ -119,112 +123,162 @@ def measured_peaks():
 
 
 # ------------------------------------------------------------------ our arm
+def _cfg1_inputs(dev, rank):
+    import torch
+
+    spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1 + rank)).to(dev)
+    vort = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 1001 + rank, zero_mean=True)).to(dev)
+    div = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 2001 + rank, zero_mean=True)).to(dev)
+    return spec, vort, div
+
+
+class Cfg1:
+    """One step of the transform-throughput configuration on one handle:
+    synthesis + analysis of the scalar fields, vector synthesis + analysis of
+    the vorticity/divergence pairs (14 kernel launches)."""
+
+    LAUNCHES = 2 + 2 + 5 + 5
+
+    def __init__(self, prec, dev, spec, vort, div):
+        import torch
+
+        from sph_swe_b200.sph import Sph
+
+        self.s = Sph(L_CFG1, precision=prec)
+        assert (self.s.nlat, self.s.nphi) == (384, 768)
+        self.spec, self.vort, self.div = spec, vort, div
+        self.grid = torch.empty(N_SCALAR, self.s.nphi, self.s.nlat, dtype=torch.float64, device=dev)
+        self.spec_out = torch.empty_like(spec)
+        self.u = self.v = self.z = self.d = None
+
+    def step(self):
+        s = self.s
+        s.SH_to_spat(self.spec, out=self.grid)
+        s.spat_to_SH(self.grid, out=self.spec_out)
+        self.u, self.v = s.vec_SH_to_spat(self.vort, self.div)
+        self.z, self.d = s.vec_spat_to_SH(self.u, self.v)
+
+    def sync_ok(self):
+        from sph_swe_b200 import capi
+
+        capi.check(capi.lib().sph_sync(self.s.h, None))
+
+
+def _time(fn, steps, st):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        fn()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _max_over_ranks(ms, world, dev):
+    import torch
+
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def _per_field_rel(a, b):
+    import torch
+
+    a = a.reshape(a.shape[0], -1)
+    b = b.reshape(b.shape[0], -1)
+    r = torch.linalg.vector_norm(a - b, dim=1) / torch.linalg.vector_norm(b, dim=1)
+    return {"max": float(r.max()), "median": float(r.median()), "fields": int(r.numel())}
+
+
 def run_ours(args, rank, world):
     import torch
 
     from sph_swe_b200 import build as b
     b.build()
-    from sph_swe_b200.sph import Sph
+    from sph_swe_b200 import capi
 
     dev = torch.device("cuda", rank % max(1, torch.cuda.device_count()))
     torch.cuda.set_device(dev)
-    s = Sph(L_CFG1)
-    assert (s.nlat, s.nphi) == (384, 768)
+    st = torch.cuda.current_stream()
     gl, gf, per_contr = cfg1_flops()
     flops_step = gl + gf
-
-    spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1 + rank)).to(dev)
-    vort = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 1001 + rank, zero_mean=True)).to(dev)
-    div = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 2001 + rank, zero_mean=True)).to(dev)
-    grid = torch.empty(N_SCALAR, s.nphi, s.nlat, dtype=torch.float64, device=dev)
-    spec_out = torch.empty_like(spec)
-    vo = torch.empty_like(vort)
-    do = torch.empty_like(div)
-
-    def step():
-        s.SH_to_spat(spec, out=grid)
-        s.spat_to_SH(grid, out=spec_out)
-        u, v = s.vec_SH_to_spat(vort, div)
-        z, d = s.vec_spat_to_SH(u, v)
-        return z, d
-
-    launches_per_step = 2 + 2 + 5 + 5
-    for _ in range(args.warmup):
-        step()
+    spec, vort, div = _cfg1_inputs(dev, rank)
+    forms = {"fp64": Cfg1(capi.SPH_PREC_FP64, dev, spec, vort, div),
+             "mixed": Cfg1(capi.SPH_PREC_MIXED, dev, spec, vort, div)}
+    for c in forms.values():
+        for _ in range(args.warmup):
+            c.step()
+        c.sync_ok()
     torch.cuda.synchronize()
 
-    # accuracy of this configuration: fwd(inv(x)) vs x, and inverse vs the oracle on one field
-    z, d = step()
-    torch.cuda.synchronize()
-    rt_scalar = float(torch.linalg.vector_norm(spec_out - spec) / torch.linalg.vector_norm(spec))
-    rt_vec = float(torch.linalg.vector_norm(z - vort) / torch.linalg.vector_norm(vort))
+    # accuracy of the mixed form against the FP64 path (which matches the oracle
+    # to 1e-12), per field: synthesis grids, analysis round trip, vector pair
+    f64, mx = forms["fp64"], forms["mixed"]
+    accuracy = {
+        "scalar_synthesis_vs_fp64": _per_field_rel(mx.grid, f64.grid),
+        "scalar_roundtrip_vs_input": _per_field_rel(mx.spec_out, spec),
+        "vector_u_vs_fp64": _per_field_rel(mx.u, f64.u),
+        "vector_v_vs_fp64": _per_field_rel(mx.v, f64.v),
+        "vorticity_roundtrip_vs_input": _per_field_rel(mx.z, vort),
+        "divergence_roundtrip_vs_input": _per_field_rel(mx.d, div),
+        "fp64_scalar_roundtrip_vs_input": _per_field_rel(f64.spec_out, spec),
+        "fp64_vorticity_roundtrip_vs_input": _per_field_rel(f64.z, vort),
+    }
 
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    st = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev.index) as clk:
-        e0.record(st)
-        for _ in range(args.steps):
-            step()
-        e1.record(st)
+    ms = {}
+    clocks = None
+    for name in ("fp64", "mixed"):
+        c = forms[name]
+        if world > 1:
+            torch.distributed.barrier()
         torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = flops_step * world / (ms * 1e-3) / 1e9
+        if name == "mixed":
+            with ClockSampler(dev.index) as clk:
+                ms[name] = _time(c.step, args.steps, st)
+            clocks = clk.summary()
+        else:
+            ms[name] = _time(c.step, args.steps, st)
+        c.sync_ok()
+        if world > 1:
+            torch.distributed.barrier()
+        ms[name] = _max_over_ranks(ms[name], world, dev)
+    value = flops_step * world / (ms["mixed"] * 1e-3) / 1e9
+    value_fp64 = flops_step * world / (ms["fp64"] * 1e-3) / 1e9
 
-    # dominant kernel: the FP64 Legendre stage, timed alone on the same stream
-    four = torch.empty(N_SCALAR, L_CFG1 + 1, s.nlat, dtype=torch.complex128, device=dev)
-    for _ in range(3):
-        s.legendre_synthesis(spec, four)
-        s.legendre_analysis(four, spec_out)
-    torch.cuda.synchronize()
-    nrep = max(3, args.steps)
-    e2, e3, e4 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    e2.record(st)
-    for _ in range(nrep):
-        s.legendre_synthesis(spec, four)
-    e3.record(st)
-    for _ in range(nrep):
-        s.legendre_analysis(four, spec_out)
-    e4.record(st)
-    torch.cuda.synchronize()
-    t_syn = e2.elapsed_time(e3) / nrep * 1e-3
-    t_ana = e3.elapsed_time(e4) / nrep * 1e-3
-    leg_flops = per_contr * N_SCALAR
-    # FP64 peak for the roofline: cuBLAS DGEMM measured in this run
-    a = torch.randn(4096, 4096, dtype=torch.float64, device=dev)
-    bm = torch.randn(4096, 4096, dtype=torch.float64, device=dev)
-    for _ in range(2):
-        torch.matmul(a, bm)
-    torch.cuda.synchronize()
-    best = 1e9
-    for _ in range(5):
-        e5, e6 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e5.record(st)
-        torch.matmul(a, bm)
-        e6.record(st)
+    # Legendre stages timed alone on the same stream (64 scalar fields)
+    leg = {}
+    for name, c in forms.items():
+        four = torch.empty(N_SCALAR, L_CFG1 + 1, c.s.nlat, dtype=torch.complex128, device=dev)
+        for _ in range(3):
+            c.s.legendre_synthesis(spec, four)
+            c.s.legendre_analysis(four, c.spec_out)
         torch.cuda.synchronize()
-        best = min(best, e5.elapsed_time(e6) * 1e-3)
-    fp64_peak = 2.0 * 4096 ** 3 / best / 1e12
-    del a, bm
-    achieved = leg_flops / t_ana / 1e12
-    roofline = {"bound": "tensor", "kernel": "k_legendre_analysis (FP64, 64 fields, T255)", "achieved": achieved,
-                "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
-                "peak_source": "FP64 dense: cuBLAS DGEMM 4096^3 measured in this run (no FP64 figure in "
-                               "MEASURED_PEAKS.json)",
-                "legendre_synthesis_tflops": leg_flops / t_syn / 1e12}
-    if args.traffic is not None:
-        roofline["traffic"] = args.traffic
+        nrep = max(3, min(args.steps, 50))
+        t_syn = _time(lambda: c.s.legendre_synthesis(spec, four), nrep, st) * 1e-3
+        t_ana = _time(lambda: c.s.legendre_analysis(four, c.spec_out), nrep, st) * 1e-3
+        c.sync_ok()
+        leg[name] = {"synthesis_us": t_syn * 1e6, "analysis_us": t_ana * 1e6,
+                     "synthesis_tflops": per_contr * N_SCALAR / t_syn / 1e12,
+                     "analysis_tflops": per_contr * N_SCALAR / t_ana / 1e12}
+        del four
+    peaks, src = measured_peaks()
+    tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2.0
+    achieved = per_contr * N_SCALAR / (leg["mixed"]["analysis_us"] * 1e-6) / 1e12
+    roofline = {"bound": "tensor", "kernel": "k_legendre_tc<AnaDir<64>> (split-TF32 analysis, 64 fields, T255)",
+                "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s", "frac": achieved / tf32_peak,
+                "traffic": args.traffic,
+                "peak_source": f"dense TF32 = half the bf16 figure of MEASURED_PEAKS.json ({src}); achieved counts "
+                               "the algorithmic 2*nlm*nlat flops per field, the split form issues 3x that on the "
+                               "tensor pipe",
+                "legendre": leg}
 
-    # end-to-end through the C ABI with host buffers: H2D of the input spectra,
-    # the step, D2H of the output spectra
+    # end-to-end through the C ABI with host buffers (mixed form): H2D of the
+    # input spectra, the step, D2H of the output spectra
     h_spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1 + rank)).pin_memory()
     h_vort = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 1001 + rank, zero_mean=True)).pin_memory()
     h_div = torch.from_numpy(random_spec(L_CFG1, N_PAIRS, 2001 + rank, zero_mean=True)).pin_memory()
@@ -238,75 +292,110 @@ def run_ours(args, rank, world):
         spec.copy_(h_spec, non_blocking=True)
         vort.copy_(h_vort, non_blocking=True)
         div.copy_(h_div, non_blocking=True)
-        z, d = step()
-        o_spec.copy_(spec_out, non_blocking=True)
-        o_vort.copy_(z, non_blocking=True)
-        o_div.copy_(d, non_blocking=True)
+        mx.step()
+        o_spec.copy_(mx.spec_out, non_blocking=True)
+        o_vort.copy_(mx.z, non_blocking=True)
+        o_div.copy_(mx.d, non_blocking=True)
 
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
-    e7, e8 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e7.record(st)
-    for _ in range(args.steps):
-        e2e_step()
-    e8.record(st)
-    torch.cuda.synchronize()
-    ms_e2e = e7.elapsed_time(e8) / args.steps
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = _max_over_ranks(_time(e2e_step, args.steps, st), world, dev)
     e2e_value = flops_step * world / (ms_e2e * 1e-3) / 1e9
-    del spec, vort, div, grid, four
+    for c in forms.values():
+        c.s.close()
+    del forms, f64, mx, spec, vort, div
     torch.cuda.empty_cache()
 
-    extra = {}
+    extra = {"fp64_form": {"value": value_fp64, "unit": "GFLOP/s", "ms_per_step": ms["fp64"]},
+             "mixed_over_fp64": ms["fp64"] / ms["mixed"]}
     if not args.quick:
         extra["rk4"] = rk4_rates(dev, args)
-    return dict(value=value, ms=ms, roofline=roofline, clocks=clk.summary(),
+        extra["rexi"] = rexi_rates(dev, args)
+    return dict(value=value, ms=ms["mixed"], roofline=roofline, clocks=clocks,
                 e2e={"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                      "ms_per_step": ms_e2e},
-                launches=launches_per_step * args.steps, accuracy={"scalar_roundtrip_rel_l2": rt_scalar,
-                                                                   "vector_roundtrip_rel_l2": rt_vec},
-                extra=extra)
+                launches=Cfg1.LAUNCHES * args.steps, accuracy=accuracy, extra=extra)
+
+
+def _bump_state(s, dev, h0=1e4, amp=500.0):
+    import torch
+
+    lat0, lon0 = np.deg2rad(30.0), np.deg2rad(60.0)
+
+    def bump(lon, mu):
+        p = np.arcsin(mu)
+        c = np.sin(p) * np.sin(lat0) + np.cos(p) * np.cos(lat0) * np.cos(lon - lon0)
+        return h0 + amp * np.exp(-(np.arccos(np.clip(c, -1, 1)) / 0.1) ** 2)
+
+    st = torch.zeros(3, s.nlm, dtype=torch.complex128, device=dev)
+    st[0] = s.spat_to_SH(torch.from_numpy(s.grid_from(bump)).to(dev))
+    return st
 
 
 def rk4_rates(dev, args):
-    """Nonlinear RK4 steps/s (FP64 path) at T255 and at the T63 plain-method configuration."""
+    """Nonlinear RK4 steps/s at T255 and at the T63 plain-method configuration,
+    FP64 and mixed form, with the relative L2 of the mixed state against the
+    FP64 state after the same steps."""
     import torch
 
+    from sph_swe_b200 import capi
     from sph_swe_b200.sph import Sph
 
     # T255: the reference's non-Robert advective form is unstable at dt = 30 s
     # (the oracle diverges within 60 steps); dt = 10 s with the reference's
     # default viscosity 1e5 runs stably.  T63: the plain-method configuration.
     out = {}
-    for L, dt, a, visc in ((255, 10.0, 6.371e6, 1e5), (63, 120.0, 6.371e6, 0.0)):
-        s = Sph(L)
-        lat0, lon0 = np.deg2rad(30.0), np.deg2rad(60.0)
-
-        def bump(lon, mu):
-            p = np.arcsin(mu)
-            c = np.sin(p) * np.sin(lat0) + np.cos(p) * np.cos(lat0) * np.cos(lon - lon0)
-            return 1e4 + 500.0 * np.exp(-(np.arccos(np.clip(c, -1, 1)) / 0.1) ** 2)
-
-        hgrid = torch.from_numpy(s.grid_from(bump)).to(dev)
-        st = torch.zeros(3, s.nlm, dtype=torch.complex128, device=dev)
-        st[0] = s.spat_to_SH(hgrid)
-        p = Sph.swe_params(radius=a, dt=dt, viscosity=visc)
-        s.swe_rk4(p, st, 3)
-        torch.cuda.synchronize()
-        n = 50 if L == 255 else 200
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        s.swe_rk4(p, st, n)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / n
-        out[f"T{L}"] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms, "nsteps": n, "dt": dt, "viscosity": visc,
+    for L, dt, visc, n in ((255, 10.0, 1e5, 50), (63, 120.0, 0.0, 200)):
+        res = {}
+        states = {}
+        s0 = Sph(L)
+        st0 = _bump_state(s0, dev)  # one initial state (FP64 analysis) for both forms
+        s0.close()
+        for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
+            s = Sph(L, precision=prec)
+            p = Sph.swe_params(radius=6.371e6, dt=dt, viscosity=visc)
+            st = st0.clone()
+            s.swe_rk4(p, st, 3)
+            torch.cuda.synchronize()
+            st = st0.clone()
+            ms = _time(lambda: s.swe_rk4(p, st, n), 1, torch.cuda.current_stream()) / n
+            capi.check(capi.lib().sph_sync(s.h, None))
+            states[name] = st
+            res[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms}
+            s.close()
+        rel = {q: float(torch.linalg.vector_norm(states["mixed"][k] - states["fp64"][k]) /
+                        torch.linalg.vector_norm(states["fp64"][k])) for k, q in enumerate("huv")}
+        out[f"T{L}"] = {**res, "mixed_over_fp64": res["mixed"]["steps_per_s"] / res["fp64"]["steps_per_s"],
+                        "nsteps": n, "dt": dt, "viscosity": visc, "mixed_rel_l2_vs_fp64_after_nsteps": rel,
                         "kernel_launches_per_step": 4 * 11 + 1}
-        s.close()
+    return out
+
+
+def rexi_rates(dev, args):
+    """REXI configuration: T127 192x384, Robert linear SWE about h0 = 1e4 m,
+    Gaussian-approximation REXI h = 0.2, M = 256 (535 poles), tau = 3600 s,
+    24 steps from the Gaussian bump; FP64 direct banded solves."""
+    import torch
+
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph, rexi_coefficients
+
+    s = Sph(127)
+    a, br, _ = rexi_coefficients(0.2, 256, False)
+    rx = s.rexi(a, br, radius=6.371e6, tau=3600.0)
+    st0 = _bump_state(s, dev)
+    st = st0.clone()
+    rx.step(st, 2)
+    torch.cuda.synchronize()
+    st = st0.clone()
+    n = 24
+    ms = _time(lambda: rx.step(st, n), 1, torch.cuda.current_stream()) / n
+    capi.check(capi.lib().sph_sync(s.h, None))
+    out = {"T127_M256_fp64": {"steps_per_s": 1000.0 / ms, "ms_per_step": ms, "poles": int(len(a)), "nsteps": n,
+                              "tau": 3600.0}}
+    rx.close()
+    s.close()
     return out
 
 
@@ -405,9 +494,10 @@ def main():
         line = {
             "metric": METRIC, "value": r["value"], "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64 (Legendre GEMMs split-tf32, f32 chunk sums folded into f64)",
+            "data": "synthetic",
             "config": {"workload": "SHT throughput: T255 384x768 Gauss grid, 64 scalar fields + 32 vort/div pairs, "
-                                   "inverse + forward per step (FP64 plain method)",
+                                   "inverse + forward per step, mixed-precision form",
                        "lmax": L_CFG1, "nlat": 384, "nphi": 768, "fields": N_SCALAR, "vector_pairs": N_PAIRS,
                        "gflop_per_step": sum(cfg1_flops()[:2]) / 1e9,
                        "l2": "inputs larger than L2 (>= 270 MB touched per step); no flush"},

@@ -215,6 +215,16 @@ int sph_rexi_create(sph_handle* h, const double* alpha, const double* beta, int 
                     sph_rexi** out);
 int sph_rexi_destroy(sph_rexi* r);
 
+/* REXI coefficients (host computation, no device needed): poles alpha and the
+ * weights beta_re / beta_im of e^{ix} ~ sum_n beta_n / (ix + alpha_n), from the
+ * L = 11 Gaussian approximation with step h and M terms (N = M + 11 poles each
+ * side; half != 0 keeps n = -N..0 with doubled weights).  alpha, beta_re and
+ * beta_im are interleaved complex arrays of capacity cap; *npoles receives the
+ * pole count (cap = 0 and NULL arrays: size query).
+ * Replaces REXI::setup (rexi/REXI.hpp:52-131). */
+int sph_rexi_coefficients(double h, int M, int half, int cap, double* alpha, double* beta_re, double* beta_im,
+                          int* npoles);
+
 /* nsteps REXI steps in place on state = [h | u | v] (3*nlm complex): all poles
  * x all m x both l-parities are solved in one launch per step; replaces the
  * serial pole loop of AppSWE::run (AppSWE.hpp:580-729) with

@@ -4,7 +4,8 @@
 // latitude-contiguous (coalesced) accesses of the theta-contiguous grid,
 // transformed in shared memory by a mixed-radix Stockham FFT (FP64), and only
 // the zonal wavenumbers m <= L are kept (analysis) / fed (synthesis).
-// Two real rings are packed into one complex FFT.
+// Two real rings are packed into one complex FFT.  Ring lengths 3 * 2^k (the
+// automatic grids) use the compile-time kernels of fft_fixed.cuh.
 #include "common.cuh"
 
 namespace sphgpu {
@@ -23,6 +24,12 @@ struct RingMap {
     int src[16];
     int mod[16];
 };
+
+}  // namespace sphgpu
+
+#include "fft_fixed.cuh"
+
+namespace sphgpu {
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -283,7 +290,24 @@ static int ring_tile(int n, int complex_rings) {
     return jt;
 }
 
+template <int N>
+static size_t fixed_smem() {
+    return (size_t)fftx::seqs<N>() * fftx::stride<N>() * sizeof(double2);
+}
+
+template <int N>
+static int fixed_attr() {
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_analysis_real_n<N>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fixed_smem<N>()));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_synthesis_real_n<N>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fixed_smem<N>()));
+    return SPH_OK;
+}
+
 int fft_kernels_init() {
+    for (int rc : {fixed_attr<96>(), fixed_attr<192>(), fixed_attr<384>(), fixed_attr<768>(), fixed_attr<1536>(),
+                   fixed_attr<3072>()})
+        if (rc) return rc;
     const int bytes = 200 * 1024;
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_analysis_real, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_synthesis_real, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -295,6 +319,24 @@ int fft_kernels_init() {
 int ring_analysis_real(const Handle* h, const double* spat, long long ld_spat, double2* F, long long ldF, int mF,
                        int batch, cudaStream_t s) {
     if (batch <= 0) return SPH_OK;
+    switch (h->nphi) {
+#define SPH_RA(NN)                                                                                                   \
+    case NN:                                                                                                         \
+        k_ring_analysis_real_n<NN><<<dim3((h->nlat + 2 * fftx::seqs<NN>() - 1) / (2 * fftx::seqs<NN>()), batch),    \
+                                     fftx::NT, fixed_smem<NN>(), s>>>(spat, ld_spat, F, ldF, mF, h->L, h->nlat,     \
+                                                                      h->fft.tw);                                    \
+        SPH_CUDA_TRY(cudaGetLastError());                                                                            \
+        return SPH_OK;
+        SPH_RA(96)
+        SPH_RA(192)
+        SPH_RA(384)
+        SPH_RA(768)
+        SPH_RA(1536)
+        SPH_RA(3072)
+#undef SPH_RA
+        default:
+            break;
+    }
     const int JT = ring_tile(h->nphi, 0);
     const size_t sm = (size_t)JT * h->nphi * sizeof(double2);  // 2 buffers of JT/2 sequences
     dim3 grid((h->nlat + JT - 1) / JT, batch);
@@ -322,6 +364,24 @@ int ring_synthesis_real(const Handle* h, const double2* F, long long ldF, int mF
             map.src[k] = src[k];
             map.mod[k] = mod ? mod[k] : 0;
         }
+    }
+    switch (h->nphi) {
+#define SPH_RS(NN)                                                                                                   \
+    case NN:                                                                                                         \
+        k_ring_synthesis_real_n<NN><<<dim3((h->nlat + 2 * fftx::seqs<NN>() - 1) / (2 * fftx::seqs<NN>()), batch),   \
+                                      fftx::NT, fixed_smem<NN>(), s>>>(F, ldF, mF, h->L, spat, ld_spat, h->nlat,    \
+                                                                       h->fft.tw, map);                              \
+        SPH_CUDA_TRY(cudaGetLastError());                                                                            \
+        return SPH_OK;
+        SPH_RS(96)
+        SPH_RS(192)
+        SPH_RS(384)
+        SPH_RS(768)
+        SPH_RS(1536)
+        SPH_RS(3072)
+#undef SPH_RS
+        default:
+            break;
     }
     k_ring_synthesis_real<<<grid, 256, sm, s>>>(F, ldF, mF, h->L, spat, ld_spat, h->nlat, dev_plan(h->fft), h->fft.tw, JT,
                                                 map);

@@ -1012,13 +1012,14 @@ static int tc_attr() {
 }
 
 static int g_tc_sms = 0;
-static int g_tc_group = 2;
+static int g_tc_group = 1;
 
 int tc_kernels_init() {
     int dev = 0;
     SPH_CUDA_TRY(cudaGetDevice(&dev));
     SPH_CUDA_TRY(cudaDeviceGetAttribute(&g_tc_sms, cudaDevAttrMultiProcessorCount, dev));
-    if (const char* e = getenv("SPH_TC_GROUP")) g_tc_group = atoi(e) == 1 ? 1 : 2;
+    // chunks per FP32 accumulation group: 1 (default, each 16-term chunk folded into FP64) or 2
+    if (const char* e = getenv("SPH_TC_GROUP")) g_tc_group = atoi(e) == 2 ? 2 : 1;
     if (int rc = tc_attr<16>()) return rc;
     if (int rc = tc_attr<32>()) return rc;
     return tc_attr<64>();

@@ -28,6 +28,19 @@ def _ptr(t: torch.Tensor):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def rexi_coefficients(h: float = 0.2, M: int = 256, half: bool = False):
+    """REXI poles alpha and weights beta_re, beta_im (complex128 arrays) of
+    e^{ix} ~ sum_n beta_n / (ix + alpha_n); see sph_rexi_coefficients."""
+    L = capi.lib()
+    n = ctypes.c_int()
+    capi.check(L.sph_rexi_coefficients(h, M, int(half), 0, None, None, None, ctypes.byref(n)))
+    out = [np.zeros(n.value, np.complex128) for _ in range(3)]
+    dp = ctypes.POINTER(ctypes.c_double)
+    capi.check(L.sph_rexi_coefficients(h, M, int(half), n.value, *(o.view(np.float64).ctypes.data_as(dp) for o in out),
+                                       ctypes.byref(n)))
+    return tuple(out)
+
+
 class Sph:
     """One transform handle (replaces SPHConfig + its shtns_cfg)."""
 

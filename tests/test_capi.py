@@ -3,6 +3,8 @@ exports every entry point declared in include/sph_gpu.h (no compute calls)."""
 import os
 import re
 
+import numpy as np
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -48,3 +50,33 @@ def test_error_reporting_without_gpu(lib):
     assert rc == capi.SPH_ERR_ARG
     assert "lmax == mmax" in capi.last_error()
     assert lib.sph_info(None, None, None, None, None, None) == capi.SPH_ERR_ARG
+
+
+@pytest.mark.parametrize("M,half", [(64, False), (256, False), (256, True), (32, True)])
+def test_rexi_coefficients_match_oracle(oracle_mod, M, half):
+    """Host-side coefficient generation of the library against the oracle's
+    REXI::setup restatement, and the approximation of e^{ix} it is built for."""
+    from sph_swe_b200.sph import rexi_coefficients
+
+    a, br, bi = rexi_coefficients(0.2, M, half)
+    ra, rbr, rbi = oracle_mod.rexi_coeffs(0.2, M, half=half)
+    assert len(a) == len(ra) == (M + 12 if half else 2 * (M + 11) + 1)
+    for x, y in ((a, ra), (br, rbr), (bi, rbi)):
+        assert np.max(np.abs(x - y)) <= 1e-14 * np.max(np.abs(y))
+    # the full pole set approximates e^{ix} on |x| <= M h / 2 (both parts)
+    xs = np.linspace(-0.5 * M * 0.2, 0.5 * M * 0.2, 101)
+    if not half:
+        approx = np.array([np.sum((br / (1j * x + a)).real) + 1j * np.sum((bi / (1j * x + a)).real) for x in xs])
+        assert np.max(np.abs(approx - np.exp(1j * xs))) < 1e-7
+
+
+def test_rexi_coefficients_reject_bad_arguments():
+    import ctypes
+
+    from sph_swe_b200 import capi
+
+    n = ctypes.c_int()
+    assert capi.lib().sph_rexi_coefficients(0.0, 10, 0, 0, None, None, None, ctypes.byref(n)) == capi.SPH_ERR_ARG
+    buf = (ctypes.c_double * 4)()
+    assert capi.lib().sph_rexi_coefficients(0.2, 10, 0, 2, buf, buf, buf, ctypes.byref(n)) == capi.SPH_ERR_ARG
+    assert "capacity" in capi.last_error()

@@ -6,10 +6,10 @@ Tolerances (relative L2 against the FP64 oracle / FP64 GPU path):
   vector synthesis u, v                   <= 2e-6
   vector round trip vort -> u,v -> vort   <= 5e-5  (the analysis of u, v divides
       by l(l+1) and amplifies the split-TF32 error at high degree)
-  nonlinear RK4, T63, 200 steps: h <= 1e-6; u, v <= 5e-5 (measured 2e-5: the
-      tensor core accumulates in FP32, which bounds each transform near 2e-7,
-      and the 200-step map amplifies that by ~100 in the velocity, which
-      starts from rest)
+  nonlinear RK4, T63, 200 steps: h <= 1e-6; u, v <= 1e-4 (measured 4e-5:
+      the two-term TF32 split (22 bits) and the FP32 rounding of each MMA
+      bound each transform near 2e-7, and the 200-step map amplifies that by
+      ~100 in the velocity, which starts from rest)
 """
 import numpy as np
 import pytest
@@ -101,7 +101,7 @@ def test_config0_rk4_vs_oracle(gpu, oracle_mod):
     out = st.cpu().numpy()
     rh, ru, rv, rc = g.swe_run((p.radius, p.gravity, p.omega, p.h0, p.viscosity, p.dt), h, u, v, 200)
     assert rc == 0
-    for q, (ref, tol) in enumerate(((rh, TOL), (ru, 5e-5), (rv, 5e-5))):
+    for q, (ref, tol) in enumerate(((rh, TOL), (ru, 1e-4), (rv, 1e-4))):
         assert rel_l2(out[q], ref) < tol, q
 
 
