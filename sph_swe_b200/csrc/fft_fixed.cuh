@@ -184,10 +184,24 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const doub
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
     const double* src = spat + (long long)blockIdx.y * ld_spat;
-    for (int idx = threadIdx.x; idx < N * JT; idx += fftx::NT) {
-        const int i = idx / JT, jj = idx % JT;
-        const int j = j0 + jj;
-        reinterpret_cast<double*>(&fbuf[(jj >> 1) * SN + i])[jj & 1] = (j < nlat) ? src[(long long)i * nlat + j] : 0.0;
+    // tile load in batches of U independent loads per thread
+    constexpr int PER = N * JT / fftx::NT;
+    constexpr int U = PER <= 12 ? PER : 8;
+    static_assert((N * JT) % fftx::NT == 0 && PER % U == 0, "tile divides into batches");
+    for (int base = 0; base < N * JT; base += U * fftx::NT) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int idx = base + threadIdx.x + u * fftx::NT;
+            const int i = idx / JT, j = j0 + idx % JT;
+            v[u] = (j < nlat) ? __ldg(&src[(long long)i * nlat + j]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int idx = base + threadIdx.x + u * fftx::NT;
+            const int i = idx / JT, jj = idx % JT;
+            reinterpret_cast<double*>(&fbuf[(jj >> 1) * SN + i])[jj & 1] = v[u];
+        }
     }
     __syncthreads();
     fftx::passes<N, 0, -1>(fbuf, tw);
@@ -229,12 +243,13 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const dou
     for (int idx = threadIdx.x; idx < P * SN; idx += fftx::NT) fbuf[idx] = make_double2(0, 0);
     __syncthreads();
     const int mm = min(min(mF - 1, L), (N - 1) / 2);
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < (mm + 1) * P; idx += fftx::NT) {
         const int m = idx / P, q = idx % P;
         const int j = j0 + 2 * q;
         double2 X = make_double2(0, 0), Y = make_double2(0, 0);
-        if (j < nlat) X = in[(long long)m * nlat + j];
-        if (j + 1 < nlat) Y = in[(long long)m * nlat + j + 1];
+        if (j < nlat) X = __ldg(&in[(long long)m * nlat + j]);
+        if (j + 1 < nlat) Y = __ldg(&in[(long long)m * nlat + j + 1]);
         if (mod) {  // d/dlambda: times i*m
             X = make_double2(-m * X.y, m * X.x);
             Y = make_double2(-m * Y.y, m * Y.x);
@@ -249,12 +264,12 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const dou
     __syncthreads();
     fftx::passes<N, 0, +1>(fbuf, tw);
     double* out = spat + (long long)k * ld_spat;
+#pragma unroll 8
     for (int idx = threadIdx.x; idx < N * JT; idx += fftx::NT) {
         const int i = idx / JT, jj = idx % JT;
         const int j = j0 + jj;
-        if (j >= nlat) continue;
         const double2 z = fbuf[(jj >> 1) * SN + i];
-        out[(long long)i * nlat + j] = (jj & 1) ? z.y : z.x;
+        if (j < nlat) out[(long long)i * nlat + j] = (jj & 1) ? z.y : z.x;
     }
 }
 

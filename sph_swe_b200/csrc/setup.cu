@@ -9,12 +9,15 @@
 namespace sphgpu {
 
 // One thread per northern node k: Newton iteration on P_n from the Tricomi
-// start cos(pi (k + 3/4) / (n + 1/2)); mirrored to the southern half.
+// start cos(pi (k + 3/4) / (n + 1/2)); mirrored to the southern half.  Once a
+// step is below 1e-14 the iteration is converged to within rounding after one
+// more (quadratically convergent) step.
 __global__ void k_gauss_nodes(int n, double* __restrict__ x, double* __restrict__ w) {
     const int nh = (n + 1) / 2;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nh) return;
     double z = cos(kPi * (k + 0.75) / (n + 0.5));
+    bool last = false;
     for (int it = 0; it < 100; it++) {
         double p0 = 1.0, p1 = z;
         for (int i = 2; i <= n; i++) {
@@ -25,7 +28,8 @@ __global__ void k_gauss_nodes(int n, double* __restrict__ x, double* __restrict_
         double dp = n * (z * p1 - p0) / (z * z - 1.0);
         double dz = p1 / dp;
         z -= dz;
-        if (fabs(dz) <= 1e-16 * fabs(z) + 1e-300 && it > 0) break;
+        if (last) break;
+        if (fabs(dz) < 1e-14) last = true;
     }
     double p0 = 1.0, p1 = z;
     for (int i = 2; i <= n; i++) {
