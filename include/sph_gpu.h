@@ -150,7 +150,7 @@ enum sph_spec_op_id {
     SPH_OP_MU = 2,         /* mu x (Galerkin)                SPHOperators::mu (:268-297)          */
     SPH_OP_MU2 = 3,        /* mu^2 x (Galerkin)              SPHOperators::mu2 (:303-333)         */
     SPH_OP_LAPLACE = 4,    /* -n(n+1) x                      SPHOperators::laplace (:482-498)     */
-    SPH_OP_HELMHOLTZ = 5,  /* x / (a + (-(b/r^2) n(n+1)));  args a, b (complex) and r in b.y? see below */
+    SPH_OP_HELMHOLTZ = 5,  /* x / (a - b n(n+1)), b = b_ref / r^2  spec_solve_helmholtz (SPHData.hpp:475-497) */
     SPH_OP_SCALE = 6,      /* a x                            SPHData operator*(double/complex)    */
     SPH_OP_AXPY = 7        /* out = out + a x                SPHData operator+= with scaling      */
 };
@@ -232,6 +232,24 @@ int sph_rexi_coefficients(double h, int M, int half, int cap, double* alpha, dou
  * SPHSolverComplex::solve -> zgbsv (SPHSolverComplex.hpp:462-511,
  * BandedMatrixSolver.hpp:416-427). */
 int sph_rexi_step(sph_rexi* r, double* state, int nsteps, void* stream);
+
+/* ---------------------------------------------------------------- grid arithmetic */
+
+/* elementwise grid operations of sph_spat_op */
+enum sph_spat_op_kind {
+    SPH_SPAT_MUL = 0,        /* out = alpha * x * y                              */
+    SPH_SPAT_AXPBY = 1,      /* out = alpha * x + beta * y   (y may be NULL)     */
+    SPH_SPAT_FILL = 2,       /* out = alpha                                      */
+    SPH_SPAT_ADD_CONST = 3,  /* out = x + alpha                                  */
+    SPH_SPAT_CMUL = 4        /* complex: out = alpha * x * y, n complex elements */
+};
+
+/* n elements (doubles; complex elements for SPH_SPAT_CMUL) on the stream; in
+ * place allowed.  The grid arithmetic of SPHData / SPHDataComplex: the grid
+ * product operator* (SPHData.hpp:334-353, SPHDataComplex.hpp:321-340) and the
+ * scalar grid updates spat_set_value / spat_set_zero (SPHData.hpp:768-798). */
+int sph_spat_op(sph_handle* h, int op, const double* x, const double* y, double* out, double alpha, double beta,
+                long long n, void* stream);
 
 /* ---------------------------------------------------------------- errors */
 

@@ -18,6 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libsphgpu.so")
+CLI_SRC = os.path.join(HERE, "cli", "sh_example.cpp")
+CLI = os.path.join(HERE, "sh_example")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -34,14 +36,27 @@ def sources():
 
 def headers():
     return sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) +
-                  glob.glob(os.path.join(INCLUDE, "*.h")))
+                  glob.glob(os.path.join(INCLUDE, "*.h")) + glob.glob(os.path.join(INCLUDE, "sph_swe", "*.hpp")))
 
 
 def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) <= t for f in sources() + headers() + [__file__])
+    t = min(os.path.getmtime(LIB), os.path.getmtime(CLI))
+    return all(os.path.getmtime(f) <= t for f in sources() + headers() + [CLI_SRC, __file__])
+
+
+def build_cli() -> str:
+    """The sh_example driver, linked against the in-tree library (rpath $ORIGIN)."""
+    cuda = os.path.dirname(os.path.dirname(nvcc()))
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+    tmp = CLI + ".tmp"
+    cmd = [cxx, "-std=c++17", "-O2", "-I", INCLUDE, "-I", os.path.join(cuda, "include"), CLI_SRC, "-o", tmp,
+           "-L", HERE, "-lsphgpu", "-L", os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN",
+           "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, CLI)
+    return CLI
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
@@ -73,6 +88,7 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     tmp = LIB + ".tmp"
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
+    build_cli()
     return LIB
 
 

@@ -22,7 +22,7 @@ EXPORTS = (
     "sph_spat_to_SH", "sph_SH_to_spat", "sph_SH_to_spat_noalloc", "sph_cplx_spat_to_SH", "sph_cplx_SH_to_spat",
     "sph_vec_SH_to_spat", "sph_vec_spat_to_SH", "sph_legendre_synthesis", "sph_legendre_analysis", "sph_spec_op",
     "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched",
-    "sph_rexi_coefficients", "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_sync", "sph_last_error",
+    "sph_spat_op", "sph_rexi_coefficients", "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_sync", "sph_last_error",
 )
 
 
@@ -78,6 +78,7 @@ def lib():
         L.sph_rexi_coefficients.argtypes = [d, i, i, i, dp, dp, dp, ip]
         L.sph_rexi_step.argtypes = [vp, vp, i, vp]
         L.sph_sync.argtypes = [vp, vp]
+        L.sph_spat_op.argtypes = [vp, i, vp, vp, vp, d, d, ll, vp]
         L.sph_last_error.argtypes = [ctypes.c_char_p, i]
         for n in EXPORTS:
             getattr(L, n).restype = ctypes.c_int

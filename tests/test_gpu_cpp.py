@@ -1,0 +1,107 @@
+"""The C++ class surface (include/sph_swe/sph_swe.hpp) and the sh_example
+driver against the oracle: operators of SPHData / SPHOperators through a
+compiled C++ program, and shallow-water runs of sh_example (RK4 and REXI)
+compared with the oracle's runs of the same configuration."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests.helpers import bump_state, random_spec, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "sph_swe_b200")
+
+
+@pytest.fixture(scope="module")
+def classes_bin(gpu, tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("cpp") / "classes_check")
+    cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "cpp", "classes_check.cpp"), "-o", out, "-L", PKG, "-lsphgpu",
+           "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath," + PKG, "-Wl,-rpath,/usr/local/cuda/lib64"]
+    subprocess.run(cmd, check=True)
+    return out
+
+
+@pytest.mark.parametrize("L", [31, 63])
+def test_class_operators_match_oracle(classes_bin, oracle_mod, tmp_path, L):
+    g = oracle_mod.Grid(L)
+    x, y = random_spec(L, 2, seed=40 + L)
+    inp = tmp_path / "in.bin"
+    np.concatenate([x, y]).astype(np.complex128).tofile(inp)
+    outp = tmp_path / "out.bin"
+    r = subprocess.run([classes_bin, str(L), str(inp), str(outp)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    nphi, nlat, nlm, ncplx = map(int, r.stdout.split()[:4])
+    assert (nphi, nlat, nlm) == (g.nphi, g.nlat, g.nlm)
+    raw = np.fromfile(outp, np.uint8)
+    kinds = "sssssgggsssgsss" + "s"
+    blocks, off = [], 0
+    for k in kinds:
+        n = nlm * 16 if k == "s" else nphi * nlat * 8
+        blocks.append(raw[off:off + n].view(np.complex128 if k == "s" else np.float64))
+        off += n
+    assert off == raw.size
+    ref = {}
+    for i, op in enumerate(["diff_lon", "d1mu2", "mu", "mu2", "laplace", "grad_lon", "grad_lat", "div_lat", "mul123",
+                            "add100"]):
+        ref[i] = g.real_op(op, x, kind="spec")[1]
+    for i in range(10):
+        b = blocks[i] if kinds[i] == "s" else blocks[i].reshape(nphi, nlat)
+        assert rel_l2(b, ref[i]) < 1e-12, i
+    assert rel_l2(blocks[10], x - y) < 1e-14
+    assert rel_l2(blocks[11].reshape(nphi, nlat), g.SH_to_spat(x) * g.SH_to_spat(y)) < 1e-12
+    n = np.concatenate([np.arange(m, L + 1) for m in range(L + 1)])
+    assert rel_l2(blocks[12], x / (1.5 - 2.0e-3 / 9.0 * n * (n + 1))) < 1e-14
+    # vort = F(grad_lon(y)) - F(grad_lat(x)), div = F(grad_lon(x)) + F(div_lat(y))
+    vort = g.spat_to_SH(g.real_op("grad_lon", y, kind="spec")[1]) - g.spat_to_SH(g.real_op("grad_lat", x, kind="spec")[1])
+    div = g.spat_to_SH(g.real_op("grad_lon", x, kind="spec")[1]) + g.spat_to_SH(g.real_op("div_lat", y, kind="spec")[1])
+    assert rel_l2(blocks[13], vort) < 1e-12
+    assert rel_l2(blocks[14], div) < 1e-12
+    assert rel_l2(blocks[15], g.spat_to_SH(g.grid_from(lambda lon, mu: mu * np.cos(lon) + 2.0))) < 1e-13
+    assert "nan 0" in r.stdout
+
+
+def _run_cli(args, tmp_path):
+    dump = tmp_path / "state.bin"
+    r = subprocess.run([os.path.join(PKG, "sh_example"), *args, f"D{dump}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return np.fromfile(dump, np.complex128), r.stdout
+
+
+def test_sh_example_rk4_matches_oracle(gpu, oracle_mod, tmp_path):
+    """sh_example T31 P0 N1 R120 E2400 Q10 (reference defaults otherwise: a = 6.37122e6,
+    viscosity 1e5), 20 RK4 steps; a trailing T<k> is ignored as in the reference."""
+    st, out = _run_cli(["T31", "P0", "N1", "R120", "E2400", "O1e9", "Q10", "T99"], tmp_path)
+    assert "Using T=31 on 48 x 96" in out
+    g = oracle_mod.Grid(31)
+    h = g.spat_to_SH(bump_state(g))
+    z = np.zeros(g.nlm, complex)
+    rh, ru, rv, rc = g.swe_run((6.37122e6, 9.80616, 7.292e-5, 1e4, 1e5, 120.0), h, z, z, 20)
+    assert rc == 0
+    for q, ref in enumerate((rh, ru, rv)):
+        assert rel_l2(st[q * g.nlm:(q + 1) * g.nlm], ref) < 1e-10, q
+
+
+def test_sh_example_rexi_matches_oracle(gpu, oracle_mod, tmp_path):
+    """sh_example T31 P0 N0 S1 M64 H0.2 I0 R3600 E7200 Q10: REXI (Robert), full pole set."""
+    st, out = _run_cli(["T31", "P0", "N0", "S1", "M64", "H0.2", "I0", "R3600", "E7200", "O1e9", "Q10"], tmp_path)
+    assert "REXI poles: 151" in out
+    g = oracle_mod.Grid(31)
+    h = g.spat_to_SH(bump_state(g))
+    z = np.zeros(g.nlm, complex)
+    rh, ru, rv, npol = g.rexi_run((6.37122e6, 9.80616, 7.292e-5, 1e4, 1e5, 3600.0), h, z, z, 2, rexi_h=0.2, rexi_M=64,
+                                  half=False, robert=1)
+    for q, ref in enumerate((rh, ru, rv)):
+        assert rel_l2(st[q * g.nlm:(q + 1) * g.nlm], ref) < 1e-10, q
+
+
+def test_sh_example_rejects_bad_usage(gpu):
+    exe = os.path.join(PKG, "sh_example")
+    assert subprocess.run([exe], capture_output=True).returncode != 0
+    assert subprocess.run([exe, "T31", "P1", "R1", "E1"], capture_output=True).returncode != 0
+    r = subprocess.run([exe, "T31", "P0", "N1", "S0", "M32", "R100", "E100"], capture_output=True, text=True)
+    assert r.returncode != 0 and "Robert" in r.stderr
