@@ -312,6 +312,8 @@ def run_ours(args, rank, world):
     if not args.quick:
         extra["rk4"] = rk4_rates(dev, args)
         extra["rexi"] = rexi_rates(dev, args)
+        extra["ensemble"] = ensemble_rates(dev, args)
+        extra["T1023"] = t1023_rates(dev, args)
     return dict(value=value, ms=ms["mixed"], roofline=roofline, clocks=clocks,
                 e2e={"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                      "ms_per_step": ms_e2e},
@@ -396,6 +398,130 @@ def rexi_rates(dev, args):
                               "tau": 3600.0}}
     rx.close()
     s.close()
+    return out
+
+
+def t1023_rates(dev, args):
+    """T1023 configuration: 1536 x 3072 Gauss grid, nonlinear equations in
+    Robert variables, zonal jet 80 sech^2((phi - 45 deg)/0.1) m/s with h in
+    gradient-wind balance (mean 1e4 m) plus a 120 m bump at (30N, 60E),
+    dt = 15 s, 50 steps; FP64 and mixed form, mass drift (Y_00 of h)."""
+    import torch
+
+    from sph_swe_b200 import capi, scenarios
+    from sph_swe_b200.sph import Sph
+
+    L, n, dt = 1023, 50, 15.0
+    res, states = {}, {}
+    st0 = None
+    for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
+        s = Sph(L, precision=prec)
+        if st0 is None:
+            h, u, v = scenarios.sech2_jet(s, radius=6.371e6, bump_amp=120.0)
+            c = torch.from_numpy(np.cos(s.lat)).to(dev)[None, :]
+            st0 = torch.stack([s.spat_to_SH(torch.from_numpy(h).to(dev)),
+                               s.spat_to_SH(torch.from_numpy(u).to(dev) * c),
+                               s.spat_to_SH(torch.from_numpy(v).to(dev) * c)])
+        p = Sph.swe_params(radius=6.371e6, dt=dt, nonlinear=2, robert=1)
+        st = st0.clone()
+        s.swe_rk4(p, st, 3)
+        torch.cuda.synchronize()
+        st = st0.clone()
+        ms = _time(lambda: s.swe_rk4(p, st, n), 1, torch.cuda.current_stream()) / n
+        capi.check(capi.lib().sph_sync(s.h, None))
+        m0, m1 = st0[0, 0].real.item(), st[0, 0].real.item()
+        res[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms, "mass_drift_rel": abs(m1 - m0) / abs(m0)}
+        states[name] = st
+        s.close()
+    rel = {q: float(torch.linalg.vector_norm(states["mixed"][k] - states["fp64"][k]) /
+                    torch.linalg.vector_norm(states["fp64"][k])) for k, q in enumerate(("h", "U", "V"))}
+    out = {**res, "mixed_over_fp64": res["mixed"]["steps_per_s"] / res["fp64"]["steps_per_s"], "nsteps": n, "dt": dt,
+           "grid": "1536 x 3072", "form": "nonlinear, Robert variables", "mixed_rel_l2_vs_fp64_after_nsteps": rel}
+    del states, st0
+    torch.cuda.empty_cache()
+    return out
+
+
+ENSEMBLE = ((31, 96), (63, 96), (127, 48), (255, 16))
+ENSEMBLE_STEPS = 100
+
+
+def _random_bumps(s, n, rng, h0=1e4):
+    """n grids h0 + A exp(-(d/sigma)^2): A ~ U(100, 800) m, centre uniform on
+    the sphere (sin(lat) ~ U(-1, 1), lon ~ U(0, 2 pi)), sigma ~ U(0.05, 0.2) rad."""
+    out = []
+    for _ in range(n):
+        amp, z, lon0, sig = rng.uniform(100, 800), rng.uniform(-1, 1), rng.uniform(0, 2 * np.pi), rng.uniform(0.05, 0.2)
+        lat0 = np.arcsin(z)
+
+        def f(lon, mu, lat0=lat0, lon0=lon0, amp=amp, sig=sig):
+            p = np.arcsin(mu)
+            c = np.sin(p) * np.sin(lat0) + np.cos(p) * np.cos(lat0) * np.cos(lon - lon0)
+            return h0 + amp * np.exp(-(np.arccos(np.clip(c, -1, 1)) / sig) ** 2)
+
+        out.append(s.grid_from(f))
+    return np.stack(out)
+
+
+def ensemble_rates(dev, args):
+    """Ensemble configuration: 256 members (96 x T31, 96 x T63, 48 x T127,
+    16 x T255), nonlinear RK4 with dt = 120 * 63 / T s, 100 steps, one CUDA
+    graph replay per step for all members (each truncation on its own graph
+    branch).  FP64 and mixed form; the FP64 form is also timed group by group
+    (one batched graph per truncation, run one after another) to show what the
+    branches overlap; the mixed state is compared with the FP64 state."""
+    import torch
+
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Ensemble, Sph
+
+    rng = np.random.default_rng(20261203)
+    init = {}
+    for L, n in ENSEMBLE:
+        s = Sph(L)
+        st = torch.zeros(n, 3, s.nlm, dtype=torch.complex128, device=dev)
+        st[:, 0] = s.spat_to_SH(torch.from_numpy(_random_bumps(s, n, rng)).to(dev))
+        init[L] = st
+        s.close()
+    stream = torch.cuda.current_stream()
+    out, finals = {}, {}
+    for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
+        groups = []
+        for L, n in ENSEMBLE:
+            s = Sph(L, precision=prec)
+            groups.append((s, Sph.swe_params(radius=6.371e6, dt=120.0 * 63 / L), init[L].clone(), None))
+        e = Ensemble(groups)
+        e.step(3)
+        for (_, _, st, _), (L, _) in zip(groups, ENSEMBLE):
+            st.copy_(init[L])
+        torch.cuda.synchronize()
+        ms = _time(lambda: e.step(ENSEMBLE_STEPS), 1, stream) / ENSEMBLE_STEPS
+        members = sum(n for _, n in ENSEMBLE)
+        out[name] = {"member_steps_per_s": members * 1000.0 / ms, "ms_per_ensemble_step": ms,
+                     "kernel_launches_per_step": e.launches}
+        finals[name] = [g[2].clone() for g in groups]
+        if name == "fp64":
+            seq = 0.0
+            for s, p, st, _ in groups:
+                st.copy_(init[s.L])
+                s.swe_rk4_batched(p, st, 3)
+                torch.cuda.synchronize()
+                seq += _time(lambda: s.swe_rk4_batched(p, st, ENSEMBLE_STEPS), 1, stream) / ENSEMBLE_STEPS
+            out[name]["ms_per_step_groups_one_after_another"] = seq
+        e.close()
+        for s, *_ in groups:
+            s.close()
+        del groups
+    rel = {}
+    for (L, n), a, b in zip(ENSEMBLE, finals["mixed"], finals["fp64"]):
+        r = (torch.linalg.vector_norm(a - b, dim=2) / torch.linalg.vector_norm(b, dim=2)).max(dim=0).values
+        rel[f"T{L}"] = {q: float(r[k]) for k, q in enumerate("huv")}
+    out["members"] = {f"T{L}": n for L, n in ENSEMBLE}
+    out["nsteps"] = ENSEMBLE_STEPS
+    out["mixed_over_fp64"] = out["mixed"]["member_steps_per_s"] / out["fp64"]["member_steps_per_s"]
+    out["mixed_max_rel_l2_vs_fp64_after_nsteps"] = rel
+    del finals, init
+    torch.cuda.empty_cache()
     return out
 
 

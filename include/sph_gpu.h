@@ -57,6 +57,7 @@ enum sph_precision {
 
 typedef struct sph_handle sph_handle;
 typedef struct sph_rexi sph_rexi;
+typedef struct sph_ensemble sph_ensemble;
 
 /* ---------------------------------------------------------------- setup */
 
@@ -175,20 +176,24 @@ typedef struct sph_swe_params {
     double h0;         /* mean depth (SimVars::h0)          */
     double viscosity;  /* nu    (SimVars::viscosity2)       */
     double dt;         /* time step (current_timestep_size) */
-    int nonlinear;     /* SimVars::use_nonlinear_equations  */
+    int nonlinear;     /* SimVars::use_nonlinear_equations: 0 linear, 1 the
+                          reference's nonlinear advective form (robert is then
+                          ignored, as AppSWE.hpp:622-650 does), 2 nonlinear
+                          equations in Robert variables U = u cos(phi),
+                          V = v cos(phi) with the metric terms (new form)     */
     int robert;        /* SimVars::use_robert_functions     */
 } sph_swe_params;
 
 /* One SWE tendency evaluation: state = [h | u | v] spectral (3*nlm complex,
  * contiguous) -> tend = [h_t | u_t | v_t].  Follows the projection points of
- * AppSWE::p_run_euler_timestep_update (AppSWE.hpp:738-823). */
+ * AppSWE::p_run_euler_timestep_update (AppSWE.hpp:574-659). */
 int sph_swe_tendency(sph_handle* h, const sph_swe_params* p, const double* state, double* tend, void* stream);
 
 /* nsteps classical RK4 steps in place on state = [h | u | v] (3*nlm complex),
  * as TimesteppingRK::run_rk_timestep order 4 (TimesteppingRK.hpp:310-392)
- * driven by AppSWE::run (AppSWE.hpp:457-499).  The step is captured once in a
+ * driven by AppSWE::run (AppSWE.hpp:293-336).  The step is captured once in a
  * CUDA graph and replayed.  Returns SPH_ERR_NAN if h became non-finite
- * (AppSWE.hpp:486-491). */
+ * (AppSWE.hpp:322-327). */
 int sph_swe_rk4(sph_handle* h, const sph_swe_params* p, double* state, int nsteps, void* stream);
 
 /* Batched ensemble: nmem independent members, state of member k at
@@ -196,6 +201,23 @@ int sph_swe_rk4(sph_handle* h, const sph_swe_params* p, double* state, int nstep
  * dt_k = dts[k] (host array, may be NULL = p->dt). */
 int sph_swe_rk4_batched(sph_handle* h, const sph_swe_params* p, const double* dts, double* state, int nmem,
                         int nsteps, void* stream);
+
+/* Ensemble of uneven truncations advanced by one CUDA graph.  Group g holds
+ * nmem[g] members of truncation handles[g]; member k of group g has its state
+ * [h | u | v] (3*nlm complex) at states[g] + 6*nlm*k doubles and its own
+ * dt = dts[g][k] (dts or dts[g] may be NULL: params[g].dt).  The step of every
+ * group is captured once, each group on its own graph branch; one replay
+ * advances all members by one RK4 step.  The reference runs one AppSWE::run
+ * (AppSWE.hpp:293-336) per member; the member arithmetic is that of
+ * sph_swe_rk4_batched.  The state pointers are bound at creation. */
+int sph_ensemble_create(int ngroups, sph_handle* const* handles, const sph_swe_params* params, double* const* states,
+                        const int* nmem, const double* const* dts, sph_ensemble** out);
+/* nsteps graph replays on stream; SPH_ERR_NAN names the groups whose h became
+ * non-finite. */
+int sph_ensemble_step(sph_ensemble* e, int nsteps, void* stream);
+/* kernel launches in one replay of the step graph */
+int sph_ensemble_launches(const sph_ensemble* e);
+int sph_ensemble_destroy(sph_ensemble* e);
 
 /* ---------------------------------------------------------------- REXI */
 
@@ -210,7 +232,7 @@ typedef struct sph_rexi_params {
 
 /* Prepare a REXI integrator for npoles poles alpha[k], beta[k] (host arrays of
  * interleaved complex).  Replaces the per-pole SWERexiSPH[Robert]::setup loop
- * (AppSWE.hpp:517-577, SWERexiSPHRobert.hpp:68-132). */
+ * (AppSWE.hpp:381-412, SWERexiSPHRobert.hpp:68-132). */
 int sph_rexi_create(sph_handle* h, const double* alpha, const double* beta, int npoles, const sph_rexi_params* p,
                     sph_rexi** out);
 int sph_rexi_destroy(sph_rexi* r);
@@ -227,7 +249,7 @@ int sph_rexi_coefficients(double h, int M, int half, int cap, double* alpha, dou
 
 /* nsteps REXI steps in place on state = [h | u | v] (3*nlm complex): all poles
  * x all m x both l-parities are solved in one launch per step; replaces the
- * serial pole loop of AppSWE::run (AppSWE.hpp:580-729) with
+ * serial pole loop of AppSWE::run (AppSWE.hpp:414-566) with
  * SWERexiSPH[Robert]::solve (SWERexiSPHRobert.hpp:139-258) and
  * SPHSolverComplex::solve -> zgbsv (SPHSolverComplex.hpp:462-511,
  * BandedMatrixSolver.hpp:416-427). */

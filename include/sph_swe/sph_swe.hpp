@@ -649,9 +649,12 @@ struct SWEParameters {
     double viscosity2 = 1e5;
     bool use_nonlinear_equations = true;
     bool use_robert_functions = false;
+    // nonlinear equations in Robert variables with the metric terms (a form the
+    // reference does not have: its nonlinear branch ignores use_robert_functions)
+    bool use_nonlinear_robert = false;
 };
 
-// nonlinear / linear RK4 of AppSWE::run (AppSWE.hpp:457-499, TimesteppingRK.hpp:310-392):
+// nonlinear / linear RK4 of AppSWE::run (AppSWE.hpp:293-336, TimesteppingRK.hpp:310-392):
 // the three fields are packed into one device state and stepped by sph_swe_rk4.
 class SWERK4 {
   public:
@@ -666,7 +669,8 @@ class SWERK4 {
     void run(SPHData& h, SPHData& u, SPHData& v, double dt, int nsteps) {
         pack(h, u, v);
         sph_swe_params sp = {p_.earth_radius, p_.gravitation, p_.coriolis_omega, p_.h0, p_.viscosity2, dt,
-                             p_.use_nonlinear_equations ? 1 : 0, p_.use_robert_functions ? 1 : 0};
+                             p_.use_nonlinear_robert ? 2 : (p_.use_nonlinear_equations ? 1 : 0),
+                             (p_.use_robert_functions || p_.use_nonlinear_robert) ? 1 : 0};
         check(sph_swe_rk4(cfg_->handle(), &sp, reinterpret_cast<double*>(state_), nsteps, cfg_->s()), "sph_swe_rk4");
         unpack(h, u, v);
     }
@@ -699,7 +703,7 @@ class SWERK4 {
     }
 };
 
-// REXI time stepping of AppSWE::run (AppSWE.hpp:500-732) with the Robert
+// REXI time stepping of AppSWE::run (AppSWE.hpp:337-568) with the Robert
 // formulation: the serial pole loop over SWERexiSPHRobert::setup/solve
 // (SWERexiSPHRobert.hpp:68-258) is one sph_rexi_step over all poles.
 class SWERexiRobert : public SWERK4 {

@@ -286,10 +286,12 @@ public:
 // ---------------------------------------------------------------- SWE app
 struct SWEParams {
     double a = 6.37122e6, g = 9.80616, omega = 7.292e-5, h0 = 1e4, visc = 0.0, dt = 120.0;
+    // nonlinear: 0 linear, 1 the reference's nonlinear advective form (robert
+    // ignored), 2 nonlinear equations in Robert variables (U, V = u, v cos(phi))
     int nonlinear = 1, robert = 0;
 };
 
-// AppSWE::p_run_euler_timestep_update (AppSWE.hpp:738-823)
+// AppSWE::p_run_euler_timestep_update (AppSWE.hpp:574-659)
 void swe_tendency(const SWEParams& p, const Field& fdata, const Field& h, const Field& u, const Field& v,
                   Field& h_t, Field& u_t, Field& v_t);
 // TimesteppingRK RK4 (TimesteppingRK.hpp:310-392)

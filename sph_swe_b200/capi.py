@@ -22,6 +22,7 @@ EXPORTS = (
     "sph_spat_to_SH", "sph_SH_to_spat", "sph_SH_to_spat_noalloc", "sph_cplx_spat_to_SH", "sph_cplx_SH_to_spat",
     "sph_vec_SH_to_spat", "sph_vec_spat_to_SH", "sph_legendre_synthesis", "sph_legendre_analysis", "sph_spec_op",
     "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched",
+    "sph_ensemble_create", "sph_ensemble_step", "sph_ensemble_launches", "sph_ensemble_destroy",
     "sph_spat_op", "sph_rexi_coefficients", "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_sync", "sph_last_error",
 )
 
@@ -73,6 +74,11 @@ def lib():
         L.sph_swe_tendency.argtypes = [vp, ctypes.POINTER(SWEParams), vp, vp, vp]
         L.sph_swe_rk4.argtypes = [vp, ctypes.POINTER(SWEParams), vp, i, vp]
         L.sph_swe_rk4_batched.argtypes = [vp, ctypes.POINTER(SWEParams), dp, vp, i, i, vp]
+        L.sph_ensemble_create.argtypes = [i, ctypes.POINTER(vp), ctypes.POINTER(SWEParams), ctypes.POINTER(vp), ip,
+                                          ctypes.POINTER(dp), ctypes.POINTER(vp)]
+        L.sph_ensemble_step.argtypes = [vp, i, vp]
+        L.sph_ensemble_launches.argtypes = [vp]
+        L.sph_ensemble_destroy.argtypes = [vp]
         L.sph_rexi_create.argtypes = [vp, dp, dp, i, ctypes.POINTER(RexiParams), ctypes.POINTER(vp)]
         L.sph_rexi_destroy.argtypes = [vp]
         L.sph_rexi_coefficients.argtypes = [d, i, i, i, dp, dp, dp, ip]

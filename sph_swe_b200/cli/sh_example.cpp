@@ -7,12 +7,15 @@
 //
 // Same single-letter flags and defaults as the reference (SimVars.hpp:14-79);
 // as in the reference, a trailing T<k> after the first argument is ignored.
-// New letters: K selects the precision form (0 FP64, 1 mixed) and D<file>
+// New values and letters: N2 selects the nonlinear equations in Robert
+// variables (U, V = u, v cos(phi), with metric terms; the reference has no such
+// form), K selects the precision form (0 FP64, 1 mixed) and D<file>
 // writes the final spectral state [h | u | v] (complex128, packed layout) to a
 // file.  Programs: P0 (shallow-water run); the reference's test programs
 // P1..P5 are not part of this driver.
 // Scenarios: Q0 the reference's Gaussian bump (AppSWE.hpp:99-128), Q10 the
 // 500 m bump at (30N, 60E) with sigma = 0.1 a of the plain-method configuration.
+// Initial velocities are zero; with Robert variables the state is U, V.
 #include <sph_swe/sph_swe.hpp>
 
 #include <algorithm>
@@ -32,7 +35,7 @@ namespace {
 struct Vars {
     int n = -1, m = -1, nlon = 0, nlat = 0;
     int program = 0;
-    bool nonlinear = true;
+    int nonlinear = 1;
     int rexi_M = 128;
     bool use_rexi = false;
     double rexi_h = 0.2;
@@ -75,7 +78,7 @@ int parse(int argc, char** argv, Vars& v) {
         switch (argv[i][0]) {
             case 'F': v.omega = std::atof(a); break;
             case 'P': v.program = std::atoi(a); break;
-            case 'N': v.nonlinear = std::atoi(a) != 0; break;
+            case 'N': v.nonlinear = std::atoi(a); break;
             case 'M': v.rexi_M = std::atoi(a); v.use_rexi = v.rexi_M > 0; break;
             case 'H': v.rexi_h = std::atof(a); break;
             case 'I': v.half_poles = std::atoi(a) != 0; break;
@@ -139,7 +142,7 @@ int main(int argc, char** argv) {
         std::printf("Using T=%d on %d x %d (nlat x nphi), precision %s\n", v.n, nlat, nphi,
                     v.precision == SPH_PREC_MIXED ? "mixed" : "fp64");
         std::printf(" + gravity %g, radius %g, h0 %g, omega %g, viscosity %g, nonlinear %d, robert %d\n", v.gravity,
-                    v.radius, v.h0, v.omega, v.visc, (int)v.nonlinear, v.robert);
+                    v.radius, v.h0, v.omega, v.visc, v.nonlinear, v.robert);
         std::printf(" + scenario %d, dt %g, end %g, REXI %d (M %d, h %g, half %d)\n", v.scenario, v.dt, v.tend,
                     (int)v.use_rexi, v.rexi_M, v.rexi_h, (int)v.half_poles);
 
@@ -155,8 +158,9 @@ int main(int argc, char** argv) {
         p.coriolis_omega = v.omega;
         p.h0 = v.h0;
         p.viscosity2 = v.visc;
-        p.use_nonlinear_equations = v.nonlinear;
+        p.use_nonlinear_equations = v.nonlinear != 0;
         p.use_robert_functions = v.robert != 0;
+        p.use_nonlinear_robert = v.nonlinear == 2;
 
         const long long nsteps = (long long)std::llround(v.tend / v.dt);
         const long long out_every = v.out_dt > 0.0 ? std::max<long long>(1, std::llround(v.out_dt / v.dt)) : nsteps;

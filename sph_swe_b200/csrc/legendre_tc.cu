@@ -32,6 +32,9 @@
 // memory and returns.
 #include "common.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstdlib>
 #include <vector>
@@ -78,6 +81,15 @@ struct MixedTables {
     int lmax = 0;
     int nhp = 0;                  // checkpoint row stride: nh rounded up to a multiple of 4 (16 B rows of ints)
     int* flag = nullptr;          // device error flag (bit 0: a wait gave up)
+    // split-TF32 P tables streamed by TMA (legendre_tcs.cuh)
+    float* S = nullptr;           // synthesis layout
+    float* A = nullptr;           // analysis layout
+    long long* soff = nullptr;    // [m] first z row of order m in S
+    long long* aoff = nullptr;    // [m] first row of order m in A
+    long long zS = 0, rowsA = 0;
+    int zA = 0;
+    bool streamed = false;
+    CUtensorMap mapS, mapA;
 };
 
 // Offsets of degree m's blocks in the coefficient and checkpoint tables of
@@ -332,6 +344,9 @@ __global__ void k_tc_ck(int nh, int nhp, int lmax, int mm, const double* __restr
     }
 }
 
+static int tcs_tables_build(Handle* h, MixedTables* T);
+static bool g_tc_stream = true;
+
 int tc_tables_build(Handle* h, int lmax) {
     if (h->mixed) return SPH_OK;
     MixedTables* T = new MixedTables();
@@ -351,6 +366,8 @@ int tc_tables_build(Handle* h, int lmax) {
     SPH_CUDA_TRY(cudaGetLastError());
     k_tc_ck<<<dim3((nh + 127) / 128, mm + 1), 128>>>(nh, T->nhp, lmax, mm, h->mu, T->ab, T->ck, T->ckx);
     SPH_CUDA_TRY(cudaGetLastError());
+    if (g_tc_stream)
+        if (int rc = tcs_tables_build(h, T)) return rc;
     SPH_CUDA_TRY(cudaDeviceSynchronize());
     return SPH_OK;
 }
@@ -358,7 +375,7 @@ int tc_tables_build(Handle* h, int lmax) {
 void tc_tables_free(Handle* h) {
     MixedTables* T = static_cast<MixedTables*>(h->mixed);
     if (!T) return;
-    void* bufs[] = {T->ab, T->ck, T->ckx, T->flag};
+    void* bufs[] = {T->ab, T->ck, T->ckx, T->flag, T->S, T->A, T->soff, T->aoff};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete T;
@@ -1001,8 +1018,69 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
     }
 }
 
+#include "legendre_tcs.cuh"
+
+static int encode_map(CUtensorMap* map, float* base, unsigned long long d1, unsigned long long d2) {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* f = nullptr;
+        SPH_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+        if (!f || q != cudaDriverEntryPointSuccess) {
+            set_error("cuTensorMapEncodeTiled is not available");
+            return SPH_ERR_CUDA;
+        }
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    // dims (x = 4 floats, d1 rows, d2 slices, 2 parts); box 4 x 128 x 4 x 2
+    const cuuint64_t dims[4] = {4, d1, d2, 2};
+    const cuuint64_t strides[3] = {16, 16ull * d1, 16ull * d1 * d2};
+    const cuuint32_t box[4] = {4, (cuuint32_t)tc::M, 4, 2};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+        return SPH_ERR_CUDA;
+    }
+    return SPH_OK;
+}
+
+static int tcs_tables_build(Handle* h, MixedTables* T) {
+    const int tl = T->lmax, nh = h->nh, mm = std::min(tl, h->L);
+    std::vector<long long> so(mm + 2, 0), ao(mm + 2, 0);
+    for (int m = 0; m <= mm; m++) {
+        so[m + 1] = so[m] + 8LL * tcs_nchunks(tl, m);
+        ao[m + 1] = ao[m] + tcs_nlp(tl, m, 0) + tcs_nlp(tl, m, 1);
+    }
+    T->zS = so[mm + 1];
+    T->rowsA = ao[mm + 1];
+    T->zA = (nh + 3) / 4;
+    const size_t bs = sizeof(float) * 2 * (size_t)T->zS * nh * 4, ba = sizeof(float) * 2 * (size_t)T->zA * T->rowsA * 4;
+    SPH_CUDA_TRY(cudaMalloc(&T->S, bs));
+    SPH_CUDA_TRY(cudaMalloc(&T->A, ba));
+    SPH_CUDA_TRY(cudaMemset(T->S, 0, bs));
+    SPH_CUDA_TRY(cudaMemset(T->A, 0, ba));
+    SPH_CUDA_TRY(cudaMalloc(&T->soff, sizeof(long long) * (mm + 2)));
+    SPH_CUDA_TRY(cudaMalloc(&T->aoff, sizeof(long long) * (mm + 2)));
+    SPH_CUDA_TRY(cudaMemcpy(T->soff, so.data(), sizeof(long long) * (mm + 2), cudaMemcpyHostToDevice));
+    SPH_CUDA_TRY(cudaMemcpy(T->aoff, ao.data(), sizeof(long long) * (mm + 2), cudaMemcpyHostToDevice));
+    k_tcs_tables<<<dim3((nh + 127) / 128, mm + 1), 128>>>(nh, tl, mm, h->mu, T->soff, T->aoff, T->zS, T->rowsA, T->zA,
+                                                          T->S, T->A);
+    SPH_CUDA_TRY(cudaGetLastError());
+    if (int rc = encode_map(&T->mapS, T->S, (unsigned long long)nh, (unsigned long long)T->zS)) return rc;
+    if (int rc = encode_map(&T->mapA, T->A, (unsigned long long)T->rowsA, (unsigned long long)T->zA)) return rc;
+    T->streamed = true;
+    return SPH_OK;
+}
+
 template <int NC>
 static int tc_attr() {
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tcs<SynS<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, tss::BYTES));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tcs<AnaS<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, tss::BYTES));
     const int bytes = (int)tc_smem_bytes();
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tc<SynDir<NC>, NC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -1020,6 +1098,9 @@ int tc_kernels_init() {
     SPH_CUDA_TRY(cudaDeviceGetAttribute(&g_tc_sms, cudaDevAttrMultiProcessorCount, dev));
     // chunks per FP32 accumulation group: 1 (default, each 16-term chunk folded into FP64) or 2
     if (const char* e = getenv("SPH_TC_GROUP")) g_tc_group = atoi(e) == 2 ? 2 : 1;
+    // P_l^m operand: streamed from split-TF32 tables by TMA (default) or
+    // regenerated from recurrence checkpoints (SPH_TC_STREAM=0)
+    if (const char* e = getenv("SPH_TC_STREAM")) g_tc_stream = atoi(e) != 0;
     if (int rc = tc_attr<16>()) return rc;
     if (int rc = tc_attr<32>()) return rc;
     return tc_attr<64>();
@@ -1072,13 +1153,51 @@ static int tc_launch(TcArgs& a, int nrt, int nm, const double2* in, double2* out
     return SPH_OK;
 }
 
+static TsArgs make_sargs(const Handle* h, const MixedTables* T, int lmax, int batch, long long ld_spec, long long ldF) {
+    TsArgs a;
+    a.soff = T->soff;
+    a.aoff = T->aoff;
+    a.w = h->w;
+    a.tlmax = T->lmax;
+    a.lmax = lmax;
+    a.nh = h->nh;
+    a.nlat = h->nlat;
+    a.batch = batch;
+    a.nct = a.nrt = a.ntiles = 0;
+    a.group = g_tc_group;
+    a.ld_spec = ld_spec;
+    a.ldF = ldF;
+    a.flag = T->flag;
+    return a;
+}
+
+template <template <int> class Dir>
+static int tcs_launch(const CUtensorMap& map, TsArgs& a, int nrt, int nm, const double2* in, double2* out,
+                      cudaStream_t s) {
+    const int nc = tc_cols(a.batch);
+    a.nct = (2 * a.batch + nc - 1) / nc;
+    a.nrt = nrt;
+    a.ntiles = a.nct * nrt * nm;
+    const int grid = std::max(1, std::min(a.ntiles, g_tc_sms > 0 ? g_tc_sms : 148));
+    if (nc == 16) k_legendre_tcs<Dir<16>, 16><<<grid, tss::NT, tss::BYTES, s>>>(map, a, in, out);
+    else if (nc == 32) k_legendre_tcs<Dir<32>, 32><<<grid, tss::NT, tss::BYTES, s>>>(map, a, in, out);
+    else k_legendre_tcs<Dir<64>, 64><<<grid, tss::NT, tss::BYTES, s>>>(map, a, in, out);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
 int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F, long long ldF,
                           int batch, cudaStream_t s) {
     const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
     if (int rc = check_tables(T, lmax)) return rc;
     if (batch <= 0) return SPH_OK;
+    const int nrt = (h->nh + tc::M - 1) / tc::M, nm = std::min(lmax, h->L) + 1;
+    if (T->streamed) {
+        TsArgs a = make_sargs(h, T, lmax, batch, ld_spec, ldF);
+        return tcs_launch<SynS>(T->mapS, a, nrt, nm, spec, F, s);
+    }
     TcArgs a = make_args(h, T, lmax, batch, ld_spec, ldF);
-    return tc_launch<SynDir>(a, (h->nh + tc::M - 1) / tc::M, std::min(lmax, h->L) + 1, spec, F, s);
+    return tc_launch<SynDir>(a, nrt, nm, spec, F, s);
 }
 
 int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec, int lmax,
@@ -1086,8 +1205,13 @@ int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, doubl
     const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
     if (int rc = check_tables(T, lmax)) return rc;
     if (batch <= 0) return SPH_OK;
+    const int nrt = lmax / (2 * tc::M) + 1, nm = std::min(lmax, h->L) + 1;
+    if (T->streamed) {
+        TsArgs a = make_sargs(h, T, lmax, batch, ld_spec, ldF);
+        return tcs_launch<AnaS>(T->mapA, a, nrt, nm, F, spec, s);
+    }
     TcArgs a = make_args(h, T, lmax, batch, ld_spec, ldF);
-    return tc_launch<AnaDir>(a, lmax / (2 * tc::M) + 1, std::min(lmax, h->L) + 1, F, spec, s);
+    return tc_launch<AnaDir>(a, nrt, nm, F, spec, s);
 }
 
 int tc_check(const Handle* h) {

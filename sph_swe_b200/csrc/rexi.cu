@@ -1,7 +1,7 @@
 // REXI time integrator for the linear shallow-water equations, Robert
 // formulation (SWERexiSPHRobert.hpp), FP64 direct.
 //
-// Reference per step (AppSWE.hpp:580-729): for every pole (alpha_k, beta_k)
+// Reference per step (AppSWE.hpp:414-566): for every pole (alpha_k, beta_k)
 // SWERexiSPHRobert::solve (SWERexiSPHRobert.hpp:139-258) promotes phi0 = g h,
 // u0, v0 to complex fields, builds a right-hand side from mu / mu^2 / (1-mu^2)d/dmu
 // recurrences, solves one banded system per zonal wavenumber m for phi

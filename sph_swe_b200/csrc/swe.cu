@@ -1,6 +1,6 @@
 // Fused RK4 shallow-water step on the sphere (FP64 plain method).
 //
-// Reference: AppSWE::p_run_euler_timestep_update (AppSWE.hpp:738-823) driven
+// Reference: AppSWE::p_run_euler_timestep_update (AppSWE.hpp:574-659) driven
 // by TimesteppingRK::run_rk_timestep order 4 (TimesteppingRK.hpp:310-392).
 // The reference evaluates every operator through lazily transformed fields;
 // the projection points it produces for the nonlinear advective form are
@@ -23,11 +23,18 @@
 //   W3  spectral: A = F(HU), B = D F(cHV); Legendre synthesis (2 fields);
 //       Fourier-space latitude scaling i m A/c + B/c^2 (no FFT needed)
 //   W4  Legendre analysis of the h term; combine into the RK stage.
-// The linear forms (AppSWE.hpp:754-785) use the same waves with h0 in place
+// The linear forms (AppSWE.hpp:590-621) use the same waves with h0 in place
 // of H in the flux products and no advection terms; the Robert linear form
 // divides by c^2 and takes the geopotential gradient in spectral space.
 // With nonlinear = 1 the reference ignores use_robert_functions
-// (AppSWE.hpp:786-813) and so does this file.
+// (AppSWE.hpp:622-650) and so does this file.  nonlinear = 2 selects the
+// nonlinear equations in Robert variables U = u cos(phi), V = v cos(phi), with
+// the metric terms (no reference counterpart):
+//   h_t = -(1/a) F( [I(iM F(hU)) + I(D F(hV))] / c^2 )
+//   U_t = -(g/a) iM h + F(f V) - (1/a) F( [U U_l + V U_m] / c^2 )
+//   V_t = -(g/a) D h  - F(f U) - (1/a) F( [U V_l + V V_m + mu (U^2 + V^2)] / c^2 )
+// (U_l, U_m = grids of iM U and D U), through the same waves as the
+// advective form with the Robert linear form's spectral gradient.
 // The whole step (4 stages + update) is captured once in a CUDA graph.
 #include "common.cuh"
 #include "identities.cuh"
@@ -59,8 +66,7 @@ struct RKState {
     std::vector<double> dts_h;
 };
 
-void rk_free(Handle* h) {
-    RKState* r = static_cast<RKState*>(h->rk);
+static void rk_release(RKState* r) {
     if (!r) return;
     if (r->exec) cudaGraphExecDestroy(r->exec);
     if (r->graph) cudaGraphDestroy(r->graph);
@@ -68,16 +74,10 @@ void rk_free(Handle* h) {
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete r;
-    h->rk = nullptr;
 }
 
-static int rk_alloc(Handle* h, int nmem) {
-    RKState* r = static_cast<RKState*>(h->rk);
-    if (r && r->nmem >= nmem) return SPH_OK;
-    cudaDeviceSynchronize();
-    rk_free(h);
-    r = new RKState();
-    h->rk = r;
+// stage buffers for nmem members of one truncation
+static int rk_buffers(const Handle* h, RKState* r, int nmem) {
     r->nmem = nmem;
     const size_t nlm = h->nlm, fou = (size_t)(h->L + 1) * h->nlat, sp = h->nspat;
     const size_t M = nmem;
@@ -98,11 +98,26 @@ static int rk_alloc(Handle* h, int nmem) {
     return SPH_OK;
 }
 
+void rk_free(Handle* h) {
+    rk_release(static_cast<RKState*>(h->rk));
+    h->rk = nullptr;
+}
+
+static int rk_alloc(Handle* h, int nmem) {
+    RKState* r = static_cast<RKState*>(h->rk);
+    if (r && r->nmem >= nmem) return SPH_OK;
+    cudaDeviceSynchronize();
+    rk_free(h);
+    r = new RKState();
+    h->rk = r;
+    return rk_buffers(h, r, nmem);
+}
+
 // ------------------------------------------------------------------ kernels
 // index helpers for the real packed layout: block y = m, threads over n
 struct SweConst {
     double a, g, omega, h0, visc;
-    int mode;  // 0 nonlinear, 1 linear, 2 linear Robert
+    int mode;  // 0 nonlinear, 1 linear, 2 linear Robert, 3 nonlinear Robert
 };
 
 __device__ __forceinline__ double2 ld2(const double2* p, int L, int n, int m) {
@@ -165,6 +180,14 @@ __global__ void k_swe_pointwise(const double* __restrict__ G9, double* __restric
         B = k.h0 * (c * V);
         ut = -ga * (Hl / c) + to * (m_ * V);
         vt = -ga * (Hm / c) - to * (m_ * U);
+    } else if (k.mode == 3) {
+        // Robert variables: U, V here are u cos(phi), v cos(phi); Ul, Um their
+        // longitude derivative and (1-mu^2) d/dmu; mu (U^2 + V^2) is the metric term
+        const double ic2 = 1.0 / (c * c);
+        A = H * U;
+        B = H * V;
+        ut = to * (m_ * V) - ia * ((U * Ul + V * Um) * ic2);
+        vt = -to * (m_ * U) - ia * ((U * Vl + V * Vm + m_ * (U * U + V * V)) * ic2);
     } else {
         A = k.h0 * U;
         B = k.h0 * V;
@@ -242,8 +265,8 @@ __global__ void k_rk_stage_out(const double2* __restrict__ S, const double2* __r
     double2 ut = t4[2 * (size_t)nlm + k];
     double2 vt = t4[3 * (size_t)nlm + k];
     const double dn = n, dm = m;
-    if (kc.mode == 2) {
-        // -(g/a) iM h  and  -(g/a) D h in spectral space
+    if (kc.mode >= 2) {
+        // Robert forms: -(g/a) iM h  and  -(g/a) D h in spectral space
         const double ga = kc.g / kc.a;
         const double2 xh = x_at(0, n), lo = x_at(0, n - 1), hi = x_at(0, n + 1);
         ut.x += -ga * (-dm * xh.y);
@@ -292,7 +315,7 @@ static SweConst make_const(const sph_swe_params* p) {
     k.omega = p->omega;
     k.h0 = p->h0;
     k.visc = p->viscosity;
-    k.mode = p->nonlinear ? 0 : (p->robert ? 2 : 1);
+    k.mode = p->nonlinear == 2 ? 3 : (p->nonlinear ? 0 : (p->robert ? 2 : 1));
     return k;
 }
 
@@ -317,7 +340,7 @@ static int swe_stage(Handle* h, RKState* r, const sph_swe_params* p, const doubl
     SPH_CUDA_TRY(cudaGetLastError());
     if (int rc = legendre_synthesis_real(h, r->X2, nlm, L, r->F2, fou, 2 * nmem, s)) return rc;
     k_fourier_h<<<dim3((unsigned)((fou + 255) / 256), nmem), 256, 0, s>>>(r->F2, r->Fh, h->cosphi, nlat, mF,
-                                                                          kc.mode == 2 ? 2 : 1);
+                                                                          kc.mode >= 2 ? 2 : 1);
     SPH_CUDA_TRY(cudaGetLastError());
     if (int rc = legendre_analysis_real(h, r->Fh, fou, r->Th, nlm, L, nmem, s)) return rc;
     k_rk_stage_out<<<dim3((L + 1 + 63) / 64, L + 1, nmem), 64, 0, s>>>(S, Kp, coef, r->dts, r->T4, r->Th, Ks, L, nlm, kc);
@@ -393,6 +416,153 @@ static int rk_run(Handle* h, const sph_swe_params* p, const double* dts_h, doubl
         set_error("sph_swe_rk4: instability detected (non-finite value in h)");
         return SPH_ERR_NAN;
     }
+    return tc_check(h);
+}
+
+// ------------------------------------------------------------------ ensembles
+// Members of several truncations advanced by one CUDA graph.  Group g is the
+// batched RK4 step of its handle over nmem[g] members stored contiguously at
+// states[g]; each group is captured on its own branch (fork and join events on
+// private streams), so one replay advances every member by one step and the
+// groups' kernels may overlap where a launch leaves SMs idle (the small
+// truncations' launches are latency-bound).  Every group owns its stage
+// buffers, so a handle's own sph_swe_rk4 graph is not disturbed.
+struct EnsembleGroup {
+    Handle* h = nullptr;
+    RKState* r = nullptr;
+    sph_swe_params p{};
+    double* state = nullptr;
+    int nmem = 0;
+};
+
+struct Ensemble {
+    std::vector<EnsembleGroup> g;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+};
+
+static void ensemble_release(Ensemble* e) {
+    if (!e) return;
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    for (auto& g : e->g) rk_release(g.r);
+    delete e;
+}
+
+// streams and events of one capture, released on every return path
+struct CaptureStreams {
+    cudaStream_t cap = nullptr;
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> ev;  // ev[0]: fork; ev[1 + g]: join of group g
+    ~CaptureStreams() {
+        for (cudaStream_t x : side)
+            if (x) cudaStreamDestroy(x);
+        if (cap) cudaStreamDestroy(cap);
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
+static int ensemble_capture(Ensemble* e) {
+    const int ng = (int)e->g.size();
+    CaptureStreams cs;
+    cs.side.assign(ng, nullptr);
+    cs.ev.assign(ng + 1, nullptr);
+    SPH_CUDA_TRY(cudaStreamCreateWithFlags(&cs.cap, cudaStreamNonBlocking));
+    for (int i = 0; i < ng; i++) SPH_CUDA_TRY(cudaStreamCreateWithFlags(&cs.side[i], cudaStreamNonBlocking));
+    for (cudaEvent_t& x : cs.ev) SPH_CUDA_TRY(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    SPH_CUDA_TRY(cudaStreamBeginCapture(cs.cap, cudaStreamCaptureModeThreadLocal));
+    int rc = SPH_OK;
+    cudaError_t ce = cudaEventRecord(cs.ev[0], cs.cap);
+    for (int i = 0; i < ng && rc == SPH_OK && ce == cudaSuccess; i++) {
+        EnsembleGroup& g = e->g[i];
+        ce = cudaStreamWaitEvent(cs.side[i], cs.ev[0], 0);
+        if (ce != cudaSuccess) break;
+        rc = swe_step(g.h, g.r, &g.p, reinterpret_cast<double2*>(g.state), g.nmem, cs.side[i]);
+        if (rc != SPH_OK) break;
+        ce = cudaEventRecord(cs.ev[1 + i], cs.side[i]);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cs.cap, cs.ev[1 + i], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(cs.cap, &graph);
+    if (rc != SPH_OK || ce != cudaSuccess || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc != SPH_OK) return rc;
+        set_error(std::string("ensemble graph capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+        return SPH_ERR_CUDA;
+    }
+    e->graph = graph;
+    size_t nodes = 0;
+    SPH_CUDA_TRY(cudaGraphGetNodes(graph, nullptr, &nodes));
+    std::vector<cudaGraphNode_t> list(nodes);
+    if (nodes) SPH_CUDA_TRY(cudaGraphGetNodes(graph, list.data(), &nodes));
+    e->launches = 0;
+    for (cudaGraphNode_t n : list) {
+        cudaGraphNodeType t;
+        SPH_CUDA_TRY(cudaGraphNodeGetType(n, &t));
+        if (t == cudaGraphNodeTypeKernel) e->launches++;
+    }
+    SPH_CUDA_TRY(cudaGraphInstantiate(&e->exec, graph, 0));
+    return SPH_OK;
+}
+
+static int ensemble_create(int ngroups, sph_handle* const* handles, const sph_swe_params* params,
+                           double* const* states, const int* nmem, const double* const* dts, Ensemble** out) {
+    if (!out || ngroups <= 0 || !handles || !params || !states || !nmem) {
+        set_error("sph_ensemble_create: bad arguments");
+        return SPH_ERR_ARG;
+    }
+    *out = nullptr;
+    for (int i = 0; i < ngroups; i++) {
+        if (!handles[i] || !states[i] || nmem[i] <= 0 || nmem[i] > 65535 / 9) {
+            set_error("sph_ensemble_create: group " + std::to_string(i) +
+                      ": needs a handle, a state and 1 .. 7281 members");
+            return SPH_ERR_ARG;
+        }
+    }
+    Ensemble* e = new Ensemble();
+    e->g.resize(ngroups);
+    for (int i = 0; i < ngroups; i++) {
+        EnsembleGroup& g = e->g[i];
+        g.h = reinterpret_cast<Handle*>(handles[i]);
+        g.p = params[i];
+        g.state = states[i];
+        g.nmem = nmem[i];
+        g.r = new RKState();
+        if (int rc = rk_buffers(g.h, g.r, g.nmem)) { ensemble_release(e); return rc; }
+        std::vector<double> d(g.nmem);
+        for (int k = 0; k < g.nmem; k++) d[k] = (dts && dts[i]) ? dts[i][k] : g.p.dt;
+        const cudaError_t ce = cudaMemcpy(g.r->dts, d.data(), sizeof(double) * g.nmem, cudaMemcpyHostToDevice);
+        if (ce != cudaSuccess) {
+            set_error(std::string("sph_ensemble_create: ") + cudaGetErrorString(ce));
+            ensemble_release(e);
+            return SPH_ERR_CUDA;
+        }
+    }
+    if (int rc = ensemble_capture(e)) { ensemble_release(e); return rc; }
+    *out = e;
+    return SPH_OK;
+}
+
+static int ensemble_run(Ensemble* e, int nsteps, cudaStream_t s) {
+    if (!e || nsteps < 0) { set_error("sph_ensemble_step: bad arguments"); return SPH_ERR_ARG; }
+    const int ng = (int)e->g.size();
+    for (auto& g : e->g) SPH_CUDA_TRY(cudaMemsetAsync(g.r->flag, 0, sizeof(int), s));
+    for (int i = 0; i < nsteps; i++) SPH_CUDA_TRY(cudaGraphLaunch(e->exec, s));
+    std::vector<int> flags(ng, 0);
+    for (int i = 0; i < ng; i++)
+        SPH_CUDA_TRY(cudaMemcpyAsync(&flags[i], e->g[i].r->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPH_CUDA_TRY(cudaStreamSynchronize(s));
+    std::string bad;
+    for (int i = 0; i < ng; i++)
+        if (flags[i]) bad += (bad.empty() ? "" : ", ") + std::to_string(i);
+    if (!bad.empty()) {
+        set_error("sph_ensemble_step: instability detected (non-finite value in h) in group(s) " + bad);
+        return SPH_ERR_NAN;
+    }
+    for (auto& g : e->g)
+        if (int rc = tc_check(g.h)) return rc;
     return SPH_OK;
 }
 
@@ -428,6 +598,29 @@ int sph_swe_rk4_batched(sph_handle* hh, const sph_swe_params* p, const double* d
     Handle* h = reinterpret_cast<Handle*>(hh);
     if (!h) { set_error("sph_swe_rk4_batched: NULL handle"); return SPH_ERR_ARG; }
     return rk_run(h, p, dts, state, nmem, nsteps, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int sph_ensemble_create(int ngroups, sph_handle* const* handles, const sph_swe_params* params, double* const* states,
+                        const int* nmem, const double* const* dts, sph_ensemble** out) {
+    Ensemble* e = nullptr;
+    const int rc = ensemble_create(ngroups, handles, params, states, nmem, dts, &e);
+    if (out) *out = reinterpret_cast<sph_ensemble*>(e);
+    return rc;
+}
+
+int sph_ensemble_step(sph_ensemble* e, int nsteps, void* stream) {
+    return ensemble_run(reinterpret_cast<Ensemble*>(e), nsteps, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int sph_ensemble_launches(const sph_ensemble* e) {
+    return e ? reinterpret_cast<const Ensemble*>(e)->launches : 0;
+}
+
+int sph_ensemble_destroy(sph_ensemble* e) {
+    if (!e) return SPH_OK;
+    cudaDeviceSynchronize();
+    ensemble_release(reinterpret_cast<Ensemble*>(e));
+    return SPH_OK;
 }
 
 }  // extern "C"

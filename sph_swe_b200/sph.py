@@ -207,3 +207,50 @@ class Rexi:
             self.close()
         except Exception:
             pass
+
+
+class Ensemble:
+    """Members of several truncations advanced by one CUDA graph.
+
+    groups: list of (sph, params, state, dts) with state a contiguous
+    complex128 tensor of shape (nmem, 3, nlm) on the device (bound at creation,
+    stepped in place) and dts a per-member array or None (params.dt)."""
+
+    def __init__(self, groups):
+        n = len(groups)
+        vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        self._keep = []
+        handles = (vp * n)(*[g[0].h for g in groups])
+        params = (capi.SWEParams * n)(*[g[1] for g in groups])
+        states = (vp * n)(*[g[2].data_ptr() for g in groups])
+        nmem = (ctypes.c_int * n)(*[g[2].numel() // (3 * g[0].nlm) for g in groups])
+        dts = (dp * n)()
+        for k, g in enumerate(groups):
+            if g[0].nlm * 3 * nmem[k] != g[2].numel() or not g[2].is_contiguous():
+                raise ValueError(f"group {k}: state must be contiguous (nmem, 3, nlm)")
+            if g[3] is not None:
+                arr = np.ascontiguousarray(g[3], np.float64)
+                self._keep.append(arr)
+                dts[k] = arr.ctypes.data_as(dp)
+        self.groups = groups
+        e = ctypes.c_void_p()
+        capi.check(capi.lib().sph_ensemble_create(n, handles, params, states, nmem, dts, ctypes.byref(e)))
+        self.e = e
+
+    @property
+    def launches(self) -> int:
+        return capi.lib().sph_ensemble_launches(self.e)
+
+    def step(self, nsteps: int = 1):
+        capi.check(capi.lib().sph_ensemble_step(self.e, nsteps, _stream()))
+
+    def close(self):
+        if getattr(self, "e", None):
+            capi.lib().sph_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

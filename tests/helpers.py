@@ -73,3 +73,21 @@ def bump_state(grid, amp=500.0, lat0_deg=30.0, lon0_deg=60.0, sigma_frac=0.1, h0
         return h0 + amp * np.exp(-(d / sigma_frac) ** 2)
 
     return grid.grid_from(f)
+
+
+def random_bumps(grid, n, rng, h0=1e4):
+    """n grids h0 + A exp(-(d/sigma)^2): A ~ U(100, 800) m, centre uniform on
+    the sphere (sin(lat) ~ U(-1, 1), lon ~ U(0, 2 pi)), sigma ~ U(0.05, 0.2)
+    radians; returns an array (n, nphi, nlat)."""
+    out = []
+    for _ in range(n):
+        amp, z, lon0, sig = rng.uniform(100, 800), rng.uniform(-1, 1), rng.uniform(0, 2 * np.pi), rng.uniform(0.05, 0.2)
+        lat0 = np.arcsin(z)
+
+        def f(lon, mu, lat0=lat0, lon0=lon0, amp=amp, sig=sig):
+            p = np.arcsin(mu)
+            c = np.sin(p) * np.sin(lat0) + np.cos(p) * np.cos(lat0) * np.cos(lon - lon0)
+            return h0 + amp * np.exp(-(np.arccos(np.clip(c, -1, 1)) / sig) ** 2)
+
+        out.append(grid.grid_from(f))
+    return np.stack(out)

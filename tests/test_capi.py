@@ -50,6 +50,12 @@ def test_error_reporting_without_gpu(lib):
     assert rc == capi.SPH_ERR_ARG
     assert "lmax == mmax" in capi.last_error()
     assert lib.sph_info(None, None, None, None, None, None) == capi.SPH_ERR_ARG
+    e = ctypes.c_void_p()
+    assert lib.sph_ensemble_create(0, None, None, None, None, None, ctypes.byref(e)) == capi.SPH_ERR_ARG
+    assert "sph_ensemble_create" in capi.last_error()
+    assert lib.sph_ensemble_step(None, 1, None) == capi.SPH_ERR_ARG
+    assert lib.sph_ensemble_launches(None) == 0
+    assert lib.sph_ensemble_destroy(None) == capi.SPH_OK
 
 
 @pytest.mark.parametrize("M,half", [(64, False), (256, False), (256, True), (32, True)])

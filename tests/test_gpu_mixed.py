@@ -113,3 +113,37 @@ def test_reuse_and_sync_stay_clean(gpu):
         again = s.SH_to_spat(x)
     _sync_ok(s)
     assert torch.equal(first, again)
+
+
+_GEN_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from oracle import oracle as O
+from sph_swe_b200 import capi
+from sph_swe_b200.sph import Sph
+from tests.helpers import random_spec, rel_l2
+L, nb = 127, 20
+s, g = Sph(L, precision=capi.SPH_PREC_MIXED), O.Grid(L)
+spec = random_spec(L, nb, seed=3)
+ref = g.SH_to_spat(spec)
+out = s.SH_to_spat(torch.from_numpy(spec).cuda()).cpu().numpy()
+back = s.spat_to_SH(torch.from_numpy(ref).cuda()).cpu().numpy()
+assert capi.lib().sph_sync(s.h, None) == 0
+ana = g.spat_to_SH(ref)
+print(max(rel_l2(out[b], ref[b]) for b in range(nb)), max(rel_l2(back[b], ana[b]) for b in range(nb)))
+"""
+
+
+def test_checkpoint_generator_path_vs_oracle(gpu):
+    """The P operand regenerated on the CUDA cores from recurrence checkpoints
+    (SPH_TC_STREAM=0) instead of streamed from the split tables."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, SPH_TC_STREAM="0", PYTHONPATH=root)
+    r = subprocess.run([sys.executable, "-c", _GEN_SCRIPT, root], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    syn, ana = (float(x) for x in r.stdout.split()[-2:])
+    assert syn < TOL and ana < TOL

@@ -1,5 +1,5 @@
 """Parity of the CUDA RK4 shallow-water path with the oracle, which follows
-the reference's lazy-field projection points (AppSWE.hpp:738-823,
+the reference's lazy-field projection points (AppSWE.hpp:574-659,
 TimesteppingRK.hpp:310-392).  Tolerance: relative L2 <= 1e-10 on h, u, v."""
 import numpy as np
 import pytest
