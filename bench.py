@@ -347,8 +347,11 @@ def rk4_rates(dev, args):
     # T255: the reference's non-Robert advective form is unstable at dt = 30 s
     # (the oracle diverges within 60 steps); dt = 10 s with the reference's
     # default viscosity 1e5 runs stably.  T63: the plain-method configuration.
+    # T255_vort_div: the vorticity-divergence form (state [h, zeta, delta]),
+    # stable at dt = 60 s without viscosity.
     out = {}
-    for L, dt, visc, n in ((255, 10.0, 1e5, 50), (63, 120.0, 0.0, 200)):
+    for key, L, dt, visc, n, form in (("T255", 255, 10.0, 1e5, 50, 1), ("T63", 63, 120.0, 0.0, 200, 1),
+                                      ("T255_vort_div", 255, 60.0, 0.0, 50, 2)):
         res = {}
         states = {}
         s0 = Sph(L)
@@ -356,7 +359,7 @@ def rk4_rates(dev, args):
         s0.close()
         for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
             s = Sph(L, precision=prec)
-            p = Sph.swe_params(radius=6.371e6, dt=dt, viscosity=visc)
+            p = Sph.swe_params(radius=6.371e6, dt=dt, viscosity=visc, nonlinear=form)
             st = st0.clone()
             s.swe_rk4(p, st, 3)
             torch.cuda.synchronize()
@@ -365,12 +368,14 @@ def rk4_rates(dev, args):
             capi.check(capi.lib().sph_sync(s.h, None))
             states[name] = st
             res[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms}
+            launches = capi.lib().sph_swe_rk4_launches(s.h)
             s.close()
+        names = ("h", "u", "v") if form == 1 else ("h", "vorticity", "divergence")
         rel = {q: float(torch.linalg.vector_norm(states["mixed"][k] - states["fp64"][k]) /
-                        torch.linalg.vector_norm(states["fp64"][k])) for k, q in enumerate("huv")}
-        out[f"T{L}"] = {**res, "mixed_over_fp64": res["mixed"]["steps_per_s"] / res["fp64"]["steps_per_s"],
-                        "nsteps": n, "dt": dt, "viscosity": visc, "mixed_rel_l2_vs_fp64_after_nsteps": rel,
-                        "kernel_launches_per_step": 4 * 11 + 1}
+                        max(float(torch.linalg.vector_norm(states["fp64"][k])), 1e-300)) for k, q in enumerate(names)}
+        out[key] = {**res, "mixed_over_fp64": res["mixed"]["steps_per_s"] / res["fp64"]["steps_per_s"],
+                    "nsteps": n, "dt": dt, "viscosity": visc, "mixed_rel_l2_vs_fp64_after_nsteps": rel,
+                    "kernel_launches_per_step": launches}
     return out
 
 
@@ -402,27 +407,29 @@ def rexi_rates(dev, args):
 
 
 def t1023_rates(dev, args):
-    """T1023 configuration: 1536 x 3072 Gauss grid, nonlinear equations in
-    Robert variables, zonal jet 80 sech^2((phi - 45 deg)/0.1) m/s with h in
-    gradient-wind balance (mean 1e4 m) plus a 120 m bump at (30N, 60E),
-    dt = 15 s, 50 steps; FP64 and mixed form, mass drift (Y_00 of h)."""
+    """T1023 configuration: 1536 x 3072 Gauss grid, full nonlinear equations in
+    vorticity-divergence form with Robert velocities on the grid, zonal jet
+    80 sech^2((phi - 45 deg)/0.1) m/s with h in gradient-wind balance (mean
+    1e4 m) plus a 120 m bump at (30N, 60E), dt = 15 s, 50 steps; FP64 and
+    mixed form; relative L2 of h and vorticity of the mixed form against the
+    FP64 form, and the mass drift (Y_00 of h) of each."""
     import torch
 
     from sph_swe_b200 import capi, scenarios
     from sph_swe_b200.sph import Sph
 
-    L, n, dt = 1023, 50, 15.0
+    L, n, dt, a = 1023, 50, 15.0, 6.371e6
     res, states = {}, {}
     st0 = None
     for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
         s = Sph(L, precision=prec)
         if st0 is None:
-            h, u, v = scenarios.sech2_jet(s, radius=6.371e6, bump_amp=120.0)
+            h, u, v = scenarios.sech2_jet(s, radius=a, bump_amp=120.0)
             c = torch.from_numpy(np.cos(s.lat)).to(dev)[None, :]
-            st0 = torch.stack([s.spat_to_SH(torch.from_numpy(h).to(dev)),
-                               s.spat_to_SH(torch.from_numpy(u).to(dev) * c),
-                               s.spat_to_SH(torch.from_numpy(v).to(dev) * c)])
-        p = Sph.swe_params(radius=6.371e6, dt=dt, nonlinear=2, robert=1)
+            z, d = s.vec_spat_to_SH(torch.from_numpy(u[None]).to(dev) * c, torch.from_numpy(v[None]).to(dev) * c,
+                                    robert=True)
+            st0 = torch.stack([s.spat_to_SH(torch.from_numpy(h).to(dev)), z[0] / a, d[0] / a])
+        p = Sph.swe_params(radius=a, dt=dt, nonlinear=2)
         st = st0.clone()
         s.swe_rk4(p, st, 3)
         torch.cuda.synchronize()
@@ -431,12 +438,14 @@ def t1023_rates(dev, args):
         capi.check(capi.lib().sph_sync(s.h, None))
         m0, m1 = st0[0, 0].real.item(), st[0, 0].real.item()
         res[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms, "mass_drift_rel": abs(m1 - m0) / abs(m0)}
+        launches = capi.lib().sph_swe_rk4_launches(s.h)
         states[name] = st
         s.close()
     rel = {q: float(torch.linalg.vector_norm(states["mixed"][k] - states["fp64"][k]) /
-                    torch.linalg.vector_norm(states["fp64"][k])) for k, q in enumerate(("h", "U", "V"))}
+                    torch.linalg.vector_norm(states["fp64"][k])) for k, q in enumerate(("h", "vorticity", "divergence"))}
     out = {**res, "mixed_over_fp64": res["mixed"]["steps_per_s"] / res["fp64"]["steps_per_s"], "nsteps": n, "dt": dt,
-           "grid": "1536 x 3072", "form": "nonlinear, Robert variables", "mixed_rel_l2_vs_fp64_after_nsteps": rel}
+           "grid": "1536 x 3072", "form": "nonlinear, vorticity-divergence with Robert velocities",
+           "mixed_rel_l2_vs_fp64_after_nsteps": rel, "kernel_launches_per_step": launches}
     del states, st0
     torch.cuda.empty_cache()
     return out
@@ -550,6 +559,42 @@ def cpu_baseline(min_seconds=10.0, max_reps=50):
                       f"(oracle C++/OpenMP FP64, {dt:.1f} s)"}
 
 
+def profile_case():
+    """One small instance of each workload, for ncu captures of every kernel
+    family (no timing): transforms of 64 scalar fields at T255 in both forms,
+    one nonlinear RK4 step at T255 (advective and vorticity-divergence forms),
+    one REXI step at T127 (M = 64) and one spectral operator pass."""
+    import torch
+
+    from sph_swe_b200 import build as b
+    b.build()
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph, rexi_coefficients
+
+    dev = torch.device("cuda", 0)
+    for prec in (capi.SPH_PREC_FP64, capi.SPH_PREC_MIXED):
+        s = Sph(L_CFG1, precision=prec)
+        spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1)).to(dev)
+        s.spat_to_SH(s.SH_to_spat(spec))
+        st = _bump_state(s, dev)
+        for form in (1, 2):
+            s.swe_rk4(Sph.swe_params(radius=6.371e6, dt=10.0, viscosity=1e5, nonlinear=form), st.clone(), 1)
+        capi.check(capi.lib().sph_sync(s.h, None))
+        s.close()
+    s = Sph(L_CFG1)
+    x = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 2)).to(dev)
+    s.spec_op("laplace", x)
+    s.close()
+    s = Sph(127)
+    a, br, _ = rexi_coefficients(0.2, 64, False)
+    rx = s.rexi(a, br, radius=6.371e6, tau=3600.0)
+    rx.step(_bump_state(s, dev), 1)
+    torch.cuda.synchronize()
+    rx.close()
+    s.close()
+    print(json.dumps({"profile_case": "done"}))
+
+
 def run_reference(args, rank, world):
     """CPU arm: the oracle (C++/OpenMP FP64 restatement; the reference's own
     SHTNS/FFTW/LAPACK build is unavailable on this machine) on all host cores.
@@ -594,7 +639,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="skip the RK4 side measurements")
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the dominant kernel")
+    ap.add_argument("--profile-case", action="store_true", help="run one small instance of each workload (for ncu)")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case()
+        return
     args.warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -178,9 +178,10 @@ typedef struct sph_swe_params {
     double dt;         /* time step (current_timestep_size) */
     int nonlinear;     /* SimVars::use_nonlinear_equations: 0 linear, 1 the
                           reference's nonlinear advective form (robert is then
-                          ignored, as AppSWE.hpp:622-650 does), 2 nonlinear
-                          equations in Robert variables U = u cos(phi),
-                          V = v cos(phi) with the metric terms (new form)     */
+                          ignored, as AppSWE.hpp:622-650 does), 2 the full
+                          nonlinear equations in vorticity-divergence form
+                          with Robert velocities on the grid (new form; the
+                          state is then [h | vorticity | divergence])        */
     int robert;        /* SimVars::use_robert_functions     */
 } sph_swe_params;
 
@@ -189,12 +190,17 @@ typedef struct sph_swe_params {
  * AppSWE::p_run_euler_timestep_update (AppSWE.hpp:574-659). */
 int sph_swe_tendency(sph_handle* h, const sph_swe_params* p, const double* state, double* tend, void* stream);
 
-/* nsteps classical RK4 steps in place on state = [h | u | v] (3*nlm complex),
+/* nsteps classical RK4 steps in place on state = [h | u | v] (3*nlm complex;
+ * [h | vorticity | divergence] with nonlinear = 2),
  * as TimesteppingRK::run_rk_timestep order 4 (TimesteppingRK.hpp:310-392)
  * driven by AppSWE::run (AppSWE.hpp:293-336).  The step is captured once in a
  * CUDA graph and replayed.  Returns SPH_ERR_NAN if h became non-finite
  * (AppSWE.hpp:322-327). */
 int sph_swe_rk4(sph_handle* h, const sph_swe_params* p, double* state, int nsteps, void* stream);
+
+/* kernel launches in one replay of the handle's captured RK4 step graph (0
+ * before the first sph_swe_rk4 / sph_swe_rk4_batched call) */
+int sph_swe_rk4_launches(const sph_handle* h);
 
 /* Batched ensemble: nmem independent members, state of member k at
  * state + 3*nlm*k (complex), all with the same handle and parameters except
@@ -272,6 +278,25 @@ enum sph_spat_op_kind {
  * scalar grid updates spat_set_value / spat_set_zero (SPHData.hpp:768-798). */
 int sph_spat_op(sph_handle* h, int op, const double* x, const double* y, double* out, double alpha, double beta,
                 long long n, void* stream);
+
+/* ---------------------------------------------------------------- autotuner */
+
+/* Time the kernel variants of the handle for `batch` fields per launch on
+ * `stream` and keep the fastest for every later call with that batch: the
+ * column tile (8, 16 or 32 fields per CTA) and P_l^m source (streamed table
+ * or regenerated) of the tensor-core Legendre stages of a mixed handle, and
+ * the rings per CTA of the fixed-length ring FFTs.  json (optional, capacity
+ * cap bytes) receives the table with every candidate's time.  Variants are
+ * exact alternatives (no change of arithmetic beyond the last bits of
+ * P_l^m).  A captured RK4 graph of the handle is re-captured on its next
+ * call; ensembles take the variants in force at sph_ensemble_create.  No
+ * counterpart in the reference (SHTNS picks its own algorithm at
+ * shtns_set_grid, SPHConfig.hpp:324-352). */
+int sph_autotune(sph_handle* h, int batch, char* json, int cap, void* stream);
+/* Re-apply a table written by sph_autotune (same truncation, grid, precision). */
+int sph_tune_load(sph_handle* h, const char* json);
+/* Back to the built-in rules. */
+int sph_tune_clear(sph_handle* h);
 
 /* ---------------------------------------------------------------- errors */
 

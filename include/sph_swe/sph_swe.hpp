@@ -649,9 +649,10 @@ struct SWEParameters {
     double viscosity2 = 1e5;
     bool use_nonlinear_equations = true;
     bool use_robert_functions = false;
-    // nonlinear equations in Robert variables with the metric terms (a form the
-    // reference does not have: its nonlinear branch ignores use_robert_functions)
-    bool use_nonlinear_robert = false;
+    // full nonlinear equations in vorticity-divergence form with Robert
+    // velocities on the grid (a form the reference does not have); the stepper's
+    // prognostic fields are then h, vorticity, divergence
+    bool use_vort_div_form = false;
 };
 
 // nonlinear / linear RK4 of AppSWE::run (AppSWE.hpp:293-336, TimesteppingRK.hpp:310-392):
@@ -669,8 +670,8 @@ class SWERK4 {
     void run(SPHData& h, SPHData& u, SPHData& v, double dt, int nsteps) {
         pack(h, u, v);
         sph_swe_params sp = {p_.earth_radius, p_.gravitation, p_.coriolis_omega, p_.h0, p_.viscosity2, dt,
-                             p_.use_nonlinear_robert ? 2 : (p_.use_nonlinear_equations ? 1 : 0),
-                             (p_.use_robert_functions || p_.use_nonlinear_robert) ? 1 : 0};
+                             p_.use_vort_div_form ? 2 : (p_.use_nonlinear_equations ? 1 : 0),
+                             p_.use_robert_functions ? 1 : 0};
         check(sph_swe_rk4(cfg_->handle(), &sp, reinterpret_cast<double*>(state_), nsteps, cfg_->s()), "sph_swe_rk4");
         unpack(h, u, v);
     }

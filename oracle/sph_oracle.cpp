@@ -1265,31 +1265,6 @@ void swe_tendency(const SWEParams& p, const Field& fdata, const Field& i_h, cons
             o_u_t += f(i_v);
             o_v_t -= f(i_u);
         }
-    } else if (p.nonlinear == 2) {
-        // Nonlinear equations in Robert variables U = u cos(phi), V = v cos(phi)
-        // with the metric terms (no reference counterpart; the reference's
-        // nonlinear branch ignores use_robert_functions):
-        //   h_t = -(1/a) [d(hU)/dlambda + (1-mu^2) d(hV)/dmu] / cos^2
-        //   U_t = -(g/a) dh/dlambda + f V - (1/a) [U dU/dlambda + V (1-mu^2) dU/dmu] / cos^2
-        //   V_t = -(g/a) (1-mu^2) dh/dmu - f U
-        //         - (1/a) [U dV/dlambda + V (1-mu^2) dV/dmu + mu (U^2 + V^2)] / cos^2
-        // written with the reference's Robert operators (SPHOperators.hpp:129-210);
-        // every product is formed on the grid and projected once.
-        auto mu_c2 = [](const Field& x) {
-            Field o = x;
-            o.spat_update_lambda_gaussian_grid([](double, double mu, double& d) { d *= mu / (1.0 - mu * mu); });
-            return o;
-        };
-        o_h_t = -(op::robert_div_lon(i_h * i_u) + op::robert_div_lat(i_h * i_v)) * (1.0 / p.a);
-        o_u_t = -op::robert_grad_lon(i_h) * (p.g / p.a);
-        o_v_t = -op::robert_grad_lat(i_h) * (p.g / p.a);
-        if (p.omega != 0) {
-            o_u_t += f(i_v);
-            o_v_t -= f(i_u);
-        }
-        o_u_t -= (i_u * op::robert_div_lon(i_u) + i_v * op::robert_div_lat(i_u)) * (1.0 / p.a);
-        o_v_t -= (i_u * op::robert_div_lon(i_v) + i_v * op::robert_div_lat(i_v) + i_u * mu_c2(i_u) + i_v * mu_c2(i_v)) *
-                 (1.0 / p.a);
     } else {
         o_h_t = -(op::div_lon(i_h * i_u) + op::div_lat(i_h * i_v)) * (1.0 / p.a);
         o_u_t = -op::grad_lon(i_h) * (p.g / p.a);

@@ -287,7 +287,7 @@ public:
 struct SWEParams {
     double a = 6.37122e6, g = 9.80616, omega = 7.292e-5, h0 = 1e4, visc = 0.0, dt = 120.0;
     // nonlinear: 0 linear, 1 the reference's nonlinear advective form (robert
-    // ignored), 2 nonlinear equations in Robert variables (U, V = u, v cos(phi))
+    // ignored); the vorticity-divergence form is restated in oracle/vortdiv.py
     int nonlinear = 1, robert = 0;
 };
 

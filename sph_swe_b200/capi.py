@@ -21,8 +21,9 @@ EXPORTS = (
     "sph_create", "sph_destroy", "sph_info", "sph_grid",
     "sph_spat_to_SH", "sph_SH_to_spat", "sph_SH_to_spat_noalloc", "sph_cplx_spat_to_SH", "sph_cplx_SH_to_spat",
     "sph_vec_SH_to_spat", "sph_vec_spat_to_SH", "sph_legendre_synthesis", "sph_legendre_analysis", "sph_spec_op",
-    "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched",
+    "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched", "sph_swe_rk4_launches",
     "sph_ensemble_create", "sph_ensemble_step", "sph_ensemble_launches", "sph_ensemble_destroy",
+    "sph_autotune", "sph_tune_load", "sph_tune_clear",
     "sph_spat_op", "sph_rexi_coefficients", "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_sync", "sph_last_error",
 )
 
@@ -76,6 +77,10 @@ def lib():
         L.sph_swe_rk4_batched.argtypes = [vp, ctypes.POINTER(SWEParams), dp, vp, i, i, vp]
         L.sph_ensemble_create.argtypes = [i, ctypes.POINTER(vp), ctypes.POINTER(SWEParams), ctypes.POINTER(vp), ip,
                                           ctypes.POINTER(dp), ctypes.POINTER(vp)]
+        L.sph_swe_rk4_launches.argtypes = [vp]
+        L.sph_autotune.argtypes = [vp, i, ctypes.c_char_p, i, vp]
+        L.sph_tune_load.argtypes = [vp, ctypes.c_char_p]
+        L.sph_tune_clear.argtypes = [vp]
         L.sph_ensemble_step.argtypes = [vp, i, vp]
         L.sph_ensemble_launches.argtypes = [vp]
         L.sph_ensemble_destroy.argtypes = [vp]

@@ -7,9 +7,10 @@
 //
 // Same single-letter flags and defaults as the reference (SimVars.hpp:14-79);
 // as in the reference, a trailing T<k> after the first argument is ignored.
-// New values and letters: N2 selects the nonlinear equations in Robert
-// variables (U, V = u, v cos(phi), with metric terms; the reference has no such
-// form), K selects the precision form (0 FP64, 1 mixed) and D<file>
+// New values and letters: N2 selects the full nonlinear equations in
+// vorticity-divergence form with Robert velocities on the grid (the reference
+// has no such form; the state is then h, vorticity, divergence), K selects the
+// precision form (0 FP64, 1 mixed) and D<file>
 // writes the final spectral state [h | u | v] (complex128, packed layout) to a
 // file.  Programs: P0 (shallow-water run); the reference's test programs
 // P1..P5 are not part of this driver.
@@ -160,7 +161,7 @@ int main(int argc, char** argv) {
         p.viscosity2 = v.visc;
         p.use_nonlinear_equations = v.nonlinear != 0;
         p.use_robert_functions = v.robert != 0;
-        p.use_nonlinear_robert = v.nonlinear == 2;
+        p.use_vort_div_form = v.nonlinear == 2;
 
         const long long nsteps = (long long)std::llround(v.tend / v.dt);
         const long long out_every = v.out_dt > 0.0 ? std::max<long long>(1, std::llround(v.out_dt / v.dt)) : nsteps;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstddef>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -56,6 +57,8 @@ struct Handle {
     void* mixed = nullptr;
     // RK4 buffers and captured step graph (swe.cu)
     void* rk = nullptr;
+    // autotuned kernel variants: key (kind << 32 | batch) -> variant (tune.cu)
+    std::map<long long, int> tune;
     // workspace (Fourier-space buffer and grids)
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -65,7 +68,16 @@ struct Handle {
 };
 
 int ensure_workspace(Handle* h, size_t bytes);
-void rk_free(Handle* h);  // swe.cu
+
+// kernel variants chosen by the autotuner (tune.cu); 0 = the built-in rule
+enum TuneKind { TUNE_TC_SYNTHESIS = 0, TUNE_TC_ANALYSIS = 1, TUNE_RING_ANALYSIS = 2, TUNE_RING_SYNTHESIS = 3 };
+inline int tune_get(const Handle* h, int kind, int batch, int dflt) {
+    if (h->tune.empty()) return dflt;
+    const auto it = h->tune.find(((long long)kind << 32) | (unsigned)batch);
+    return it == h->tune.end() ? dflt : it->second;
+}
+void rk_free(Handle* h);        // swe.cu
+void rk_invalidate(Handle* h);  // swe.cu: the next RK4 call re-captures its step graph
 
 // ---- kernels launched by the C-ABI layer (stream-ordered)
 int setup_tables(Handle* h);

@@ -290,18 +290,42 @@ static int ring_tile(int n, int complex_rings) {
     return jt;
 }
 
-template <int N>
+// sequences per CTA of the fixed-length kernels: variant 0 the default, 1 half of it
+template <int N, int V>
+constexpr int fixed_p() { return V == 0 ? fftx::seqs<N>() : fftx::seqs<N>() / 2; }
+
+template <int N, int P>
 static size_t fixed_smem() {
-    return (size_t)fftx::seqs<N>() * fftx::stride<N>() * sizeof(double2);
+    return (size_t)P * fftx::stride<N>() * sizeof(double2);
+}
+
+template <int N, int P>
+static int fixed_attr_p() {
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_analysis_real_n<N, P>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fixed_smem<N, P>()));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_synthesis_real_n<N, P>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fixed_smem<N, P>()));
+    return SPH_OK;
 }
 
 template <int N>
 static int fixed_attr() {
-    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_analysis_real_n<N>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fixed_smem<N>()));
-    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_ring_synthesis_real_n<N>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fixed_smem<N>()));
-    return SPH_OK;
+    if (int rc = fixed_attr_p<N, fixed_p<N, 0>()>()) return rc;
+    return fixed_attr_p<N, fixed_p<N, 1>()>();
+}
+
+template <int N, int P>
+static void launch_ra(const Handle* h, const double* spat, long long ld_spat, double2* F, long long ldF, int mF, int batch,
+                      cudaStream_t s) {
+    k_ring_analysis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::NT, fixed_smem<N, P>(), s>>>(
+        spat, ld_spat, F, ldF, mF, h->L, h->nlat, h->fft.tw);
+}
+
+template <int N, int P>
+static void launch_rs(const Handle* h, const double2* F, long long ldF, int mF, double* spat, long long ld_spat, int batch,
+                      const RingMap& map, cudaStream_t s) {
+    k_ring_synthesis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::NT, fixed_smem<N, P>(), s>>>(
+        F, ldF, mF, h->L, spat, ld_spat, h->nlat, h->fft.tw, map);
 }
 
 int fft_kernels_init() {
@@ -319,12 +343,12 @@ int fft_kernels_init() {
 int ring_analysis_real(const Handle* h, const double* spat, long long ld_spat, double2* F, long long ldF, int mF,
                        int batch, cudaStream_t s) {
     if (batch <= 0) return SPH_OK;
+    const int var = tune_get(h, TUNE_RING_ANALYSIS, batch, 0);
     switch (h->nphi) {
 #define SPH_RA(NN)                                                                                                   \
     case NN:                                                                                                         \
-        k_ring_analysis_real_n<NN><<<dim3((h->nlat + 2 * fftx::seqs<NN>() - 1) / (2 * fftx::seqs<NN>()), batch),    \
-                                     fftx::NT, fixed_smem<NN>(), s>>>(spat, ld_spat, F, ldF, mF, h->L, h->nlat,     \
-                                                                      h->fft.tw);                                    \
+        if (var) launch_ra<NN, fixed_p<NN, 1>()>(h, spat, ld_spat, F, ldF, mF, batch, s);                            \
+        else launch_ra<NN, fixed_p<NN, 0>()>(h, spat, ld_spat, F, ldF, mF, batch, s);                                \
         SPH_CUDA_TRY(cudaGetLastError());                                                                            \
         return SPH_OK;
         SPH_RA(96)
@@ -365,12 +389,12 @@ int ring_synthesis_real(const Handle* h, const double2* F, long long ldF, int mF
             map.mod[k] = mod ? mod[k] : 0;
         }
     }
+    const int var = tune_get(h, TUNE_RING_SYNTHESIS, batch, 0);
     switch (h->nphi) {
 #define SPH_RS(NN)                                                                                                   \
     case NN:                                                                                                         \
-        k_ring_synthesis_real_n<NN><<<dim3((h->nlat + 2 * fftx::seqs<NN>() - 1) / (2 * fftx::seqs<NN>()), batch),   \
-                                      fftx::NT, fixed_smem<NN>(), s>>>(F, ldF, mF, h->L, spat, ld_spat, h->nlat,    \
-                                                                       h->fft.tw, map);                              \
+        if (var) launch_rs<NN, fixed_p<NN, 1>()>(h, F, ldF, mF, spat, ld_spat, batch, map, s);                       \
+        else launch_rs<NN, fixed_p<NN, 0>()>(h, F, ldF, mF, spat, ld_spat, batch, map, s);                           \
         SPH_CUDA_TRY(cudaGetLastError());                                                                            \
         return SPH_OK;
         SPH_RS(96)

@@ -2,10 +2,12 @@
 // grids use: 96, 192, 384, 768, 1536, 3072), used by fft.cu in place of the
 // generic kernels for those lengths.
 //
-// A CTA of 256 threads transforms P complex sequences (P = 8 up to N = 768),
-// i.e. 2P consecutive latitude rings of one field packed in pairs (ring 2q
-// real part, ring 2q+1 imaginary part), so that every longitude row of the
-// tile is one 128-byte run of the theta-contiguous grid.  Sequence rows are
+// A CTA of 256 threads transforms P complex sequences (by default P = 8 up to
+// N = 768, i.e. 16 rings: every longitude row of the tile is one 128-byte run
+// of the theta-contiguous grid; P is a template parameter so that the
+// autotuner can trade tile width for CTAs per SM), i.e. 2P consecutive
+// latitude rings of one field packed in pairs (ring 2q real part, ring 2q+1
+// imaginary part).  Sequence rows are
 // padded by one element so that the tile loads hit distinct banks.  The Stockham passes (radix 3 first, then
 // 8, 4, 2; all radices and strides compile-time) run in place in a single
 // shared-memory buffer: each pass reads its butterfly inputs into registers,
@@ -19,7 +21,7 @@ namespace sphgpu {
 namespace fftx {
 
 constexpr int NT = 256;     // threads per CTA
-// complex sequences per CTA (2 P real rings) and their padded row stride
+// default complex sequences per CTA (2 P real rings) and the padded row stride
 template <int N>
 constexpr int seqs() { return N <= 768 ? 8 : (N == 1536 ? 4 : 2); }
 template <int N>
@@ -117,15 +119,14 @@ constexpr int ls_at(int N, int q) {
     return ls;
 }
 
-// One Stockham pass on seqs<N>() sequences in place: butterflies t = (f, j), j < N/R,
+// One Stockham pass on P sequences in place: butterflies t = (f, j), j < N/R,
 // inputs s[j + r N/R] times w^(r k N/(Ls R)), k = j mod Ls, outputs to
 // d[(j - k) R + k + r Ls]; w = exp(SIGN 2 pi i / N) from the table tw[t] = exp(-2 pi i t / N).
-template <int N, int Q, int SIGN>
+template <int N, int P, int Q, int SIGN>
 __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ tw) {
     constexpr int R = radix_at(N, Q);
     constexpr int Ls = ls_at(N, Q);
     constexpr int NR = N / R;
-    constexpr int P = seqs<N>();
     constexpr int SN = stride<N>();
     constexpr int TOT = P * NR;
     constexpr int IT = (TOT + NT - 1) / NT;
@@ -161,11 +162,11 @@ __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ t
     __syncthreads();
 }
 
-template <int N, int Q, int SIGN>
+template <int N, int P, int Q, int SIGN>
 __device__ __forceinline__ void passes(double2* buf, const double2* __restrict__ tw) {
     if constexpr (Q < npasses(N)) {
-        pass<N, Q, SIGN>(buf, tw);
-        passes<N, Q + 1, SIGN>(buf, tw);
+        pass<N, P, Q, SIGN>(buf, tw);
+        passes<N, P, Q + 1, SIGN>(buf, tw);
     }
 }
 
@@ -176,11 +177,11 @@ namespace sphgpu {
 
 // grid tile (2P rings, pairs packed) -> F[b][m][j], m = 0..mF-1 (m > L zero),
 // scaled by 2 pi / N (quadrature weight in longitude)
-template <int N>
+template <int N, int P>
 __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const double* __restrict__ spat, long long ld_spat,
                                                                     double2* __restrict__ F, long long ldF, int mF, int L,
                                                                     int nlat, const double2* __restrict__ tw) {
-    constexpr int P = fftx::seqs<N>(), SN = fftx::stride<N>(), JT = 2 * P;
+    constexpr int SN = fftx::stride<N>(), JT = 2 * P;
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
     const double* src = spat + (long long)blockIdx.y * ld_spat;
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const doub
         }
     }
     __syncthreads();
-    fftx::passes<N, 0, -1>(fbuf, tw);
+    fftx::passes<N, P, 0, -1>(fbuf, tw);
     const double scale = 2.0 * kPi / N;
     double2* out = F + (long long)blockIdx.y * ldF;
     for (int idx = threadIdx.x; idx < mF * P; idx += fftx::NT) {
@@ -224,12 +225,12 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const doub
 }
 
 // F[fs][m][j] (optionally times i*m) -> grid k; m = 0 contributes its real part
-template <int N>
+template <int N, int P>
 __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const double2* __restrict__ F, long long ldF, int mF,
                                                                      int L, double* __restrict__ spat, long long ld_spat,
                                                                      int nlat, const double2* __restrict__ tw,
                                                                      RingMap map) {
-    constexpr int P = fftx::seqs<N>(), SN = fftx::stride<N>(), JT = 2 * P;
+    constexpr int SN = fftx::stride<N>(), JT = 2 * P;
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
     const int k = blockIdx.y;
@@ -262,7 +263,7 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const dou
         }
     }
     __syncthreads();
-    fftx::passes<N, 0, +1>(fbuf, tw);
+    fftx::passes<N, P, 0, +1>(fbuf, tw);
     double* out = spat + (long long)k * ld_spat;
 #pragma unroll 8
     for (int idx = threadIdx.x; idx < N * JT; idx += fftx::NT) {

@@ -1020,7 +1020,8 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
 
 #include "legendre_tcs.cuh"
 
-static int encode_map(CUtensorMap* map, float* base, unsigned long long d1, unsigned long long d2) {
+// rows: padded row count (a multiple of 64), slices: z extent
+static int encode_map(CUtensorMap* map, float* base, unsigned long long rows, unsigned long long slices) {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
         cudaDriverEntryPointQueryResult q;
@@ -1032,10 +1033,10 @@ static int encode_map(CUtensorMap* map, float* base, unsigned long long d1, unsi
         }
         fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
     }
-    // dims (x = 4 floats, d1 rows, d2 slices, 2 parts); box 4 x 128 x 4 x 2
-    const cuuint64_t dims[4] = {4, d1, d2, 2};
-    const cuuint64_t strides[3] = {16, 16ull * d1, 16ull * d1 * d2};
-    const cuuint32_t box[4] = {4, (cuuint32_t)tc::M, 4, 2};
+    // dims (64 rows x 4 floats, row blocks, slices, 2 parts); box 256 x 2 x 4 x 2
+    const cuuint64_t dims[4] = {256, rows / 64, slices, 2};
+    const cuuint64_t strides[3] = {1024, 16ull * rows, 16ull * rows * slices};
+    const cuuint32_t box[4] = {256, 2, 4, 2};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1049,15 +1050,16 @@ static int encode_map(CUtensorMap* map, float* base, unsigned long long d1, unsi
 
 static int tcs_tables_build(Handle* h, MixedTables* T) {
     const int tl = T->lmax, nh = h->nh, mm = std::min(tl, h->L);
+    const int nhP = tcs_pad64(nh);
     std::vector<long long> so(mm + 2, 0), ao(mm + 2, 0);
     for (int m = 0; m <= mm; m++) {
         so[m + 1] = so[m] + 8LL * tcs_nchunks(tl, m);
-        ao[m + 1] = ao[m] + tcs_nlp(tl, m, 0) + tcs_nlp(tl, m, 1);
+        ao[m + 1] = ao[m] + tcs_pad64(tcs_nlp(tl, m, 0)) + tcs_pad64(tcs_nlp(tl, m, 1));
     }
     T->zS = so[mm + 1];
     T->rowsA = ao[mm + 1];
     T->zA = (nh + 3) / 4;
-    const size_t bs = sizeof(float) * 2 * (size_t)T->zS * nh * 4, ba = sizeof(float) * 2 * (size_t)T->zA * T->rowsA * 4;
+    const size_t bs = sizeof(float) * 2 * (size_t)T->zS * nhP * 4, ba = sizeof(float) * 2 * (size_t)T->zA * T->rowsA * 4;
     SPH_CUDA_TRY(cudaMalloc(&T->S, bs));
     SPH_CUDA_TRY(cudaMalloc(&T->A, ba));
     SPH_CUDA_TRY(cudaMemset(T->S, 0, bs));
@@ -1066,10 +1068,10 @@ static int tcs_tables_build(Handle* h, MixedTables* T) {
     SPH_CUDA_TRY(cudaMalloc(&T->aoff, sizeof(long long) * (mm + 2)));
     SPH_CUDA_TRY(cudaMemcpy(T->soff, so.data(), sizeof(long long) * (mm + 2), cudaMemcpyHostToDevice));
     SPH_CUDA_TRY(cudaMemcpy(T->aoff, ao.data(), sizeof(long long) * (mm + 2), cudaMemcpyHostToDevice));
-    k_tcs_tables<<<dim3((nh + 127) / 128, mm + 1), 128>>>(nh, tl, mm, h->mu, T->soff, T->aoff, T->zS, T->rowsA, T->zA,
-                                                          T->S, T->A);
+    k_tcs_tables<<<dim3((nh + 127) / 128, mm + 1), 128>>>(nh, nhP, tl, mm, h->mu, T->soff, T->aoff, T->zS, T->rowsA,
+                                                          T->zA, T->S, T->A);
     SPH_CUDA_TRY(cudaGetLastError());
-    if (int rc = encode_map(&T->mapS, T->S, (unsigned long long)nh, (unsigned long long)T->zS)) return rc;
+    if (int rc = encode_map(&T->mapS, T->S, (unsigned long long)nhP, (unsigned long long)T->zS)) return rc;
     if (int rc = encode_map(&T->mapA, T->A, (unsigned long long)T->rowsA, (unsigned long long)T->zA)) return rc;
     T->streamed = true;
     return SPH_OK;
@@ -1138,9 +1140,16 @@ static int check_tables(const MixedTables* T, int lmax) {
 // columns per CTA from the batch: 8, 16 or 32 fields
 static int tc_cols(int batch) { return batch <= 8 ? 16 : (batch <= 16 ? 32 : 64); }
 
+// column tile of an autotuned variant (bits 0-1: 0 rule, 1: 16, 2: 32, 3: 64)
+static int tc_cols_v(int batch, int var) {
+    const int c = var & 3;
+    return c == 0 ? tc_cols(batch) : (8 << c);
+}
+
+
 template <template <int> class Dir>
-static int tc_launch(TcArgs& a, int nrt, int nm, const double2* in, double2* out, cudaStream_t s) {
-    const int nc = tc_cols(a.batch);
+static int tc_launch(TcArgs& a, int nrt, int nm, const double2* in, double2* out, int var, cudaStream_t s) {
+    const int nc = tc_cols_v(a.batch, var);
     a.nct = (2 * a.batch + nc - 1) / nc;
     a.nrt = nrt;
     a.ntiles = a.nct * nrt * nm;
@@ -1172,9 +1181,9 @@ static TsArgs make_sargs(const Handle* h, const MixedTables* T, int lmax, int ba
 }
 
 template <template <int> class Dir>
-static int tcs_launch(const CUtensorMap& map, TsArgs& a, int nrt, int nm, const double2* in, double2* out,
+static int tcs_launch(const CUtensorMap& map, TsArgs& a, int nrt, int nm, const double2* in, double2* out, int var,
                       cudaStream_t s) {
-    const int nc = tc_cols(a.batch);
+    const int nc = tc_cols_v(a.batch, var);
     a.nct = (2 * a.batch + nc - 1) / nc;
     a.nrt = nrt;
     a.ntiles = a.nct * nrt * nm;
@@ -1192,12 +1201,13 @@ int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spe
     if (int rc = check_tables(T, lmax)) return rc;
     if (batch <= 0) return SPH_OK;
     const int nrt = (h->nh + tc::M - 1) / tc::M, nm = std::min(lmax, h->L) + 1;
-    if (T->streamed) {
+    const int var = tune_get(h, TUNE_TC_SYNTHESIS, batch, 0);
+    if (T->streamed && !(var & 4)) {
         TsArgs a = make_sargs(h, T, lmax, batch, ld_spec, ldF);
-        return tcs_launch<SynS>(T->mapS, a, nrt, nm, spec, F, s);
+        return tcs_launch<SynS>(T->mapS, a, nrt, nm, spec, F, var, s);
     }
     TcArgs a = make_args(h, T, lmax, batch, ld_spec, ldF);
-    return tc_launch<SynDir>(a, nrt, nm, spec, F, s);
+    return tc_launch<SynDir>(a, nrt, nm, spec, F, var, s);
 }
 
 int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec, int lmax,
@@ -1206,12 +1216,13 @@ int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, doubl
     if (int rc = check_tables(T, lmax)) return rc;
     if (batch <= 0) return SPH_OK;
     const int nrt = lmax / (2 * tc::M) + 1, nm = std::min(lmax, h->L) + 1;
-    if (T->streamed) {
+    const int var = tune_get(h, TUNE_TC_ANALYSIS, batch, 0);
+    if (T->streamed && !(var & 4)) {
         TsArgs a = make_sargs(h, T, lmax, batch, ld_spec, ldF);
-        return tcs_launch<AnaS>(T->mapA, a, nrt, nm, F, spec, s);
+        return tcs_launch<AnaS>(T->mapA, a, nrt, nm, F, spec, var, s);
     }
     TcArgs a = make_args(h, T, lmax, batch, ld_spec, ldF);
-    return tc_launch<AnaDir>(a, nrt, nm, F, spec, s);
+    return tc_launch<AnaDir>(a, nrt, nm, F, spec, var, s);
 }
 
 int tc_check(const Handle* h) {

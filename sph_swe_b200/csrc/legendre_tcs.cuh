@@ -6,28 +6,34 @@
 // loads that land directly in the tensor core's K-major no-swizzle layout:
 //
 //   synthesis  S[w][z][j][x]  x = l' mod 4, z = zoff(m, parity) + l' / 4
-//              (rows = latitudes j, K = degrees l = m + 2 l' + parity;
-//               each (m, parity) block padded with zeros to whole chunks)
+//              (rows = latitudes j, padded to a multiple of 64; K = degrees
+//               l = m + 2 l' + parity; each (m, parity) block padded with
+//               zeros to whole chunks)
 //   analysis   A[w][z][y][x]  x = j mod 4, z = j / 4,
-//              y = yoff(m, parity) + l' (rows = degrees, K = latitudes)
+//              y = yoff(m, parity) + l' (rows = degrees, each (m, parity)
+//              block padded with zero rows to a multiple of 64; K = latitudes)
 //
-// with w = 0 hi, 1 lo.  A box {4, 128, 4, 2} is 128 rows x 16 K x {hi, lo}:
+// with w = 0 hi, 1 lo.  A row is 16 B and 64 rows are 1 KB of contiguous
+// memory, so the tensor maps see (64 rows x 4 floats, row block, z, w) and a
+// box {256, 2, 4, 2} is 128 rows x 16 K x {hi, lo} with a 1 KB inner extent:
 // in shared memory four 2 KB slices of 128 rows x 16 B per part, i.e. core
-// matrices 128 B apart along M/N (SBO) and 2 KB apart along K (LBO).  Rows
-// beyond a table's extent (latitudes >= nh, the last degree tile) are zero
-// filled by the TMA unit or land in output rows the epilogue discards.
+// matrices 128 B apart along M/N (SBO) and 2 KB apart along K (LBO).  Row
+// blocks beyond a table's extent are zero filled by the TMA unit; padded rows
+// are zero or land in output rows the epilogue discards.
 //
-// Per SM one persistent CTA of 13 warps: producers (warps 0-7) stage the
+// Per SM one persistent CTA of 17 warps: producers (warps 0-7) stage the
 // split B operand from a cp.async prefetch ring, thread 0 also issues the A
-// loads of each stage; warp 12 issues the MMAs; consumers (warps 8-11) fold the
-// FP32 group sums into FP64 sums in tensor memory and write finished tiles.
-// Every wait is bounded as in the generator kernel.
+// loads of each stage; warp 16 issues the MMAs; consumers (warps 8-15, two per
+// tensor-memory lane quadrant, each half of the columns) fold the FP32 group
+// sums into FP64 sums in tensor memory and write finished tiles, with one
+// tensor-memory load wait per 8 columns.  Every wait is bounded as in the
+// generator kernel.
 
 namespace tss {
 constexpr int NPROD = 256;                 // producer threads (B staging; thread 0 issues the A loads)
-constexpr int NCONS = 128;
-constexpr int MMA_WARP = 12;
-constexpr int NT = 416;
+constexpr int NCONS = 256;                 // consumer threads: warp 8 + q + 4 h = lane quadrant q, column half h
+constexpr int MMA_WARP = 16;
+constexpr int NT = 544;
 constexpr int NSTAGE = 3;
 constexpr int NRAW = 3;
 constexpr int STAGE_B = 4 * tc::STAGE_F;  // 48 KB: A (32 KB) then B (16 KB)
@@ -39,9 +45,11 @@ constexpr int BYTES = OFF_BAR + 512;
 static_assert(RAW_B % 128 == 0 && STAGE_B % 1024 == 0, "aligned buffers");
 }  // namespace tss
 
-// chunks of 16 degrees per parity of order m up to degree T, and degrees of one parity
+// chunks of 16 degrees per parity of order m up to degree T, degrees of one
+// parity, and a row count rounded up to whole 64-row blocks
 __host__ __device__ inline int tcs_nchunks(int T, int m) { return (T - m) / (2 * tc::KC) + 1; }
 __host__ __device__ inline int tcs_nlp(int T, int m, int par) { return T - m - par >= 0 ? (T - m - par) / 2 + 1 : 0; }
+__host__ __device__ inline int tcs_pad64(int n) { return (n + 63) & ~63; }
 
 // K-major no-swizzle descriptor with explicit core-matrix strides (bytes)
 __device__ __forceinline__ uint64_t sdesc2(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -129,10 +137,10 @@ struct SynS {
             bp[tc::BTILE] = lo;
         }
     }
-    // TMA box origin (x, y, z) of parity par's A part
+    // TMA box origin (x, row block, z) of parity par's A part
     __device__ static int3 box(const TsArgs& a, const TcPos& p, int par) {
         const long long z = a.soff[p.m] + (long long)par * 4 * tcs_nchunks(a.tlmax, p.m) + 4 * p.kc;
-        return make_int3(0, tc::M * p.rt, (int)z);
+        return make_int3(0, 2 * p.rt, (int)z);
     }
     __device__ static void epilogue(const TsArgs& a, const TcPos& p, int cw, int col, double2* __restrict__ F,
                                     const double* e, const double* o) {
@@ -199,8 +207,8 @@ struct AnaS {
         }
     }
     __device__ static int3 box(const TsArgs& a, const TcPos& p, int par) {
-        const long long y = a.aoff[p.m] + (long long)par * tcs_nlp(a.tlmax, p.m, 0) + tc::M * p.rt;
-        return make_int3(0, (int)y, 4 * p.kc);
+        const long long y = a.aoff[p.m] + (long long)par * tcs_pad64(tcs_nlp(a.tlmax, p.m, 0)) + tc::M * p.rt;
+        return make_int3(0, (int)(y >> 6), 4 * p.kc);
     }
     // consumer thread: TMEM lane r = degree index l' = 128 rt + r of both parities
     __device__ static void epilogue(const TsArgs& a, const TcPos& p, int cw, int col, double2* __restrict__ spec,
@@ -265,31 +273,72 @@ __device__ __forceinline__ TcPos ts_next(const TsArgs& a, TcPos p) {
     return ts_tile<Dir>(a, p.t + gridDim.x);
 }
 
-// consumer: fold a group's FP32 sums into the FP64 sums, or hand the totals to the epilogue
+// 8 FP32 columns of E and O and, unless first, their FP64 running sums
+// (16 + 16 words), one wait
+__device__ __forceinline__ void tmem_ld_block(uint32_t pe, uint32_t po, uint32_t se, uint32_t so, bool first, float* e,
+                                              float* o, float* we, float* wo) {
+    uint32_t r[48];
+    if (first) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%16];\n\t"
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8,%9,%10,%11,%12,%13,%14,%15}, [%17];\n\t"
+            "tcgen05.wait::ld.sync.aligned;"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(pe), "r"(po)
+            : "memory");
+    } else {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%48];\n\t"
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8,%9,%10,%11,%12,%13,%14,%15}, [%49];\n\t"
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, "
+            "[%50];\n\t"
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, "
+            "[%51];\n\t"
+            "tcgen05.wait::ld.sync.aligned;"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+              "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+              "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47])
+            : "r"(pe), "r"(po), "r"(se), "r"(so)
+            : "memory");
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            we[i] = __uint_as_float(r[16 + i]);
+            wo[i] = __uint_as_float(r[32 + i]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        e[i] = __uint_as_float(r[i]);
+        o[i] = __uint_as_float(r[8 + i]);
+    }
+}
+
+// consumer warp cw (0..7): lane quadrant cw & 3, columns of half cw >> 2; fold a
+// group's FP32 sums into the FP64 sums, or hand the totals to the epilogue
 template <class Dir, int NC>
 __device__ __forceinline__ void ts_consume(const TsArgs& a, const TcPos& p, uint32_t tmem, int b, int cw, bool first,
                                            bool last, double2* __restrict__ out) {
+    constexpr int HALF = NC / 2;
     const uint32_t lane = (uint32_t)((cw & 3) * 32) << 16;
+    const int c_begin = (cw >> 2) * HALF;
     const uint32_t part = tmem + lane + (uint32_t)(b * 2 * NC);
     const uint32_t sum = tmem + lane + TcCfg<NC>::ACC64;
 #pragma unroll
-    for (int c0 = 0; c0 < NC; c0 += 8) {
-        float e[8], o[8];
-        tmem_ld_pair<8>(part + c0, part + NC + c0, e, o);
+    for (int c0 = c_begin; c0 < c_begin + HALF; c0 += 8) {
+        float e[8], o[8], we[16], wo[16];
+        tmem_ld_block(part + c0, part + NC + c0, sum + 2 * c0, sum + 2 * NC + 2 * c0, first, e, o, we, wo);
         double se[8], so[8];
-        if (first) {
 #pragma unroll
-            for (int i = 0; i < 8; i++) {
-                se[i] = (double)e[i];
-                so[i] = (double)o[i];
-            }
-        } else {
-            float we[16], wo[16];
-            tmem_ld_pair<16>(sum + 2 * c0, sum + 2 * NC + 2 * c0, we, wo);
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                se[i] = __hiloint2double(__float_as_int(we[2 * i + 1]), __float_as_int(we[2 * i])) + (double)e[i];
-                so[i] = __hiloint2double(__float_as_int(wo[2 * i + 1]), __float_as_int(wo[2 * i])) + (double)o[i];
+        for (int i = 0; i < 8; i++) {
+            se[i] = (double)e[i];
+            so[i] = (double)o[i];
+            if (!first) {
+                se[i] += __hiloint2double(__float_as_int(we[2 * i + 1]), __float_as_int(we[2 * i]));
+                so[i] += __hiloint2double(__float_as_int(wo[2 * i + 1]), __float_as_int(wo[2 * i]));
             }
         }
         if (last) {
@@ -477,22 +526,22 @@ __global__ void __launch_bounds__(tss::NT, 1) k_legendre_tcs(const __grid_consta
 // ------------------------------------------------------------------ tables
 // thread per (northern latitude j, order m): the FP64 recurrence of the P
 // table (same steps and scaling), split into TF32 hi/lo, written to both tables
-__global__ void k_tcs_tables(int nh, int tlmax, int mm, const double* __restrict__ x, const long long* __restrict__ soff,
-                             const long long* __restrict__ aoff, long long zS, long long rowsA, int zA,
-                             float* __restrict__ S, float* __restrict__ A) {
+__global__ void k_tcs_tables(int nh, int nhP, int tlmax, int mm, const double* __restrict__ x,
+                             const long long* __restrict__ soff, const long long* __restrict__ aoff, long long zS,
+                             long long rowsA, int zA, float* __restrict__ S, float* __restrict__ A) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (j >= nh || m > mm) return;
     const double z = x[j];
     const double sn = sqrt((1.0 - z) * (1.0 + z));
-    const long long sw = zS * nh * 4, aw = (long long)zA * rowsA * 4;
+    const long long sw = zS * nhP * 4, aw = (long long)zA * rowsA * 4;
     const long long s0 = soff[m], s1 = s0 + 4LL * tcs_nchunks(tlmax, m);
-    const long long a0 = aoff[m], a1 = a0 + tcs_nlp(tlmax, m, 0);
+    const long long a0 = aoff[m], a1 = a0 + tcs_pad64(tcs_nlp(tlmax, m, 0));
     auto put = [&](int l, double v) {
         const int d = l - m, par = d & 1, lp = d >> 1;
         float hi, lo;
         split_tf32(v, hi, lo);
-        const long long is = (((par ? s1 : s0) + (lp >> 2)) * nh + j) * 4 + (lp & 3);
+        const long long is = (((par ? s1 : s0) + (lp >> 2)) * nhP + j) * 4 + (lp & 3);
         S[is] = hi;
         S[is + sw] = lo;
         const long long ia = (((long long)(j >> 2)) * rowsA + (par ? a1 : a0) + lp) * 4 + (j & 3);

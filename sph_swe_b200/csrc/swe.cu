@@ -27,18 +27,26 @@
 // of H in the flux products and no advection terms; the Robert linear form
 // divides by c^2 and takes the geopotential gradient in spectral space.
 // With nonlinear = 1 the reference ignores use_robert_functions
-// (AppSWE.hpp:622-650) and so does this file.  nonlinear = 2 selects the
-// nonlinear equations in Robert variables U = u cos(phi), V = v cos(phi), with
-// the metric terms (no reference counterpart):
-//   h_t = -(1/a) F( [I(iM F(hU)) + I(D F(hV))] / c^2 )
-//   U_t = -(g/a) iM h + F(f V) - (1/a) F( [U U_l + V U_m] / c^2 )
-//   V_t = -(g/a) D h  - F(f U) - (1/a) F( [U V_l + V V_m + mu (U^2 + V^2)] / c^2 )
-// (U_l, U_m = grids of iM U and D U), through the same waves as the
-// advective form with the Robert linear form's spectral gradient.
+// (AppSWE.hpp:622-650) and so does this file.
+//
+// nonlinear = 2 selects a form the reference does not have: the full
+// nonlinear equations in vorticity-divergence form with the Robert velocity
+// U = u c, V = v c on the grid (the NCAR spectral model's formulation; state
+// [h | zeta | delta], physical units).  With eta = zeta + 2 Omega mu:
+//   zeta_t  = -(1/a) div(eta v),  h_t = -(1/a) div(h v)
+//   delta_t =  (1/a) curl(eta v) - (1/a^2) lap(g h + (U^2 + V^2) / (2 c^2))
+// One wave each way: the exact vector synthesis of (a zeta, a delta) to U, V
+// plus the syntheses of zeta and h (4 fields, degree L+1 kept); pointwise
+// A, B = eta (U, V) / c^2, C, D = h (U, V) / c^2, E; 5 analyses of degree L+1;
+// div / curl by the integration-by-parts recurrence of the vector analysis.
+// No grid value is differentiated, so the truncation error is not divided by
+// cos^2 at the polar rings, and div has no l = 0 term: h_00 (mass) and
+// zeta_00 change by rounding only.
 // The whole step (4 stages + update) is captured once in a CUDA graph.
 #include "common.cuh"
 #include "identities.cuh"
 
+#include <algorithm>
 #include <cstring>
 
 namespace sphgpu {
@@ -64,6 +72,7 @@ struct RKState {
     cudaStream_t stream = nullptr;
     sph_swe_params params{};
     std::vector<double> dts_h;
+    int launches = 0;  // kernel launches in one replay of the step graph
 };
 
 static void rk_release(RKState* r) {
@@ -81,7 +90,9 @@ static int rk_buffers(const Handle* h, RKState* r, int nmem) {
     r->nmem = nmem;
     const size_t nlm = h->nlm, fou = (size_t)(h->L + 1) * h->nlat, sp = h->nspat;
     const size_t M = nmem;
-    SPH_CUDA_TRY(cudaMalloc(&r->X6, sizeof(double2) * 6 * nlm * M));
+    // X6 also holds the 5 degree-(L+1) analyses of the vorticity-divergence form
+    const size_t nlmp = (size_t)(h->L + 2) * (h->L + 3) / 2;
+    SPH_CUDA_TRY(cudaMalloc(&r->X6, sizeof(double2) * std::max(6 * nlm, 5 * nlmp) * M));
     SPH_CUDA_TRY(cudaMalloc(&r->F6, sizeof(double2) * 6 * fou * M));
     SPH_CUDA_TRY(cudaMalloc(&r->G9, sizeof(double) * 9 * sp * M));
     SPH_CUDA_TRY(cudaMalloc(&r->G4, sizeof(double) * 4 * sp * M));
@@ -103,6 +114,10 @@ void rk_free(Handle* h) {
     h->rk = nullptr;
 }
 
+void rk_invalidate(Handle* h) {
+    if (RKState* r = static_cast<RKState*>(h->rk)) r->state = nullptr;
+}
+
 static int rk_alloc(Handle* h, int nmem) {
     RKState* r = static_cast<RKState*>(h->rk);
     if (r && r->nmem >= nmem) return SPH_OK;
@@ -117,7 +132,7 @@ static int rk_alloc(Handle* h, int nmem) {
 // index helpers for the real packed layout: block y = m, threads over n
 struct SweConst {
     double a, g, omega, h0, visc;
-    int mode;  // 0 nonlinear, 1 linear, 2 linear Robert, 3 nonlinear Robert
+    int mode;  // 0 nonlinear, 1 linear, 2 linear Robert
 };
 
 __device__ __forceinline__ double2 ld2(const double2* p, int L, int n, int m) {
@@ -180,14 +195,6 @@ __global__ void k_swe_pointwise(const double* __restrict__ G9, double* __restric
         B = k.h0 * (c * V);
         ut = -ga * (Hl / c) + to * (m_ * V);
         vt = -ga * (Hm / c) - to * (m_ * U);
-    } else if (k.mode == 3) {
-        // Robert variables: U, V here are u cos(phi), v cos(phi); Ul, Um their
-        // longitude derivative and (1-mu^2) d/dmu; mu (U^2 + V^2) is the metric term
-        const double ic2 = 1.0 / (c * c);
-        A = H * U;
-        B = H * V;
-        ut = to * (m_ * V) - ia * ((U * Ul + V * Um) * ic2);
-        vt = -to * (m_ * U) - ia * ((U * Vl + V * Vm + m_ * (U * U + V * V)) * ic2);
     } else {
         A = k.h0 * U;
         B = k.h0 * V;
@@ -265,8 +272,8 @@ __global__ void k_rk_stage_out(const double2* __restrict__ S, const double2* __r
     double2 ut = t4[2 * (size_t)nlm + k];
     double2 vt = t4[3 * (size_t)nlm + k];
     const double dn = n, dm = m;
-    if (kc.mode >= 2) {
-        // Robert forms: -(g/a) iM h  and  -(g/a) D h in spectral space
+    if (kc.mode == 2) {
+        // -(g/a) iM h  and  -(g/a) D h in spectral space
         const double ga = kc.g / kc.a;
         const double2 xh = x_at(0, n), lo = x_at(0, n - 1), hi = x_at(0, n + 1);
         ut.x += -ga * (-dm * xh.y);
@@ -307,6 +314,126 @@ __global__ void k_rk_final(double2* __restrict__ S, const double2* __restrict__ 
     if ((idx - (size_t)mem * per) < (size_t)nlm && !(isfinite(s.x) && isfinite(s.y))) atomicOr(flag, 1);
 }
 
+// ------------------------------------------------------------------ vorticity-divergence form
+// stage input x = S + (coef dt) K_prev of [h, zeta, delta]; writes, in the
+// packed layout of degree L+1, X = [U_s, V_s, zeta, h]: the Robert velocity
+// spectra of (a zeta, a delta) (inverse Laplacian, then U = i m chi - D psi,
+// V = i m psi + D chi with D the untruncated (1-mu^2) d/dmu) and the two
+// scalar fields padded with zeros at degree L+1
+__global__ void k_vd_prep(const double2* __restrict__ S, const double2* __restrict__ Kp, double coef,
+                          const double* __restrict__ dts, double2* __restrict__ X, int L, int nlm, int nlmp, double a) {
+    const int m = blockIdx.y;  // 0..L+1
+    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
+    const int Lp = L + 1;
+    if (n > Lp) return;
+    const int mem = blockIdx.z;
+    const double c = Kp ? coef * dts[mem] : 0.0;
+    const double2* s = S + (size_t)mem * 3 * nlm;
+    const double2* kp = Kp ? Kp + (size_t)mem * 3 * nlm : nullptr;
+    auto x_at = [&](int q, int nn) -> double2 {
+        if (nn < m || nn > L || m > L) return make_double2(0, 0);
+        const int kk = pidx(L, nn, m);
+        double2 v = s[(size_t)q * nlm + kk];
+        if (kp) {
+            const double2 t = kp[(size_t)q * nlm + kk];
+            v.x += c * t.x;
+            v.y += c * t.y;
+        }
+        return v;
+    };
+    auto inv = [&](int q, int nn) -> double2 {  // a x / (-nn (nn + 1))
+        if (nn <= 0) return make_double2(0, 0);
+        const double2 v = x_at(q, nn);
+        const double f = -a / ((double)nn * (nn + 1.0));
+        return make_double2(v.x * f, v.y * f);
+    };
+    const int k = pidx(Lp, n, m);
+    double2* o = X + (size_t)mem * 4 * nlmp;
+    if (m > L) {
+        o[k] = o[nlmp + k] = o[2 * (size_t)nlmp + k] = o[3 * (size_t)nlmp + k] = make_double2(0, 0);
+        return;
+    }
+    const double dn = n, dm = m;
+    const double cl = (-dn + 1.0) * idR(dn - 1, dm), ch = (dn + 2.0) * idS(dn + 1, dm);
+    const double2 psi = inv(1, n), chi = inv(2, n);
+    const double2 psl = inv(1, n - 1), psh = inv(1, n + 1), chl = inv(2, n - 1), chh = inv(2, n + 1);
+    o[k] = make_double2(-dm * chi.y - (cl * psl.x + ch * psh.x), dm * chi.x - (cl * psl.y + ch * psh.y));
+    o[nlmp + k] = make_double2(-dm * psi.y + (cl * chl.x + ch * chh.x), dm * psi.x + (cl * chl.y + ch * chh.y));
+    o[2 * (size_t)nlmp + k] = x_at(1, n);
+    o[3 * (size_t)nlmp + k] = x_at(0, n);
+}
+
+// G4 per member [U, V, zeta, h] -> G5 [eta U / c^2, eta V / c^2, h U / c^2, h V / c^2, g h + (U^2 + V^2) / (2 c^2)]
+__global__ void k_vd_pointwise(const double* __restrict__ G4, double* __restrict__ G5, const double* __restrict__ mu,
+                               const double* __restrict__ cosphi, int nlat, int nspat, double grav, double omega) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nspat) return;
+    const int mem = blockIdx.y;
+    const int j = idx % nlat;
+    const double* g = G4 + (size_t)mem * 4 * nspat + idx;
+    double* o = G5 + (size_t)mem * 5 * nspat + idx;
+    const double U = g[0], V = g[(size_t)nspat], Z = g[2 * (size_t)nspat], H = g[3 * (size_t)nspat];
+    const double c = cosphi[j];
+    const double ic2 = 1.0 / (c * c);
+    const double eta = Z + 2.0 * omega * mu[j];
+    o[0] = eta * U * ic2;
+    o[(size_t)nspat] = eta * V * ic2;
+    o[2 * (size_t)nspat] = H * U * ic2;
+    o[3 * (size_t)nspat] = H * V * ic2;
+    o[4 * (size_t)nspat] = grav * H + 0.5 * (U * U + V * V) * ic2;
+}
+
+// K_s = [h_t, zeta_t, delta_t] from the degree-(L+1) analyses A5 = [a(A), a(B), a(C), a(D), a(E)]
+__global__ void k_vd_stage_out(const double2* __restrict__ S, const double2* __restrict__ Kp, double coef,
+                               const double* __restrict__ dts, const double2* __restrict__ A5,
+                               double2* __restrict__ Ks, int L, int nlm, int nlmp, double a, double visc) {
+    const int m = blockIdx.y;
+    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n > L) return;
+    const int mem = blockIdx.z;
+    const int Lp = L + 1;
+    const double2* aA = A5 + (size_t)mem * 5 * nlmp;
+    auto at = [&](int q, int nn) -> double2 {
+        if (nn < m || nn > Lp) return make_double2(0, 0);
+        return aA[(size_t)q * nlmp + pidx(Lp, nn, m)];
+    };
+    const double dn = n, dm = m;
+    const double el = (dn + 1.0) * idR(dn - 1, dm), eh = dn * idS(dn + 1, dm);
+    const double2 A0 = at(0, n), Al = at(0, n - 1), Ah = at(0, n + 1);
+    const double2 B0 = at(1, n), Bl = at(1, n - 1), Bh = at(1, n + 1);
+    const double2 C0 = at(2, n), Dl = at(3, n - 1), Dh = at(3, n + 1);
+    const double2 E0 = at(4, n);
+    // curl and div of (A, B), div of (C, D) on the unit sphere
+    const double2 crf = make_double2(-dm * B0.y + el * Al.x - eh * Ah.x, dm * B0.x + el * Al.y - eh * Ah.y);
+    const double2 dvf = make_double2(-dm * A0.y - el * Bl.x + eh * Bh.x, dm * A0.x - el * Bl.y + eh * Bh.y);
+    const double2 dvh = make_double2(-dm * C0.y - el * Dl.x + eh * Dh.x, dm * C0.x - el * Dl.y + eh * Dh.y);
+    const double ia = 1.0 / a, ll = dn * (dn + 1.0);
+    double2 ht = make_double2(-ia * dvh.x, -ia * dvh.y);
+    double2 zt = make_double2(-ia * dvf.x, -ia * dvf.y);
+    double2 dt = make_double2(ia * crf.x + ll * ia * ia * E0.x, ia * crf.y + ll * ia * ia * E0.y);
+    const int k = pidx(L, n, m);
+    if (visc != 0.0) {
+        const double c = Kp ? coef * dts[mem] : 0.0;
+        const double sc = -visc * ia * ia * ll;
+        double2 x[3];
+        for (int q = 0; q < 3; q++) {
+            x[q] = S[((size_t)mem * 3 + q) * nlm + k];
+            if (Kp) {
+                const double2 t = Kp[((size_t)mem * 3 + q) * nlm + k];
+                x[q].x += c * t.x;
+                x[q].y += c * t.y;
+            }
+        }
+        ht.x += sc * x[0].x; ht.y += sc * x[0].y;
+        zt.x += sc * x[1].x; zt.y += sc * x[1].y;
+        dt.x += sc * x[2].x; dt.y += sc * x[2].y;
+    }
+    double2* o = Ks + (size_t)mem * 3 * nlm;
+    o[k] = ht;
+    o[(size_t)nlm + k] = zt;
+    o[2 * (size_t)nlm + k] = dt;
+}
+
 // ------------------------------------------------------------------ host pipeline
 static SweConst make_const(const sph_swe_params* p) {
     SweConst k;
@@ -315,7 +442,7 @@ static SweConst make_const(const sph_swe_params* p) {
     k.omega = p->omega;
     k.h0 = p->h0;
     k.visc = p->viscosity;
-    k.mode = p->nonlinear == 2 ? 3 : (p->nonlinear ? 0 : (p->robert ? 2 : 1));
+    k.mode = p->nonlinear ? 0 : (p->robert ? 2 : 1);
     return k;
 }
 
@@ -340,12 +467,40 @@ static int swe_stage(Handle* h, RKState* r, const sph_swe_params* p, const doubl
     SPH_CUDA_TRY(cudaGetLastError());
     if (int rc = legendre_synthesis_real(h, r->X2, nlm, L, r->F2, fou, 2 * nmem, s)) return rc;
     k_fourier_h<<<dim3((unsigned)((fou + 255) / 256), nmem), 256, 0, s>>>(r->F2, r->Fh, h->cosphi, nlat, mF,
-                                                                          kc.mode >= 2 ? 2 : 1);
+                                                                          kc.mode == 2 ? 2 : 1);
     SPH_CUDA_TRY(cudaGetLastError());
     if (int rc = legendre_analysis_real(h, r->Fh, fou, r->Th, nlm, L, nmem, s)) return rc;
     k_rk_stage_out<<<dim3((L + 1 + 63) / 64, L + 1, nmem), 64, 0, s>>>(S, Kp, coef, r->dts, r->T4, r->Th, Ks, L, nlm, kc);
     SPH_CUDA_TRY(cudaGetLastError());
     return SPH_OK;
+}
+
+// one tendency evaluation of the vorticity-divergence form
+static int swe_stage_vd(Handle* h, RKState* r, const sph_swe_params* p, const double2* S, const double2* Kp,
+                        double coef, double2* Ks, int nmem, cudaStream_t s) {
+    const int L = h->L, Lp = L + 1, nlm = h->nlm, nlat = h->nlat, mF = L + 1;
+    const int nlmp = (Lp + 1) * (Lp + 2) / 2;
+    const long long fou = (long long)mF * nlat;
+    k_vd_prep<<<dim3((Lp + 1 + 63) / 64, Lp + 1, nmem), 64, 0, s>>>(S, Kp, coef, r->dts, r->X6, L, nlm, nlmp,
+                                                                     p->radius);
+    SPH_CUDA_TRY(cudaGetLastError());
+    if (int rc = legendre_synthesis_real(h, r->X6, nlmp, Lp, r->F6, fou, 4 * nmem, s)) return rc;
+    if (int rc = ring_synthesis_real(h, r->F6, fou, mF, r->G4, h->nspat, 4 * nmem, nullptr, nullptr, 0, 0, s)) return rc;
+    k_vd_pointwise<<<dim3((h->nspat + 255) / 256, nmem), 256, 0, s>>>(r->G4, r->G9, h->mu, h->cosphi, nlat, h->nspat,
+                                                                      p->gravity, p->omega);
+    SPH_CUDA_TRY(cudaGetLastError());
+    if (int rc = ring_analysis_real(h, r->G9, h->nspat, r->F6, fou, mF, 5 * nmem, s)) return rc;
+    if (int rc = legendre_analysis_real(h, r->F6, fou, r->X6, nlmp, Lp, 5 * nmem, s)) return rc;
+    k_vd_stage_out<<<dim3((L + 1 + 63) / 64, L + 1, nmem), 64, 0, s>>>(S, Kp, coef, r->dts, r->X6, Ks, L, nlm, nlmp,
+                                                                       p->radius, p->viscosity);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+static int swe_any_stage(Handle* h, RKState* r, const sph_swe_params* p, const double2* S, const double2* Kp,
+                         double coef, double2* Ks, int nmem, cudaStream_t s) {
+    if (p->nonlinear == 2) return swe_stage_vd(h, r, p, S, Kp, coef, Ks, nmem, s);
+    return swe_stage(h, r, p, S, Kp, coef, Ks, nmem, s);
 }
 
 static int swe_step(Handle* h, RKState* r, const sph_swe_params* p, double2* S, int nmem, cudaStream_t s) {
@@ -354,13 +509,29 @@ static int swe_step(Handle* h, RKState* r, const sph_swe_params* p, double2* S, 
     double2* K1 = r->K + st;
     double2* K2 = r->K + 2 * st;
     double2* K3 = r->K + 3 * st;
-    if (int rc = swe_stage(h, r, p, S, nullptr, 0.0, K0, nmem, s)) return rc;
-    if (int rc = swe_stage(h, r, p, S, K0, 0.5, K1, nmem, s)) return rc;
-    if (int rc = swe_stage(h, r, p, S, K1, 0.5, K2, nmem, s)) return rc;
-    if (int rc = swe_stage(h, r, p, S, K2, 1.0, K3, nmem, s)) return rc;
+    if (int rc = swe_any_stage(h, r, p, S, nullptr, 0.0, K0, nmem, s)) return rc;
+    if (int rc = swe_any_stage(h, r, p, S, K0, 0.5, K1, nmem, s)) return rc;
+    if (int rc = swe_any_stage(h, r, p, S, K1, 0.5, K2, nmem, s)) return rc;
+    if (int rc = swe_any_stage(h, r, p, S, K2, 1.0, K3, nmem, s)) return rc;
     const size_t tot = st;
     k_rk_final<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(S, r->K, r->dts, nmem, h->nlm, r->flag);
     SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+// kernel launches in a captured graph
+static int kernel_nodes(cudaGraph_t graph, int* out) {
+    size_t nodes = 0;
+    SPH_CUDA_TRY(cudaGraphGetNodes(graph, nullptr, &nodes));
+    std::vector<cudaGraphNode_t> list(nodes);
+    if (nodes) SPH_CUDA_TRY(cudaGraphGetNodes(graph, list.data(), &nodes));
+    int k = 0;
+    for (cudaGraphNode_t n : list) {
+        cudaGraphNodeType t;
+        SPH_CUDA_TRY(cudaGraphNodeGetType(n, &t));
+        if (t == cudaGraphNodeTypeKernel) k++;
+    }
+    *out = k;
     return SPH_OK;
 }
 
@@ -400,6 +571,7 @@ static int rk_run(Handle* h, const sph_swe_params* p, const double* dts_h, doubl
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) { set_error(std::string("graph capture: ") + cudaGetErrorString(e)); return SPH_ERR_CUDA; }
         r->graph = g;
+        if (int krc = kernel_nodes(g, &r->launches)) return krc;
         SPH_CUDA_TRY(cudaGraphInstantiate(&r->exec, g, 0));
         r->state = state;
         r->stream = s;
@@ -493,16 +665,7 @@ static int ensemble_capture(Ensemble* e) {
         return SPH_ERR_CUDA;
     }
     e->graph = graph;
-    size_t nodes = 0;
-    SPH_CUDA_TRY(cudaGraphGetNodes(graph, nullptr, &nodes));
-    std::vector<cudaGraphNode_t> list(nodes);
-    if (nodes) SPH_CUDA_TRY(cudaGraphGetNodes(graph, list.data(), &nodes));
-    e->launches = 0;
-    for (cudaGraphNode_t n : list) {
-        cudaGraphNodeType t;
-        SPH_CUDA_TRY(cudaGraphNodeGetType(n, &t));
-        if (t == cudaGraphNodeTypeKernel) e->launches++;
-    }
+    if (int rc = kernel_nodes(graph, &e->launches)) return rc;
     SPH_CUDA_TRY(cudaGraphInstantiate(&e->exec, graph, 0));
     return SPH_OK;
 }
@@ -580,8 +743,8 @@ int sph_swe_tendency(sph_handle* hh, const sph_swe_params* p, const double* stat
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     r->state = nullptr;  // dts[0] is overwritten: the cached step graph must be re-captured
     SPH_CUDA_TRY(cudaMemcpyAsync(r->dts, &p->dt, sizeof(double), cudaMemcpyHostToDevice, s));
-    if (int rc = swe_stage(h, r, p, reinterpret_cast<const double2*>(state), nullptr, 0.0,
-                           reinterpret_cast<double2*>(tend), 1, s))
+    if (int rc = swe_any_stage(h, r, p, reinterpret_cast<const double2*>(state), nullptr, 0.0,
+                               reinterpret_cast<double2*>(tend), 1, s))
         return rc;
     SPH_CUDA_TRY(cudaStreamSynchronize(s));
     return SPH_OK;
@@ -610,6 +773,12 @@ int sph_ensemble_create(int ngroups, sph_handle* const* handles, const sph_swe_p
 
 int sph_ensemble_step(sph_ensemble* e, int nsteps, void* stream) {
     return ensemble_run(reinterpret_cast<Ensemble*>(e), nsteps, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int sph_swe_rk4_launches(const sph_handle* hh) {
+    const Handle* h = reinterpret_cast<const Handle*>(hh);
+    const RKState* r = h ? static_cast<const RKState*>(h->rk) : nullptr;
+    return r && r->exec ? r->launches : 0;
 }
 
 int sph_ensemble_launches(const sph_ensemble* e) {

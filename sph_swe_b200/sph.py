@@ -138,6 +138,35 @@ class Sph:
                                           int(cplx), _stream()))
         return out
 
+    # ------------------------------------------------------------ autotuner
+    def autotune(self, batch: int) -> dict:
+        """Time the kernel variants for `batch` fields per launch, keep the
+        fastest in the handle, return the table (see sph_autotune)."""
+        import json
+
+        buf = ctypes.create_string_buffer(1 << 16)
+        capi.check(capi.lib().sph_autotune(self.h, batch, buf, len(buf), _stream()))
+        return json.loads(buf.value.decode())
+
+    def tune_load(self, table) -> None:
+        import json
+
+        text = table if isinstance(table, str) else json.dumps(table)
+        capi.check(capi.lib().sph_tune_load(self.h, text.encode()))
+
+    def tune_clear(self) -> None:
+        capi.check(capi.lib().sph_tune_clear(self.h))
+
+    @staticmethod
+    def rk4_batches(nmem: int, nonlinear: int = 1) -> list:
+        """Fields per launch of the transform stages of one RK4 stage over nmem
+        members: Legendre synthesis 6n and 2n, analysis 4n and n, ring
+        synthesis 9n, ring analysis 4n (reference forms); 4n and 5n for the
+        vorticity-divergence form (nonlinear = 2)."""
+        if nonlinear == 2:
+            return sorted({4 * nmem, 5 * nmem})
+        return sorted({6 * nmem, 2 * nmem, 4 * nmem, nmem, 9 * nmem})
+
     # ------------------------------------------------------------ SWE
     @staticmethod
     def swe_params(radius=6.37122e6, gravity=9.80616, omega=7.292e-5, h0=1e4, viscosity=0.0, dt=120.0,

@@ -1,0 +1,79 @@
+"""The autotuner (sph_autotune / sph_tune_load / sph_tune_clear): every
+candidate variant runs, the chosen table re-applies, and the transforms give
+the same results with any variant (column tiles are exact alternatives; the
+two P_l^m sources agree to the mixed-form tolerance)."""
+import numpy as np
+import pytest
+import torch
+
+from tests.helpers import random_spec, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("L,prec", [(63, 1), (127, 0), (255, 1)])
+def test_autotune_table_and_results(gpu, oracle_mod, L, prec):
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+
+    s = Sph(L, precision=prec)
+    nb = 24
+    spec = torch.from_numpy(random_spec(L, nb, seed=L)).cuda()
+    grid0 = s.SH_to_spat(spec)
+    back0 = s.spat_to_SH(grid0)
+    table = s.autotune(nb)
+    assert table["lmax"] == L and table["batch"] == nb
+    names = {k["name"] for k in table["kernels"]}
+    assert {"ring_analysis", "ring_synthesis"} <= names
+    if prec == capi.SPH_PREC_MIXED:
+        assert {"legendre_synthesis_tc", "legendre_analysis_tc"} <= names
+        tc = [k for k in table["kernels"] if k["name"].endswith("_tc")]
+        assert all(len(k["candidates"]) == 6 for k in tc)
+    for k in table["kernels"]:
+        assert k["us"] > 0 and k["us"] == min(c["us"] for c in k["candidates"])
+    grid1 = s.SH_to_spat(spec)
+    back1 = s.spat_to_SH(grid1)
+    capi.check(capi.lib().sph_sync(s.h, None))
+    tol = 1e-15 if prec == 0 else 1e-7
+    assert rel_l2(grid1.cpu().numpy(), grid0.cpu().numpy()) < tol
+    assert rel_l2(back1.cpu().numpy(), back0.cpu().numpy()) < tol
+    # every variant forced through a loaded table gives the same transforms
+    variants = [0, 1] if prec == 0 else [1, 2, 3, 5, 6, 7]
+    for v in variants:
+        forced = {"lmax": L, "nphi": s.nphi, "kernels": [
+            {"kind": kind, "batch": nb, "variant": (v if kind < 2 else v & 1)} for kind in range(4)]}
+        s.tune_load(forced)
+        g = s.SH_to_spat(spec)
+        assert rel_l2(g.cpu().numpy(), grid0.cpu().numpy()) < tol, v
+    s.tune_clear()
+    with pytest.raises(capi.SphError):
+        s.tune_load({"lmax": L + 1, "nphi": s.nphi, "kernels": [{"kind": 0, "batch": 1, "variant": 1}]})
+
+
+def test_autotuned_rk4_matches_untuned(gpu, oracle_mod):
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+    from tests.helpers import bump_state
+
+    L = 63
+    g = oracle_mod.Grid(L)
+    h = g.spat_to_SH(bump_state(g))
+    st0 = torch.from_numpy(np.stack([h, 0 * h, 0 * h])).cuda()
+    p = Sph.swe_params(radius=6.371e6, dt=120.0)
+    out = []
+    for tune in (False, True):
+        s = Sph(L, precision=capi.SPH_PREC_MIXED)
+        st = st0.clone()
+        s.swe_rk4(p, st, 5)  # captures the step graph with the built-in rules
+        if tune:
+            for b in Sph.rk4_batches(1):
+                s.autotune(b)
+            st = st0.clone()
+            s.swe_rk4(p, st, 5)  # re-captured with the tuned variants
+            assert capi.lib().sph_swe_rk4_launches(s.h) > 0
+        else:
+            st = st0.clone()
+            s.swe_rk4(p, st, 5)
+        out.append(st.cpu().numpy())
+    for q in range(3):
+        assert rel_l2(out[1][q], out[0][q]) < 1e-6 if q else rel_l2(out[1][q], out[0][q]) < 1e-9

@@ -35,18 +35,58 @@ def test_balanced_height_area_mean(oracle_mod):
 
 
 @pytest.mark.parametrize("L", [63, 127])
-def test_jet_is_steady_in_robert_nonlinear_form(oracle_mod, L):
+def test_jet_is_steady_in_vorticity_divergence_form(oracle_mod, L):
+    from oracle.vortdiv import VortDiv
+
     g = oracle_mod.Grid(L)
+    vd = VortDiv(g)
     h, u, v = S.sech2_jet(g, radius=A, bump_amp=0.0)
     c = np.cos(np.asarray(g.lat))[None, :]
-    hs, us, vs = g.spat_to_SH(h), g.spat_to_SH(u * c), g.spat_to_SH(v * c)
-    ht, ut, vt = g.swe_tendency((A, G, OM, 1e4, 0.0, 15.0), hs, us, vs, nonlinear=2, robert=1)
-    # the gravity term alone, for scale
-    _, _, vg = g.swe_tendency((A, G, 0.0, 1e4, 0.0, 15.0), hs, 0 * us, 0 * vs, nonlinear=2, robert=1)
-    scale = np.linalg.norm(vg)
-    assert np.linalg.norm(ht) < 1e-12 * scale
-    assert np.linalg.norm(ut) < 1e-12 * scale
-    assert np.linalg.norm(vt) < (1e-2 if L == 63 else 1e-5) * scale
+    z, d = vd.vec_analysis(u * c, v * c)
+    st = (g.spat_to_SH(h), z / A, d / A)
+    ht, zt, dt = vd.tendency((A, G, OM, 1e4, 0.0, 15.0), *st)
+    # advective scales u_max / a and u_max / (a width) of each field; the
+    # gravity term of the divergence equation
+    s_h = np.linalg.norm(st[0]) * 80.0 / A
+    s_z = np.linalg.norm(st[1]) * 80.0 / (A * 0.1)
+    s_d = np.linalg.norm(G * st[0]) / A ** 2 * L * L
+    assert np.linalg.norm(ht) < 1e-12 * s_h
+    assert np.linalg.norm(zt) < 1e-12 * s_z
+    assert np.linalg.norm(dt) < (1e-6 if L == 63 else 1e-10) * s_d
+
+
+def test_oracle_vector_transforms(oracle_mod):
+    """Exact vector pair of the oracle: round trip, and solid-body rotation
+    U = cos^2(phi) has vorticity 2 mu and no divergence."""
+    from oracle.vortdiv import VortDiv
+    from tests.helpers import random_spec
+
+    g = oracle_mod.Grid(31)
+    vd = VortDiv(g)
+    z, d = random_spec(31, 2, seed=4)
+    z[0] = d[0] = 0
+    z2, d2 = vd.vec_analysis(*vd.vec_synthesis(z, d))
+    assert np.linalg.norm(z2 - z) < 1e-13 * np.linalg.norm(z)
+    assert np.linalg.norm(d2 - d) < 1e-13 * np.linalg.norm(d)
+    mu = np.asarray(g.mu)
+    U = np.broadcast_to((1 - mu ** 2)[None, :], (g.nphi, g.nlat)).copy()
+    zz, dd = vd.vec_analysis(U, 0 * U)
+    ref = g.spat_to_SH(g.grid_from(lambda lon, m: 2 * m + 0 * lon))
+    assert np.abs(zz - ref).max() < 1e-12 and np.abs(dd).max() < 1e-14
+
+
+def test_vorticity_divergence_form_conserves_mass(oracle_mod):
+    from oracle.vortdiv import VortDiv
+
+    g = oracle_mod.Grid(31)
+    vd = VortDiv(g)
+    h, u, v = S.sech2_jet(g, radius=A, bump_amp=300.0)
+    c = np.cos(np.asarray(g.lat))[None, :]
+    z, d = vd.vec_analysis(u * c, v * c)
+    h0 = g.spat_to_SH(h)
+    out = vd.rk4((A, G, OM, 1e4, 0.0, 300.0), h0, z / A, d / A, 20)
+    assert abs(out[0][0] - h0[0]) < 1e-14 * abs(h0[0])
+    assert abs(out[1][0]) < 1e-20
 
 
 def test_galewsky_state_shapes(oracle_mod):
