@@ -382,7 +382,9 @@ def rk4_rates(dev, args):
 def rexi_rates(dev, args):
     """REXI configuration: T127 192x384, Robert linear SWE about h0 = 1e4 m,
     Gaussian-approximation REXI h = 0.2, M = 256 (535 poles), tau = 3600 s,
-    24 steps from the Gaussian bump; FP64 direct banded solves."""
+    24 steps from the Gaussian bump; FP64 direct and the mixed form (complex
+    FP32 factorisation and solves, two FP64 refinement steps), with the
+    relative L2 of the mixed state against the FP64 state."""
     import torch
 
     from sph_swe_b200 import capi
@@ -390,20 +392,26 @@ def rexi_rates(dev, args):
 
     s = Sph(127)
     a, br, _ = rexi_coefficients(0.2, 256, False)
-    rx = s.rexi(a, br, radius=6.371e6, tau=3600.0)
     st0 = _bump_state(s, dev)
-    st = st0.clone()
-    rx.step(st, 2)
-    torch.cuda.synchronize()
-    st = st0.clone()
     n = 24
-    ms = _time(lambda: rx.step(st, n), 1, torch.cuda.current_stream()) / n
-    capi.check(capi.lib().sph_sync(s.h, None))
-    out = {"T127_M256_fp64": {"steps_per_s": 1000.0 / ms, "ms_per_step": ms, "poles": int(len(a)), "nsteps": n,
-                              "tau": 3600.0}}
-    rx.close()
+    out, states = {}, {}
+    for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
+        rx = s.rexi(a, br, radius=6.371e6, tau=3600.0, precision=prec)
+        st = st0.clone()
+        rx.step(st, 2)
+        torch.cuda.synchronize()
+        st = st0.clone()
+        ms = _time(lambda: rx.step(st, n), 1, torch.cuda.current_stream()) / n
+        capi.check(capi.lib().sph_sync(s.h, None))
+        out[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms}
+        states[name] = st
+        rx.close()
+    rel = {q: float(torch.linalg.vector_norm(states["mixed"][k] - states["fp64"][k]) /
+                    max(float(torch.linalg.vector_norm(states["fp64"][k])), 1e-300)) for k, q in enumerate("huv")}
     s.close()
-    return out
+    return {"T127_M256": {**out, "poles": int(len(a)), "nsteps": n, "tau": 3600.0,
+                          "mixed_over_fp64": out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"],
+                          "mixed_rel_l2_vs_fp64_after_nsteps": rel}}
 
 
 def t1023_rates(dev, args):
@@ -476,7 +484,9 @@ def ensemble_rates(dev, args):
     """Ensemble configuration: 256 members (96 x T31, 96 x T63, 48 x T127,
     16 x T255), nonlinear RK4 with dt = 120 * 63 / T s, 100 steps, one CUDA
     graph replay per step for all members (each truncation on its own graph
-    branch).  FP64 and mixed form; the FP64 form is also timed group by group
+    branch).  The members integrate the vorticity-divergence form: the
+    reference's advective u, v form is unstable at T255 with dt = 29.6 s and no
+    viscosity (the T255 group blows up within the 100 steps).  FP64 and mixed form; the FP64 form is also timed group by group
     (one batched graph per truncation, run one after another) to show what the
     branches overlap; the mixed state is compared with the FP64 state."""
     import torch
@@ -498,7 +508,7 @@ def ensemble_rates(dev, args):
         groups = []
         for L, n in ENSEMBLE:
             s = Sph(L, precision=prec)
-            groups.append((s, Sph.swe_params(radius=6.371e6, dt=120.0 * 63 / L), init[L].clone(), None))
+            groups.append((s, Sph.swe_params(radius=6.371e6, dt=120.0 * 63 / L, nonlinear=2), init[L].clone(), None))
         e = Ensemble(groups)
         e.step(3)
         for (_, _, st, _), (L, _) in zip(groups, ENSEMBLE):
@@ -513,7 +523,7 @@ def ensemble_rates(dev, args):
             seq = 0.0
             for s, p, st, _ in groups:
                 st.copy_(init[s.L])
-                s.swe_rk4_batched(p, st, 3)
+                s.swe_rk4_batched(p, st, 3)  # one batched graph per truncation
                 torch.cuda.synchronize()
                 seq += _time(lambda: s.swe_rk4_batched(p, st, ENSEMBLE_STEPS), 1, stream) / ENSEMBLE_STEPS
             out[name]["ms_per_step_groups_one_after_another"] = seq
@@ -524,7 +534,7 @@ def ensemble_rates(dev, args):
     rel = {}
     for (L, n), a, b in zip(ENSEMBLE, finals["mixed"], finals["fp64"]):
         r = (torch.linalg.vector_norm(a - b, dim=2) / torch.linalg.vector_norm(b, dim=2)).max(dim=0).values
-        rel[f"T{L}"] = {q: float(r[k]) for k, q in enumerate("huv")}
+        rel[f"T{L}"] = {q: float(r[k]) for k, q in enumerate(("h", "vorticity", "divergence"))}
     out["members"] = {f"T{L}": n for L, n in ENSEMBLE}
     out["nsteps"] = ENSEMBLE_STEPS
     out["mixed_over_fp64"] = out["mixed"]["member_steps_per_s"] / out["fp64"]["member_steps_per_s"]

@@ -1,5 +1,7 @@
 // REXI time integrator for the linear shallow-water equations, Robert
-// formulation (SWERexiSPHRobert.hpp), FP64 direct.
+// formulation (SWERexiSPHRobert.hpp): FP64 direct, or (mixed form) complex
+// FP32 banded factorisation and solves with two steps of FP64 iterative
+// refinement (residuals of the FP64 system, corrections from the FP32 factors).
 //
 // Reference per step (AppSWE.hpp:414-566): for every pole (alpha_k, beta_k)
 // SWERexiSPHRobert::solve (SWERexiSPHRobert.hpp:139-258) promotes phi0 = g h,
@@ -59,7 +61,7 @@ struct RexiPlan {
     cudaStream_t stream = nullptr;
 };
 
-template <int MAXN>
+template <int MAXN, bool MIXED>
 __global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -76,7 +78,7 @@ __global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
     const double2 a = d.alpha[valid ? pole : 0];
     const double2 bt = valid ? d.beta[pole] : make_double2(0, 0);
     double2 phi[MAXN], ra[MAXN], rb[MAXN];
-    const bool ok = rexi_lane<MAXN>(d, m, a, phi, ra, rb);
+    const bool ok = rexi_lane<MAXN, MIXED>(d, m, a, phi, ra, rb);
     if (!ok && valid) atomicOr(d.flag, 2);
     // beta scaling and reduction over the 32 poles of this warp
     double2* outp = d.part + (size_t)g * 3 * nc;
@@ -242,6 +244,8 @@ static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     d.ngroups = R->ngroups;
     d.ncplx = nc;
     d.coriolis = (R->p.coriolis && R->p.omega != 0.0) ? 1 : 0;
+    // mixed form: complex FP32 factorisation and solves, two FP64 refinement steps
+    d.refine = R->p.precision == SPH_PREC_MIXED ? 2 : 0;
     d.r = R->p.radius;
     d.ir = ir;
     d.T = 2.0 * R->p.omega;
@@ -256,9 +260,15 @@ static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     d.flag = R->flag;
     const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
     const unsigned nb = (unsigned)((nthreads + 63) / 64);
-    if (L + 1 <= 64) k_rexi_solve<64><<<nb, 64, 0, s>>>(d);
-    else if (L + 1 <= 128) k_rexi_solve<128><<<nb, 64, 0, s>>>(d);
-    else k_rexi_solve<256><<<nb, 64, 0, s>>>(d);
+    if (d.refine > 0) {
+        if (L + 1 <= 64) k_rexi_solve<64, true><<<nb, 64, 0, s>>>(d);
+        else if (L + 1 <= 128) k_rexi_solve<128, true><<<nb, 64, 0, s>>>(d);
+        else k_rexi_solve<256, true><<<nb, 64, 0, s>>>(d);
+    } else {
+        if (L + 1 <= 64) k_rexi_solve<64, false><<<nb, 64, 0, s>>>(d);
+        else if (L + 1 <= 128) k_rexi_solve<128, false><<<nb, 64, 0, s>>>(d);
+        else k_rexi_solve<256, false><<<nb, 64, 0, s>>>(d);
+    }
     SPH_CUDA_TRY(cudaGetLastError());
     const double visc_fac = R->p.viscosity * R->p.tau / (R->p.radius * R->p.radius);
     k_rx_finish<<<gr, 64, 0, s>>>(R->part, R->ngroups, nc, state, L, nlm, 1.0 / g, visc_fac, R->flag);
@@ -296,8 +306,8 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
         set_error("sph_rexi_create: only the Robert formulation (SWERexiSPHRobert) runs on the GPU path");
         return SPH_ERR_ARG;
     }
-    if (p->precision != SPH_PREC_FP64) {
-        set_error("sph_rexi_create: precision must be SPH_PREC_FP64 in this build");
+    if (p->precision != SPH_PREC_FP64 && p->precision != SPH_PREC_MIXED) {
+        set_error("sph_rexi_create: precision must be SPH_PREC_FP64 or SPH_PREC_MIXED");
         return SPH_ERR_ARG;
     }
     if (h->L > 255) {

@@ -20,6 +20,7 @@ namespace sphgpu {
 struct RexiDev {
     int L, npoles, ngroups, ncplx;
     int coriolis;
+    int refine;  // 0: FP64 direct; k > 0: complex FP32 factor/solve + k FP64 refinement steps
     double r, ir, T, P;  // radius, 1/radius, 2 Omega, average geopotential
     const double2* alpha;
     const double2* beta;
@@ -152,10 +153,163 @@ __host__ __device__ bool band_solve(int Np, Entry entry, Rhs rhs, Out out) {
     return ok;
 }
 
+__host__ __device__ inline float2 f_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ inline float2 f_mul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ inline float2 f_div(float2 a, float2 b) {
+    const float d = b.x * b.x + b.y * b.y;
+    return make_float2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__host__ __device__ inline float f_abs1(float2 a) { return fabsf(a.x) + fabsf(a.y); }
+__host__ __device__ inline float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
+__host__ __device__ inline double2 to_d(float2 a) { return make_double2((double)a.x, (double)a.y); }
+
+// The same banded system as band_solve, factored once in complex FP32 (LAPACK
+// pivot rule on |re|+|im| of the FP32 entries; U rows, multipliers and pivot
+// offsets kept per thread) and solved in FP32; then `refine` steps of FP64
+// iterative refinement: r = b - A x with A and b in FP64 (entry / rhs), the
+// correction solved with the FP32 factors, x += correction in FP64.
+template <int H, int MAXR, int NR, class Entry, class Rhs, class Out>
+__host__ __device__ bool band_solve_mixed(int Np, int refine, Entry entry, Rhs rhs, Out out) {
+    constexpr int W = 2 * H + 1;
+    float2 U[MAXR][W];
+    float2 Lm[MAXR][H];
+    signed char pv[MAXR];
+    double2 x[MAXR][NR];
+    float2 win[H + 1][W];
+#pragma unroll
+    for (int i = 0; i <= H; i++)
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - i;
+            win[i][j] = (i < Np && d >= -H && d <= H && j < Np) ? to_f(entry(i, d)) : make_float2(0.f, 0.f);
+        }
+    bool ok = true;
+    for (int k = 0; k < Np; k++) {
+        int p = 0;
+        float best = f_abs1(win[0][0]);
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const float v = (k + i < Np) ? f_abs1(win[i][0]) : -1.f;
+            if (v > best) {
+                best = v;
+                p = i;
+            }
+        }
+        if (best == 0.f) ok = false;
+        pv[k] = (signed char)p;
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < W; j++) {
+                const float2 t0 = win[0][j], ti = win[i][j];
+                win[0][j] = sw ? ti : t0;
+                win[i][j] = sw ? t0 : ti;
+            }
+        }
+        const float2 rp = best == 0.f ? make_float2(0.f, 0.f) : f_div(make_float2(1.f, 0.f), win[0][0]);
+#pragma unroll
+        for (int j = 0; j < W; j++) U[k][j] = win[0][j];
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const float2 l = f_mul(win[i][0], rp);
+            Lm[k][i - 1] = l;
+#pragma unroll
+            for (int j = 1; j < W; j++) win[i][j] = f_sub(win[i][j], f_mul(l, win[0][j]));
+        }
+#pragma unroll
+        for (int i = 0; i < H; i++) {
+#pragma unroll
+            for (int j = 0; j < W - 1; j++) win[i][j] = win[i + 1][j + 1];
+            win[i][W - 1] = make_float2(0.f, 0.f);
+        }
+        const int rn = k + 1 + H;
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - H;
+            win[H][j] = (rn < Np && k + 1 + j < Np) ? to_f(entry(rn, d)) : make_float2(0.f, 0.f);
+        }
+    }
+    // solve with the FP32 factors; b(k, r) gives the right-hand side, the
+    // solution is added to x (first pass: stored)
+    auto lu_solve = [&](auto b, bool add) {
+        float2 wr[H + 1][NR];
+#pragma unroll
+        for (int i = 0; i <= H; i++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[i][r] = i < Np ? to_f(b(i, r)) : make_float2(0.f, 0.f);
+        float2 y[MAXR][NR];
+        for (int k = 0; k < Np; k++) {
+            const int p = pv[k];
+#pragma unroll
+            for (int i = 1; i <= H; i++) {
+                const bool sw = (p == i);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const float2 t0 = wr[0][r], ti = wr[i][r];
+                    wr[0][r] = sw ? ti : t0;
+                    wr[i][r] = sw ? t0 : ti;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < NR; r++) y[k][r] = wr[0][r];
+#pragma unroll
+            for (int i = 1; i <= H; i++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) wr[i][r] = f_sub(wr[i][r], f_mul(Lm[k][i - 1], wr[0][r]));
+#pragma unroll
+            for (int i = 0; i < H; i++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) wr[i][r] = wr[i + 1][r];
+            const int rn = k + 1 + H;
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[H][r] = rn < Np ? to_f(b(rn, r)) : make_float2(0.f, 0.f);
+        }
+        float2 xs[W][NR];
+#pragma unroll
+        for (int j = 0; j < W; j++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) xs[j][r] = make_float2(0.f, 0.f);
+        for (int k = Np - 1; k >= 0; k--) {
+            const float2 rd = f_div(make_float2(1.f, 0.f), U[k][0]);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                float2 sm = y[k][r];
+#pragma unroll
+                for (int j = 1; j < W; j++) sm = f_sub(sm, f_mul(U[k][j], xs[j - 1][r]));
+                const float2 xk = f_mul(sm, rd);
+#pragma unroll
+                for (int j = W - 1; j > 0; j--) xs[j][r] = xs[j - 1][r];
+                xs[0][r] = xk;
+                x[k][r] = add ? c_add(x[k][r], to_d(xk)) : to_d(xk);
+            }
+        }
+    };
+    lu_solve([&](int k, int r) { return rhs(k, r); }, false);
+    for (int it = 0; it < refine; it++) {
+        // residual r = b - A x in FP64 (entry(k, d) = A[k][k+d])
+        lu_solve(
+            [&](int k, int r) {
+                double2 v = rhs(k, r);
+#pragma unroll
+                for (int d = -H; d <= H; d++)
+                    if (k + d >= 0 && k + d < Np) v = c_sub(v, c_mul(entry(k, d), x[k + d][r]));
+                return v;
+            },
+            true);
+    }
+    for (int k = 0; k < Np; k++)
+#pragma unroll
+        for (int r = 0; r < NR; r++) out(k, r, x[k][r]);
+    return ok;
+}
+
 // One pole, one m-block: Phi solve (both l-parities), velocity right-hand
 // sides and the two velocity solves.  Writes the unscaled phi, u, v of the
 // block's N = L+1-|m| rows to phi / ra / rb; returns false on a zero pivot.
-template <int MAXN>
+template <int MAXN, bool MIXED = false>
 __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* phi, double2* ra, double2* rb) {
     const int L = d.L;
     const int am = m < 0 ? -m : m;
@@ -203,7 +357,10 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
                 return v;
             };
             auto out = [&](int k, int, double2 x) { phi[par + 2 * k] = x; };
-            ok = band_solve<2, (MAXN + 1) / 2, 1>(Np, entry, rhs, out) && ok;
+            if constexpr (MIXED)
+                ok = band_solve_mixed<2, (MAXN + 1) / 2, 1>(Np, d.refine, entry, rhs, out) && ok;
+            else
+                ok = band_solve<2, (MAXN + 1) / 2, 1>(Np, entry, rhs, out) && ok;
         }
         // rhsa = a u0 + a ir i m phi - T mu(v0) - T ir mu(D phi)
         // rhsb = T mu(u0) + T ir mu(i m phi) + a v0 + a ir D phi
@@ -254,7 +411,10 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
                 if (r == 0) ra[par + 2 * k] = x;
                 else rb[par + 2 * k] = x;
             };
-            ok = band_solve<1, (MAXN + 1) / 2, 2>(Np, entry, rhs2, out2) && ok;
+            if constexpr (MIXED)
+                ok = band_solve_mixed<1, (MAXN + 1) / 2, 2>(Np, d.refine, entry, rhs2, out2) && ok;
+            else
+                ok = band_solve<1, (MAXN + 1) / 2, 2>(Np, entry, rhs2, out2) && ok;
         }
     } else {
         // phi = (P div0 + a phi0) / (a^2 + (P/r^2) n(n+1)); u = (u0 + ir i m phi)/a; v = (v0 + ir D phi)/a

@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 P6 = (6.371e6, 9.80616, 7.292e-5, 1e4, 0.0, 3600.0)
 
 
-def _run(gpu_sph, g, oracle_mod, L, M, half, steps, coriolis=1, fix=0, visc=0.0, seed=None):
+def _run(gpu_sph, g, oracle_mod, L, M, half, steps, coriolis=1, fix=0, visc=0.0, seed=None, precision=0):
     a, br, bi = oracle_mod.rexi_coeffs(0.2, M, half=half)
     h = g.spat_to_SH(bump_state(g))
     if seed is None:
@@ -23,7 +23,7 @@ def _run(gpu_sph, g, oracle_mod, L, M, half, steps, coriolis=1, fix=0, visc=0.0,
     p = list(P6)
     p[4] = visc
     rx = gpu_sph.rexi(a, br, radius=p[0], gravity=p[1], omega=p[2], h0=p[3], viscosity=visc, tau=p[5],
-                      coriolis=coriolis, fix_z5robert=fix)
+                      coriolis=coriolis, fix_z5robert=fix, precision=precision)
     st = torch.from_numpy(np.stack([h, u, v])).cuda()
     rx.step(st, steps)
     out = st.cpu().numpy()
@@ -58,6 +58,40 @@ def test_rexi_config2_t127_full_poles(gpu, oracle_mod):
     out, ref = _run(s, g, oracle_mod, 127, 256, False, 1)
     for q in range(3):
         assert rel_l2(out[q], ref[q]) < 1e-10, q
+
+
+@pytest.mark.parametrize("L,M,half,coriolis,seed", [(31, 64, False, 1, 3), (31, 32, True, 0, 4), (63, 64, False, 1, 6)])
+def test_mixed_rexi_matches_oracle(gpu, oracle_mod, L, M, half, coriolis, seed):
+    """Complex FP32 factorisation and solves with two FP64 refinement steps:
+    the refined solution reaches the FP64 result to ~1e-12 (tolerance 1e-9)."""
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+
+    s, g = Sph(L), oracle_mod.Grid(L)
+    out, ref = _run(s, g, oracle_mod, L, M, half, 2, coriolis, 0, 0.0, seed, precision=capi.SPH_PREC_MIXED)
+    for q in range(3):
+        assert rel_l2(out[q], ref[q]) < 1e-9, q
+
+
+def test_mixed_rexi_config2_24_steps_vs_fp64(gpu, oracle_mod):
+    """REXI configuration (T127, M = 256, 535 poles, tau = 3600 s), 24 steps:
+    mixed form against the FP64 direct form."""
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph, rexi_coefficients
+
+    s, g = Sph(127), oracle_mod.Grid(127)
+    a, br, _ = rexi_coefficients(0.2, 256, False)
+    h = g.spat_to_SH(bump_state(g))
+    st0 = torch.from_numpy(np.stack([h, 0 * h, 0 * h])).cuda()
+    outs = []
+    for prec in (capi.SPH_PREC_FP64, capi.SPH_PREC_MIXED):
+        rx = s.rexi(a, br, radius=6.371e6, tau=3600.0, precision=prec)
+        st = st0.clone()
+        rx.step(st, 24)
+        outs.append(st.cpu().numpy())
+        rx.close()
+    for q in range(3):
+        assert rel_l2(outs[1][q], outs[0][q]) < 1e-9, q
 
 
 def test_rexi_rejects_unsupported(gpu):
