@@ -398,20 +398,22 @@ def rexi_rates(dev, args):
     for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
         rx = s.rexi(a, br, radius=6.371e6, tau=3600.0, precision=prec)
         st = st0.clone()
-        rx.step(st, 2)
+        rx.step(st, 2)  # warm-up; also the accuracy sample (see below)
+        states[name] = st
         torch.cuda.synchronize()
         st = st0.clone()
         ms = _time(lambda: rx.step(st, n), 1, torch.cuda.current_stream()) / n
         capi.check(capi.lib().sph_sync(s.h, None))
         out[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms}
-        states[name] = st
         rx.close()
     rel = {q: float(torch.linalg.vector_norm(states["mixed"][k] - states["fp64"][k]) /
                     max(float(torch.linalg.vector_norm(states["fp64"][k])), 1e-300)) for k, q in enumerate("huv")}
     s.close()
+    # the reference's Robert REXI integration is not stable over many steps at
+    # this size (the oracle grows without bound as well): accuracy after 2 steps
     return {"T127_M256": {**out, "poles": int(len(a)), "nsteps": n, "tau": 3600.0,
                           "mixed_over_fp64": out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"],
-                          "mixed_rel_l2_vs_fp64_after_nsteps": rel}}
+                          "mixed_rel_l2_vs_fp64_after_2_steps": rel}}
 
 
 def t1023_rates(dev, args):
