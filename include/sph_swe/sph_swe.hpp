@@ -22,7 +22,9 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <fstream>
 #include <functional>
+#include <iomanip>
 #include <map>
 #include <mutex>
 #include <stdexcept>
@@ -341,6 +343,20 @@ class SPHData {
         data_spat_valid = false;
     }
 
+    // host grid (nphi x nlat, theta-contiguous) -> this field's grid
+    void spat_from_host(const std::vector<double>& v) {
+        if (v.size() != (size_t)sphConfig->spat_num_elems) throw std::runtime_error("spat_from_host: wrong size");
+        cuda_check(cudaMemcpyAsync(data_spat, v.data(), spat_bytes(), cudaMemcpyHostToDevice, sphConfig->stream), "ul");
+        cuda_check(cudaStreamSynchronize(sphConfig->stream), "sync");
+        data_spat_valid = true;
+        data_spec_valid = false;
+    }
+    // the spectral array was written directly (by a C-ABI call on data_spec)
+    void mark_spectral() {
+        data_spec_valid = true;
+        data_spat_valid = false;
+    }
+
     std::vector<cplx> spec_to_host() const {
         request_data_spectral();
         std::vector<cplx> v((size_t)sphConfig->spec_num_elems);
@@ -354,6 +370,39 @@ class SPHData {
         cuda_check(cudaMemcpyAsync(v.data(), data_spat, spat_bytes(), cudaMemcpyDeviceToHost, sphConfig->stream), "dl");
         cuda_check(cudaStreamSynchronize(sphConfig->stream), "sync");
         return v;
+    }
+
+    // grid as a tab-separated table in the reference's CSV layout (SPHData.hpp:935-1037):
+    // "#TI title", "#TX Longitude", "#TY Latitude", then "0" and the longitudes in
+    // degrees, then one row per latitude ring j = nlat-1 .. 0 (south to north)
+    // with the latitude in degrees first; `shifted` moves longitude 0 to the
+    // middle (spat_write_file_lon_pi_shifted)
+    void spat_write_file(const char* filename, const char* title = "", int precision = 8, bool shifted = false) const {
+        const auto v = spat_to_host();
+        const int nlon = sphConfig->spat_num_lon, nlat = sphConfig->spat_num_lat;
+        std::ofstream f(filename, std::ios_base::trunc);
+        if (!f) throw std::runtime_error(std::string("cannot write ") + filename);
+        f << std::setprecision(precision);
+        f << "#TI " << title << "\n#TX Longitude\n#TY Latitude\n0\t";
+        for (int i = 0; i < nlon; i++) {
+            const double lon = (double)i / nlon * 2.0 * M_PI;
+            f << ((shifted ? lon - M_PI : lon) / M_PI * 180.0);
+            if (i < nlon - 1) f << "\t";
+        }
+        f << "\n";
+        for (int j = nlat - 1; j >= 0; j--) {
+            f << sphConfig->lat[j] / M_PI * 180.0 << "\t";
+            for (int i = 0; i < nlon; i++) {
+                int ia = shifted ? i + nlon / 2 : i;
+                if (ia >= nlon) ia -= nlon;
+                f << v[(size_t)ia * nlat + j];
+                if (i < nlon - 1) f << "\t";
+            }
+            f << "\n";
+        }
+    }
+    void spat_write_file_lon_pi_shifted(const char* filename, const char* title = "", int precision = 8) const {
+        spat_write_file(filename, title, precision, true);
     }
 
     // reductions on the grid (SPHData.hpp:800-876) and the NaN check (SPHData.hpp:560-569,

@@ -14,9 +14,18 @@
 // writes the final spectral state [h | u | v] (complex128, packed layout) to a
 // file.  Programs: P0 (shallow-water run); the reference's test programs
 // P1..P5 are not part of this driver.
-// Scenarios: Q0 the reference's Gaussian bump (AppSWE.hpp:99-128), Q10 the
-// 500 m bump at (30N, 60E) with sigma = 0.1 a of the plain-method configuration.
-// Initial velocities are zero; with Robert variables the state is U, V.
+// Scenarios: Q0 the reference's Gaussian bump (AppSWE.hpp:99-128), Q1 the
+// Galewsky barotropic jet with its height bump (BenchmarkGalewsky.hpp:18-243:
+// zonal jet between pi/7 and pi/2 - pi/7, depth in gradient-wind balance
+// integrated ring by ring with the reference's area mean), Q10 the 500 m bump
+// at (30N, 60E) with sigma = 0.1 a of the plain-method configuration.  With
+// Robert variables the velocity state is U, V = u cos(phi), v cos(phi); with N2
+// it is the vorticity and divergence.
+// Output as the reference's AppSWE::write_output (AppSWE.hpp:60-95): at t = 0,
+// every O seconds of simulated time and at the end, the grids of h, u, v and
+// the vorticity as CSV files prog_{h,u,v,eta}_t<hours>.csv (longitude 0 in the
+// middle for Q0); with N2: prog_h, prog_eta (vorticity), prog_div.  O <= 0
+// means every half hour.
 #include <sph_swe/sph_swe.hpp>
 
 #include <algorithm>
@@ -26,7 +35,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <functional>
 #include <iostream>
+#include <vector>
 #include <string>
 
 using namespace sph_swe;
@@ -98,7 +109,107 @@ int parse(int argc, char** argv, Vars& v) {
     return 0;
 }
 
-void initial_state(const Vars& v, SPHData& h, SPHData& u, SPHData& w) {
+// Gauss-Legendre rule of n points on [-1, 1] (Newton on P_n)
+void gauss_rule(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    for (int k = 0; k < (n + 1) / 2; k++) {
+        double z = std::cos(M_PI * (k + 0.75) / (n + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; it++) {
+            double p0 = 1.0, p1 = z;
+            for (int i = 2; i <= n; i++) {
+                const double p2 = ((2.0 * i - 1.0) * z * p1 - (i - 1.0) * p0) / i;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-15) break;
+        }
+        x[k] = -z;
+        x[n - 1 - k] = z;
+        w[k] = w[n - 1 - k] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+// depth on the rings lat[j] (j = 0 north) in gradient-wind balance with the
+// zonal flow u(phi): g dh/dphi = -a u (2 Omega sin(phi) + u tan(phi) / a),
+// integrated from the south pole ring by ring (24-point Gauss rule per
+// interval) and shifted to the area mean h_avg with the reference's
+// ring-interval area terms (BenchmarkGalewsky.hpp:101-218)
+std::vector<double> balanced_height(const double* lat, int nlat, const std::function<double(double)>& u, double a,
+                                    double g, double om, double h_avg) {
+    std::vector<double> gx, gw;
+    gauss_rule(24, gx, gw);
+    auto integ = [&](double lo, double hi) {
+        const double mid = 0.5 * (lo + hi), half = 0.5 * (hi - lo);
+        double sum = 0.0;
+        for (int i = 0; i < 24; i++) {
+            const double phi = mid + half * gx[i], uu = u(phi);
+            sum += gw[i] * a * uu * (2.0 * om * std::sin(phi) + std::tan(phi) / a * uu);
+        }
+        return half * sum;
+    };
+    std::vector<double> edges;
+    edges.push_back(-0.5 * M_PI);
+    for (int j = nlat - 1; j >= 0; j--) edges.push_back(lat[j]);
+    edges.push_back(0.5 * M_PI);
+    std::vector<double> hg(edges.size() - 1);
+    double acc = 0.0, hsum = 0.0, area = 0.0;
+    for (size_t k = 0; k + 1 < edges.size(); k++) {
+        acc -= integ(edges[k], edges[k + 1]);
+        hg[k] = acc;
+        const double mterm = (std::sin(edges[k + 1]) - std::sin(edges[k])) * 2.0 * M_PI;
+        hsum += hg[k] * mterm;
+        area += mterm;
+    }
+    const double shift = h_avg - hsum / g / area;
+    std::vector<double> h(nlat);
+    for (int j = 0; j < nlat; j++) h[j] = hg[nlat - 1 - j] / g + shift;
+    return h;
+}
+
+void initial_state(const Vars& v, SPHConfig& cfg, SPHData& h, SPHData& u, SPHData& w) {
+    if (v.scenario == 1) {
+        // BenchmarkGalewsky.hpp:18-36 (constants), 59-71 (jet), 221-229 (bump)
+        const double phi0 = M_PI / 7.0, phi1 = 0.5 * M_PI - phi0, umax = 80.0;
+        const double en = std::exp(-4.0 / ((phi1 - phi0) * (phi1 - phi0)));
+        auto ujet = [&](double phi) {
+            return (phi <= phi0 || phi >= phi1) ? 0.0 : umax / en * std::exp(1.0 / ((phi - phi0) * (phi - phi1)));
+        };
+        const std::vector<double> hr =
+            balanced_height(cfg.lat, cfg.spat_num_lat, ujet, v.radius, v.gravity, v.omega, v.h0);
+        const double phi2 = M_PI / 4.0, alpha = 1.0 / 3.0, beta = 1.0 / 15.0, hhat = 120.0;
+        std::vector<double> hg((size_t)cfg.spat_num_elems), ug((size_t)cfg.spat_num_elems);
+        for (int i = 0; i < cfg.spat_num_lon; i++) {
+            const double lam = 2.0 * M_PI * i / cfg.spat_num_lon;
+            for (int j = 0; j < cfg.spat_num_lat; j++) {
+                const double phi = cfg.lat[j];
+                const size_t k = (size_t)i * cfg.spat_num_lat + j;
+                hg[k] = hr[j] + hhat * std::cos(phi) * std::exp(-std::pow((lam - M_PI) / alpha, 2.0)) *
+                                    std::exp(-std::pow((phi2 - phi) / beta, 2.0));
+                ug[k] = ujet(phi) * ((v.robert || v.nonlinear == 2) ? std::cos(phi) : 1.0);
+            }
+        }
+        h.spat_from_host(hg);
+        u.spat_from_host(ug);
+        w.spat_set_zero();
+        if (v.nonlinear == 2) {
+            // vorticity-divergence state from the Robert velocities (exact vector analysis)
+            SPHData z(&cfg), d(&cfg);
+            u.request_data_physical();
+            w.request_data_physical();
+            check(sph_vec_spat_to_SH(cfg.handle(), u.data_spat, w.data_spat, reinterpret_cast<double*>(z.data_spec),
+                                     reinterpret_cast<double*>(d.data_spec), 1, 1, cfg.s()),
+                  "sph_vec_spat_to_SH");
+            z.mark_spectral();
+            d.mark_spectral();
+            u = z * (1.0 / v.radius);
+            w = d * (1.0 / v.radius);
+        }
+        return;
+    }
     if (v.scenario == 10) {
         const double lat0 = M_PI / 6.0, lon0 = M_PI / 3.0;
         h.spat_update_lambda_gaussian_grid([&](double lon, double mu, double& o) {
@@ -148,7 +259,7 @@ int main(int argc, char** argv) {
                     (int)v.use_rexi, v.rexi_M, v.rexi_h, (int)v.half_poles);
 
         SPHData h(&cfg), u(&cfg), w(&cfg);
-        initial_state(v, h, u, w);
+        initial_state(v, cfg, h, u, w);
         h.request_data_spectral();
         u.request_data_spectral();
         w.request_data_spectral();
@@ -164,7 +275,40 @@ int main(int argc, char** argv) {
         p.use_vort_div_form = v.nonlinear == 2;
 
         const long long nsteps = (long long)std::llround(v.tend / v.dt);
-        const long long out_every = v.out_dt > 0.0 ? std::max<long long>(1, std::llround(v.out_dt / v.dt)) : nsteps;
+        const double out_dt = v.out_dt > 0.0 ? v.out_dt : 1800.0;
+        double next_out = 0.0;
+        // AppSWE::write_output (AppSWE.hpp:60-95)
+        auto write_output = [&](double t) {
+            char name[128];
+            const bool shifted = v.scenario == 0;
+            auto put = [&](const char* field, const SPHData& x, const char* title) {
+                std::snprintf(name, sizeof name, "prog_%s_t%020.8f.csv", field, t / 3600.0);
+                x.spat_write_file(name, title, 8, shifted);
+                return std::string(name);
+            };
+            const std::string fh = put("h", h, "");
+            std::printf("%s (min: %g, max: %g)\n", fh.c_str(), h.spat_reduce_min(), h.spat_reduce_max());
+            if (v.nonlinear == 2) {
+                std::printf("%s\n", put("eta", u, "vorticity").c_str());
+                std::printf("%s\n", put("div", w, "divergence").c_str());
+            } else {
+                std::printf("%s\n", put("u", u, "").c_str());
+                std::printf("%s\n", put("v", w, "").c_str());
+                const SPHData eta = SPHOperators::vort(u, w) * (1.0 / v.radius);
+                std::printf("%s\n", put("eta", eta, shifted ? "vorticity, lon pi shifted" : "").c_str());
+            }
+        };
+        // steps until the next output time (as the reference: output when t >= next_out)
+        auto steps_to_output = [&](long long done) {
+            const double t = done * v.dt;
+            if (t >= next_out) {
+                write_output(t);
+                next_out += out_dt;
+                if (next_out < t) next_out = t;
+            }
+            const long long k = (long long)std::ceil((next_out - t) / v.dt - 1e-9);
+            return std::max<long long>(1, std::min(k, nsteps - done));
+        };
         const auto t0 = std::chrono::steady_clock::now();
         long long done = 0;
         if (v.use_rexi) {
@@ -175,20 +319,19 @@ int main(int argc, char** argv) {
             std::printf(" + REXI poles: %zu\n", rexi.alpha.size());
             SWERexiRobert stepper(&cfg, p, rexi, v.dt, false, v.precision);
             while (done < nsteps) {
-                const int k = (int)std::min(out_every, nsteps - done);
-                stepper.run(h, u, w, k);
+                const long long k = steps_to_output(done);
+                stepper.run(h, u, w, (int)k);
                 done += k;
-                std::printf("t = %g  h in [%.6f, %.6f]\n", done * v.dt, h.spat_reduce_min(), h.spat_reduce_max());
             }
         } else {
             SWERK4 stepper(&cfg, p);
             while (done < nsteps) {
-                const int k = (int)std::min(out_every, nsteps - done);
-                stepper.run(h, u, w, v.dt, k);
+                const long long k = steps_to_output(done);
+                stepper.run(h, u, w, v.dt, (int)k);
                 done += k;
-                std::printf("t = %g  h in [%.6f, %.6f]\n", done * v.dt, h.spat_reduce_min(), h.spat_reduce_max());
             }
         }
+        write_output(done * v.dt);
         cuda_check(cudaDeviceSynchronize(), "sync");
         const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::printf("steps %lld  wall %.3f s  (%.1f steps/s incl. output)\n", done, secs, done / secs);

@@ -90,6 +90,9 @@ struct MixedTables {
     int zA = 0;
     bool streamed = false;
     CUtensorMap mapS, mapA;
+    // B operand prepared by the loader-only kernel (legendre_tcb.cuh)
+    float* Bbuf = nullptr;
+    size_t Bcap = 0;
 };
 
 // Offsets of degree m's blocks in the coefficient and checkpoint tables of
@@ -375,7 +378,7 @@ int tc_tables_build(Handle* h, int lmax) {
 void tc_tables_free(Handle* h) {
     MixedTables* T = static_cast<MixedTables*>(h->mixed);
     if (!T) return;
-    void* bufs[] = {T->ab, T->ck, T->ckx, T->flag, T->S, T->A, T->soff, T->aoff};
+    void* bufs[] = {T->ab, T->ck, T->ckx, T->flag, T->S, T->A, T->soff, T->aoff, T->Bbuf};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete T;
@@ -1019,6 +1022,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
 }
 
 #include "legendre_tcs.cuh"
+#include "legendre_tcb.cuh"
 
 // rows: padded row count (a multiple of 64), slices: z extent
 static int encode_map(CUtensorMap* map, float* base, unsigned long long rows, unsigned long long slices) {
@@ -1079,6 +1083,10 @@ static int tcs_tables_build(Handle* h, MixedTables* T) {
 
 template <int NC>
 static int tc_attr() {
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tcb<SynB<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, tsb::BYTES));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tcb<AnaB<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, tsb::BYTES));
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tcs<SynS<NC>, NC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, tss::BYTES));
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tcs<AnaS<NC>, NC>,
@@ -1195,6 +1203,101 @@ static int tcs_launch(const CUtensorMap& map, TsArgs& a, int nrt, int nm, const 
     return SPH_OK;
 }
 
+// bytes of prepared B stages for `cols` real columns (a multiple of the tile width)
+static size_t tcb_bytes(const Handle* h, bool syn, int lmax, int cols) {
+    const int nm = std::min(lmax, h->L) + 1;
+    const long long chunks = syn ? tcb_syn_coff(lmax, nm) : (long long)nm * ((h->nh + tc::KC - 1) / tc::KC);
+    return (size_t)chunks * (size_t)cols * tc::KC * 4 * sizeof(float);
+}
+
+// grow the B buffer; inside a stream capture it must already be large enough
+static int tcb_ensure(MixedTables* T, size_t bytes, cudaStream_t s) {
+    if (bytes <= T->Bcap) return SPH_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    SPH_CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+        set_error("tensor-core Legendre stage: operand workspace not reserved before stream capture");
+        return SPH_ERR_ARG;
+    }
+    if (T->Bbuf) {
+        SPH_CUDA_TRY(cudaDeviceSynchronize());
+        cudaFree(T->Bbuf);
+        T->Bbuf = nullptr;
+        T->Bcap = 0;
+    }
+    SPH_CUDA_TRY(cudaMalloc(&T->Bbuf, bytes));
+    T->Bcap = bytes;
+    return SPH_OK;
+}
+
+int tc_reserve(const Handle* h, int batch) {
+    MixedTables* T = static_cast<MixedTables*>(h->mixed);
+    if (!T || !T->streamed || batch <= 0) return SPH_OK;
+    // only the loader-only variant (autotuned in) needs the prepared-B buffer
+    bool used = false;
+    for (const auto& kv : h->tune) {
+        const int kind = (int)(kv.first >> 32), var = kv.second;
+        if (kind <= TUNE_TC_ANALYSIS && (var & 8) && !(var & 4)) used = true;
+    }
+    if (!used) return SPH_OK;
+    const int cols = (2 * batch + 63) / 64 * 64;  // covers every column tile width
+    const size_t need = std::max(tcb_bytes(h, true, T->lmax, cols), tcb_bytes(h, false, T->lmax, cols));
+    return tcb_ensure(T, need, nullptr);
+}
+
+template <int NC>
+static int tcb_launch_nc(const Handle* h, MixedTables* T, bool syn, TbArgs& a, const double2* in, long long ld_in,
+                         double2* out, cudaStream_t s) {
+    constexpr int PART = NC * tc::KC;
+    const dim3 pb((PART + 255) / 256);
+    if (syn) {
+        if (a.csyn > 65535) { set_error("tensor-core Legendre stage: too many chunks"); return SPH_ERR_ARG; }
+        k_tcb_prep_syn<NC><<<dim3(pb.x, (unsigned)a.csyn, a.nct), 256, 0, s>>>(in, ld_in, a.lmax, a.batch, a.csyn,
+                                                                              T->Bbuf);
+    } else {
+        if ((long long)a.nm * a.nkA > 65535) { set_error("tensor-core Legendre stage: too many chunks"); return SPH_ERR_ARG; }
+        k_tcb_prep_ana<NC><<<dim3(pb.x, a.nm * a.nkA, a.nct), 256, 0, s>>>(in, ld_in, a.nlat, a.nh, a.nm, a.nkA, h->w,
+                                                                          a.batch, T->Bbuf);
+    }
+    SPH_CUDA_TRY(cudaGetLastError());
+    const int grid = std::max(1, std::min(a.ntiles, g_tc_sms > 0 ? g_tc_sms : 148));
+    if (syn) k_legendre_tcb<SynB<NC>, NC><<<grid, tsb::NT, tsb::BYTES, s>>>(T->mapS, a, out);
+    else k_legendre_tcb<AnaB<NC>, NC><<<grid, tsb::NT, tsb::BYTES, s>>>(T->mapA, a, out);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+// loader-only kernel: prepare B, then run the contraction (in: spectra for
+// synthesis, Fourier data for analysis)
+static int tcb_launch(const Handle* h, const MixedTables* Tc, bool syn, int lmax, int batch, int nrt, int nm,
+                      const double2* in, long long ld_in, double2* out, long long ld_out, int var, cudaStream_t s) {
+    MixedTables* T = const_cast<MixedTables*>(Tc);
+    const int nc = tc_cols_v(batch, var);
+    TbArgs a;
+    a.soff = T->soff;
+    a.aoff = T->aoff;
+    a.tlmax = T->lmax;
+    a.lmax = lmax;
+    a.nh = h->nh;
+    a.nlat = h->nlat;
+    a.batch = batch;
+    a.nct = (2 * batch + nc - 1) / nc;
+    a.nrt = nrt;
+    a.nm = nm;
+    a.ntiles = a.nct * nrt * nm;
+    a.group = g_tc_group;
+    a.nkA = (h->nh + tc::KC - 1) / tc::KC;
+    a.csyn = tcb_syn_coff(lmax, nm);
+    a.ld_spec = syn ? ld_in : ld_out;
+    a.ldF = syn ? ld_out : ld_in;
+    a.flag = T->flag;
+    if (int rc = tcb_ensure(T, tcb_bytes(h, syn, lmax, a.nct * nc), s)) return rc;
+    a.B = T->Bbuf;
+    if (nc == 16) return tcb_launch_nc<16>(h, T, syn, a, in, ld_in, out, s);
+    if (nc == 32) return tcb_launch_nc<32>(h, T, syn, a, in, ld_in, out, s);
+    return tcb_launch_nc<64>(h, T, syn, a, in, ld_in, out, s);
+}
+
 int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F, long long ldF,
                           int batch, cudaStream_t s) {
     const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
@@ -1202,6 +1305,8 @@ int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spe
     if (batch <= 0) return SPH_OK;
     const int nrt = (h->nh + tc::M - 1) / tc::M, nm = std::min(lmax, h->L) + 1;
     const int var = tune_get(h, TUNE_TC_SYNTHESIS, batch, 0);
+    if (T->streamed && !(var & 4) && (var & 8))
+        return tcb_launch(h, T, true, lmax, batch, nrt, nm, spec, ld_spec, F, ldF, var, s);
     if (T->streamed && !(var & 4)) {
         TsArgs a = make_sargs(h, T, lmax, batch, ld_spec, ldF);
         return tcs_launch<SynS>(T->mapS, a, nrt, nm, spec, F, var, s);
@@ -1217,6 +1322,8 @@ int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, doubl
     if (batch <= 0) return SPH_OK;
     const int nrt = lmax / (2 * tc::M) + 1, nm = std::min(lmax, h->L) + 1;
     const int var = tune_get(h, TUNE_TC_ANALYSIS, batch, 0);
+    if (T->streamed && !(var & 4) && (var & 8))
+        return tcb_launch(h, T, false, lmax, batch, nrt, nm, F, ldF, spec, ld_spec, var, s);
     if (T->streamed && !(var & 4)) {
         TsArgs a = make_sargs(h, T, lmax, batch, ld_spec, ldF);
         return tcs_launch<AnaS>(T->mapA, a, nrt, nm, F, spec, var, s);

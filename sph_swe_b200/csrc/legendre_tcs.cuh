@@ -227,8 +227,9 @@ struct AnaS {
     }
 };
 
-// the MMAs of one staged chunk: A in the TMA layout, B in the generator kernel's layout
-template <int NC>
+// the MMAs of one staged chunk: A in the TMA layout, B in the generator kernel's
+// layout with its four parts BPART floats apart
+template <int NC, int BPART = tc::BTILE>
 __device__ __forceinline__ void tcs_issue_chunk(const float* As, const float* Bs, uint32_t tacc, bool acc) {
     constexpr uint32_t idesc = idesc_tf32(tc::M, NC);
     const uint64_t dA = sdesc2(smem_u32(As), 2048u, 128u), dB = sdesc(smem_u32(Bs));
@@ -238,8 +239,8 @@ __device__ __forceinline__ void tcs_issue_chunk(const float* As, const float* Bs
         for (int par = 0; par < 2; par++) {
             const uint64_t ah = dA + (uint64_t)((par * 2 * tc::ATILE * 4 + s * 4096) >> 4);
             const uint64_t al = ah + (uint64_t)((tc::ATILE * 4) >> 4);
-            const uint64_t bh = dB + (uint64_t)((par * 2 * tc::BTILE * 4 + s * NC * 32) >> 4);
-            const uint64_t bl = bh + (uint64_t)((tc::BTILE * 4) >> 4);
+            const uint64_t bh = dB + (uint64_t)((par * 2 * BPART * 4 + s * NC * 32) >> 4);
+            const uint64_t bl = bh + (uint64_t)((BPART * 4) >> 4);
             const uint32_t d = tacc + par * NC;
             mma_tf32(d, ah, bh, idesc, (s > 0 || acc) ? 1u : 0u);
             mma_tf32(d, ah, bl, idesc, 1u);

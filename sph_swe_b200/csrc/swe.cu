@@ -560,6 +560,9 @@ static int rk_run(Handle* h, const sph_swe_params* p, const double* dts_h, doubl
         if (r->graph) { cudaGraphDestroy(r->graph); r->graph = nullptr; }
         SPH_CUDA_TRY(cudaMemcpyAsync(r->dts, d.data(), sizeof(double) * nmem, cudaMemcpyHostToDevice, s));
         SPH_CUDA_TRY(cudaStreamSynchronize(s));
+        // the largest Legendre call of a step has 6 fields per member: workspace
+        // of autotuned kernel variants is reserved now (a capture cannot allocate)
+        if (int rc = tc_reserve(h, 6 * nmem)) return rc;
         // the legacy default stream cannot be captured: capture on a private stream
         cudaStream_t cap;
         SPH_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
@@ -683,6 +686,13 @@ static int ensemble_create(int ngroups, sph_handle* const* handles, const sph_sw
                       ": needs a handle, a state and 1 .. 7281 members");
             return SPH_ERR_ARG;
         }
+        for (int k = 0; k < i; k++)
+            if (handles[k] == handles[i]) {
+                // the groups run concurrently and a handle's workspace is not shared
+                set_error("sph_ensemble_create: groups " + std::to_string(k) + " and " + std::to_string(i) +
+                          " use the same handle");
+                return SPH_ERR_ARG;
+            }
     }
     Ensemble* e = new Ensemble();
     e->g.resize(ngroups);
@@ -694,6 +704,7 @@ static int ensemble_create(int ngroups, sph_handle* const* handles, const sph_sw
         g.nmem = nmem[i];
         g.r = new RKState();
         if (int rc = rk_buffers(g.h, g.r, g.nmem)) { ensemble_release(e); return rc; }
+        if (int rc = tc_reserve(g.h, 6 * g.nmem)) { ensemble_release(e); return rc; }
         std::vector<double> d(g.nmem);
         for (int k = 0; k < g.nmem; k++) d[k] = (dts && dts[i]) ? dts[i][k] : g.p.dt;
         const cudaError_t ce = cudaMemcpy(g.r->dts, d.data(), sizeof(double) * g.nmem, cudaMemcpyHostToDevice);

@@ -2,8 +2,10 @@
 //
 // For a batch size it times every candidate of
 //   - the tensor-core Legendre synthesis and analysis (mixed handles): column
-//     tile of 16, 32 or 64 real columns per CTA (8, 16, 32 fields), P operand
-//     streamed from the split tables or regenerated from checkpoints;
+//     tile of 16, 32 or 64 real columns per CTA (8, 16, 32 fields) x kernel:
+//     P loaded by the TMA unit and B staged by producer warps, both operands
+//     loaded by the TMA unit (B prepared once per call), or P regenerated from
+//     recurrence checkpoints;
 //   - the fixed-length ring FFTs (automatic grids): 2P rings per CTA with the
 //     default P or half of it (more CTAs per SM, shorter tiles);
 // with CUDA events on the caller's stream (one warm-up launch, then the mean
@@ -84,7 +86,8 @@ static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
         std::vector<int> cand;
         if (kind <= TUNE_TC_ANALYSIS) {
             if (!h->mixed) continue;
-            for (int src : {0, 4})
+            // B staged by producer warps (0), both operands loaded by the TMA unit (8), P regenerated (4)
+            for (int src : {0, 8, 4})
                 for (int c = 1; c <= 3; c++) cand.push_back(src | c);
         } else {
             if (!fixed_ring(h->nphi)) continue;
@@ -149,7 +152,7 @@ static int tune_load(Handle* h, const char* json) {
         if (!b || !v) break;
         batch = std::atoi(b + 8);
         var = std::atoi(v + 10);
-        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 7) {
+        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 15) {
             set_error("sph_tune_load: malformed entry");
             return SPH_ERR_ARG;
         }

@@ -67,9 +67,22 @@ def test_class_operators_match_oracle(classes_bin, oracle_mod, tmp_path, L):
 
 def _run_cli(args, tmp_path):
     dump = tmp_path / "state.bin"
-    r = subprocess.run([os.path.join(PKG, "sh_example"), *args, f"D{dump}"], capture_output=True, text=True)
+    r = subprocess.run([os.path.join(PKG, "sh_example"), *args, f"D{dump}"], capture_output=True, text=True,
+                       cwd=tmp_path)
     assert r.returncode == 0, r.stdout + r.stderr
     return np.fromfile(dump, np.complex128), r.stdout
+
+
+def _read_csv(path):
+    """the reference's CSV layout: three '#T' lines, a longitude row led by 0, rows of latitude + values"""
+    lines = open(path).read().splitlines()
+    assert lines[0].startswith("#TI") and lines[1] == "#TX Longitude" and lines[2] == "#TY Latitude"
+    rows = [np.array(l.split("\t"), float) for l in lines[3:]]
+    lon = rows[0][1:]
+    assert rows[0][0] == 0
+    lat = np.array([r[0] for r in rows[1:]])
+    vals = np.array([r[1:] for r in rows[1:]])
+    return lon, lat, vals
 
 
 def test_sh_example_rk4_matches_oracle(gpu, oracle_mod, tmp_path):
@@ -97,6 +110,35 @@ def test_sh_example_rexi_matches_oracle(gpu, oracle_mod, tmp_path):
                                   half=False, robert=1)
     for q, ref in enumerate((rh, ru, rv)):
         assert rel_l2(st[q * g.nlm:(q + 1) * g.nlm], ref) < 1e-10, q
+
+
+def test_sh_example_writes_reference_csv(gpu, oracle_mod, tmp_path):
+    """Output as AppSWE::write_output: files at t = 0, every O seconds and at the
+    end, in the reference's CSV layout; the final h grid equals the synthesis of
+    the dumped spectral state."""
+    st, out = _run_cli(["T31", "P0", "N1", "R120", "E1200", "O600", "Q10"], tmp_path)
+    names = sorted(p.name for p in tmp_path.glob("prog_*.csv"))
+    hours = sorted({n.split("_t")[1][:-4] for n in names})
+    assert [float(x) for x in hours] == [0.0, 600 / 3600, 1200 / 3600]
+    assert len(names) == 4 * len(hours)
+    g = oracle_mod.Grid(31)
+    lon, lat, vals = _read_csv(tmp_path / f"prog_h_t{1200 / 3600:020.8f}.csv")
+    assert vals.shape == (g.nlat, g.nphi)
+    np.testing.assert_allclose(lon, np.arange(g.nphi) * 360.0 / g.nphi, rtol=1e-7)
+    np.testing.assert_allclose(lat, np.degrees(np.asarray(g.lat))[::-1], rtol=1e-7)
+    grid = g.SH_to_spat(st[:g.nlm])  # (nphi, nlat), ring j = 0 north
+    np.testing.assert_allclose(vals, grid[:, ::-1].T, rtol=1e-7)
+
+
+def test_sh_example_galewsky(gpu, tmp_path):
+    """Q1 (BenchmarkGalewsky.hpp): balanced jet with its bump, Robert RK4 and the
+    vorticity-divergence form, a few steps, finite and mass-conserving in N2."""
+    for args in (["T63", "P0", "N1", "S1", "R60", "E600", "O1e9", "V0", "Q1"],
+                 ["T63", "P0", "N2", "R60", "E600", "O1e9", "V0", "Q1"]):
+        st, out = _run_cli(args, tmp_path)
+        assert np.all(np.isfinite(st)), args
+        lon, lat, vals = _read_csv(tmp_path / f"prog_h_t{0:020.8f}.csv")
+        assert 9000 < vals.min() < vals.max() < 11000
 
 
 def test_sh_example_rejects_bad_usage(gpu):

@@ -28,7 +28,7 @@ def test_autotune_table_and_results(gpu, oracle_mod, L, prec):
     if prec == capi.SPH_PREC_MIXED:
         assert {"legendre_synthesis_tc", "legendre_analysis_tc"} <= names
         tc = [k for k in table["kernels"] if k["name"].endswith("_tc")]
-        assert all(len(k["candidates"]) == 6 for k in tc)
+        assert all(len(k["candidates"]) == 9 for k in tc)
     for k in table["kernels"]:
         assert k["us"] > 0 and k["us"] == min(c["us"] for c in k["candidates"])
     grid1 = s.SH_to_spat(spec)
@@ -38,7 +38,7 @@ def test_autotune_table_and_results(gpu, oracle_mod, L, prec):
     assert rel_l2(grid1.cpu().numpy(), grid0.cpu().numpy()) < tol
     assert rel_l2(back1.cpu().numpy(), back0.cpu().numpy()) < tol
     # every variant forced through a loaded table gives the same transforms
-    variants = [0, 1] if prec == 0 else [1, 2, 3, 5, 6, 7]
+    variants = [0, 1] if prec == 0 else [1, 2, 3, 5, 6, 7, 9, 10, 11]
     for v in variants:
         forced = {"lmax": L, "nphi": s.nphi, "kernels": [
             {"kind": kind, "batch": nb, "variant": (v if kind < 2 else v & 1)} for kind in range(4)]}
