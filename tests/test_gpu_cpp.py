@@ -119,7 +119,7 @@ def test_sh_example_writes_reference_csv(gpu, oracle_mod, tmp_path):
     st, out = _run_cli(["T31", "P0", "N1", "R120", "E1200", "O600", "Q10"], tmp_path)
     names = sorted(p.name for p in tmp_path.glob("prog_*.csv"))
     hours = sorted({n.split("_t")[1][:-4] for n in names})
-    assert [float(x) for x in hours] == [0.0, 600 / 3600, 1200 / 3600]
+    np.testing.assert_allclose([float(x) for x in hours], [0.0, 600 / 3600, 1200 / 3600], atol=1e-8)
     assert len(names) == 4 * len(hours)
     g = oracle_mod.Grid(31)
     lon, lat, vals = _read_csv(tmp_path / f"prog_h_t{1200 / 3600:020.8f}.csv")
