@@ -45,6 +45,10 @@ L_CFG1 = 255
 N_SCALAR = 64
 N_PAIRS = 32
 METRIC = "SWE steps/s & SHT GFLOP/s at T255/T127 REXI: mixed vs FP64-GPU at relL2<=1e-6"
+# DRAM bytes (read + write) of one k_legendre_tcs<AnaS<64>> launch at T255 x 64
+# fields, from one ncu SpeedOfLight capture of that launch:
+# dram__bytes.sum.per_second x gpu__time_duration = 1.786 TB/s x 110.2 us
+TRAFFIC_ANA64 = 1.786e12 * 110.2e-6
 
 
 def cfg1_flops(L=L_CFG1, nlat=384, nphi=768):
@@ -177,10 +181,12 @@ def _time(fn, steps, st):
 
 
 def _max_over_ranks(ms, world, dev):
+    """the slowest rank's time (NCCL on the device, or gloo on the host)"""
     import torch
 
     if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        d = dev if torch.distributed.get_backend() == "nccl" else torch.device("cpu")
+        t = torch.tensor([ms], device=d, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     return ms
@@ -269,9 +275,9 @@ def run_ours(args, rank, world):
     peaks, src = measured_peaks()
     tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2.0
     achieved = per_contr * N_SCALAR / (leg["mixed"]["analysis_us"] * 1e-6) / 1e12
-    roofline = {"bound": "tensor", "kernel": "k_legendre_tc<AnaDir<64>> (split-TF32 analysis, 64 fields, T255)",
+    roofline = {"bound": "tensor", "kernel": "k_legendre_tcs<AnaS<64>> (split-TF32 analysis, 64 fields, T255)",
                 "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s", "frac": achieved / tf32_peak,
-                "traffic": args.traffic,
+                "traffic": args.traffic if args.traffic is not None else TRAFFIC_ANA64,
                 "peak_source": f"dense TF32 = half the bf16 figure of MEASURED_PEAKS.json ({src}); achieved counts "
                                "the algorithmic 2*nlm*nlat flops per field, the split form issues 3x that on the "
                                "tensor pipe",
@@ -650,7 +656,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="skip the RK4 side measurements")
-    ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the dominant kernel")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu DRAM bytes per launch of the dominant kernel (default: the committed capture)")
     ap.add_argument("--profile-case", action="store_true", help="run one small instance of each workload (for ncu)")
     args = ap.parse_args()
     if args.profile_case:

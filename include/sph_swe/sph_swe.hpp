@@ -351,6 +351,14 @@ class SPHData {
         data_spat_valid = true;
         data_spec_valid = false;
     }
+    // host spectrum (packed layout) -> this field's spectrum
+    void spec_from_host(const std::vector<cplx>& v) {
+        if (v.size() != (size_t)sphConfig->spec_num_elems) throw std::runtime_error("spec_from_host: wrong size");
+        cuda_check(cudaMemcpyAsync(data_spec, v.data(), spec_bytes(), cudaMemcpyHostToDevice, sphConfig->stream), "ul");
+        cuda_check(cudaStreamSynchronize(sphConfig->stream), "sync");
+        data_spec_valid = true;
+        data_spat_valid = false;
+    }
     // the spectral array was written directly (by a C-ABI call on data_spec)
     void mark_spectral() {
         data_spec_valid = true;

@@ -2,7 +2,7 @@
 // on top of libsphgpu.so through the C++ class surface of sph_swe.hpp.
 //
 //   sh_example T<n> P0 N<0|1> M<rexiM> H<h> I<halfpoles> R<dt> S<robert>
-//              Q<scenario> E<tend> V<visc> O<outdt> F<omega> W<M> [K<precision>] [D<file>]
+//              Q<scenario> E<tend> V<visc> O<outdt> F<omega> W<M> [K<precision>] [C<file>] [D<file>]
 //   sh_example <n> [<m> [<nlon> <nlat>]] <flags...>
 //
 // Same single-letter flags and defaults as the reference (SimVars.hpp:14-79);
@@ -10,7 +10,8 @@
 // New values and letters: N2 selects the full nonlinear equations in
 // vorticity-divergence form with Robert velocities on the grid (the reference
 // has no such form; the state is then h, vorticity, divergence), K selects the
-// precision form (0 FP64, 1 mixed) and D<file>
+// precision form (0 FP64, 1 mixed), C<file> resumes from a checkpoint written
+// by D<file>, and D<file>
 // writes the final spectral state [h | u | v] (complex128, packed layout) to a
 // file.  Programs: P0 (shallow-water run); the reference's test programs
 // P1..P5 are not part of this driver.
@@ -64,6 +65,7 @@ struct Vars {
     double h0 = 10000.0;
     int precision = SPH_PREC_FP64;
     std::string dump;
+    std::string resume;
 };
 
 int parse(int argc, char** argv, Vars& v) {
@@ -103,6 +105,7 @@ int parse(int argc, char** argv, Vars& v) {
             case 'W': v.rexi_M = std::atoi(a); break;
             case 'K': v.precision = std::atoi(a); break;
             case 'D': v.dump = a; break;
+            case 'C': v.resume = a; break;
             default: break;  // unknown letters (and a trailing T<k>) are ignored, as in the reference
         }
     }
@@ -259,7 +262,20 @@ int main(int argc, char** argv) {
                     (int)v.use_rexi, v.rexi_M, v.rexi_h, (int)v.half_poles);
 
         SPHData h(&cfg), u(&cfg), w(&cfg);
-        initial_state(v, cfg, h, u, w);
+        if (!v.resume.empty()) {
+            // checkpoint written by D<file>: the three spectral fields, packed layout
+            std::ifstream f(v.resume, std::ios::binary);
+            std::vector<cplx> buf((size_t)cfg.spec_num_elems);
+            for (SPHData* x : {&h, &u, &w}) {
+                f.read(reinterpret_cast<char*>(buf.data()), (std::streamsize)(buf.size() * sizeof(cplx)));
+                if (!f) throw std::runtime_error("checkpoint " + v.resume + " does not hold T" + std::to_string(v.n) +
+                                                 " spectra of [h | u | v]");
+                x->spec_from_host(buf);
+            }
+            std::printf(" + resumed from %s\n", v.resume.c_str());
+        } else {
+            initial_state(v, cfg, h, u, w);
+        }
         h.request_data_spectral();
         u.request_data_spectral();
         w.request_data_spectral();

@@ -141,6 +141,23 @@ def test_sh_example_galewsky(gpu, tmp_path):
         assert 9000 < vals.min() < vals.max() < 11000
 
 
+def test_sh_example_checkpoint_resume(gpu, tmp_path):
+    """C<file> resumes from a D<file> dump: 5 + 5 steps equal 10 steps bitwise."""
+    base = ["T31", "P0", "N1", "R120", "O1e9", "Q10"]
+    full, _ = _run_cli(base + ["E1200"], tmp_path)
+    half, _ = _run_cli(base + ["E600"], tmp_path)
+    ck = tmp_path / "half.bin"
+    half.tofile(ck)
+    again, out = _run_cli(base + ["E600", f"C{ck}"], tmp_path)
+    assert "resumed from" in out
+    assert np.array_equal(again, full)
+    bad = tmp_path / "short.bin"
+    half[:10].tofile(bad)
+    r = subprocess.run([os.path.join(PKG, "sh_example"), *base, "E600", f"C{bad}"], capture_output=True, text=True,
+                       cwd=tmp_path)
+    assert r.returncode != 0 and "checkpoint" in r.stderr
+
+
 def test_sh_example_rejects_bad_usage(gpu):
     exe = os.path.join(PKG, "sh_example")
     assert subprocess.run([exe], capture_output=True).returncode != 0

@@ -117,3 +117,24 @@ def test_nan_is_reported(gpu):
     with pytest.raises(capi.SphError) as e:
         s.swe_rk4(p, st, 1)
     assert e.value.code == capi.SPH_ERR_NAN
+
+
+def test_rk4_converges_at_fourth_order(gpu, oracle_mod):
+    """Nonlinear advective form at T31 to t = 1920 s with dt = 240 .. 30 s: the
+    error against dt = 7.5 s falls by ~2^4 per halving of dt."""
+    from sph_swe_b200.sph import Sph
+
+    s, g = Sph(31), oracle_mod.Grid(31)
+    h, u, v = _state(g, seed=None)
+    st0 = torch.from_numpy(np.stack([h, u, v])).cuda()
+    T = 1920.0
+
+    def run(dt):
+        st = st0.clone()
+        s.swe_rk4(_params(Sph, dt=dt), st, int(round(T / dt)))
+        return st.cpu().numpy()
+
+    ref = run(7.5)
+    errs = [np.linalg.norm(run(dt)[0] - ref[0]) for dt in (240.0, 120.0, 60.0, 30.0)]
+    rates = [np.log2(errs[i] / errs[i + 1]) for i in range(3)]
+    assert all(3.5 < r < 4.5 for r in rates), rates
