@@ -284,8 +284,9 @@ int sph_spat_op(sph_handle* h, int op, const double* x, const double* y, double*
 /* Time the kernel variants of the handle for `batch` fields per launch on
  * `stream` and keep the fastest for every later call with that batch: the
  * column tile (8, 16 or 32 fields per CTA) and P_l^m source (streamed table
- * or regenerated) of the tensor-core Legendre stages of a mixed handle, and
- * the rings per CTA of the fixed-length ring FFTs.  json (optional, capacity
+ * or regenerated) of the tensor-core Legendre stages of a mixed handle, or
+ * the FP64 Legendre kernel in their place where that is faster (variant 16),
+ * and the rings per CTA of the fixed-length ring FFTs.  json (optional, capacity
  * cap bytes) receives the table with every candidate's time.  Variants are
  * exact alternatives (no change of arithmetic beyond the last bits of
  * P_l^m).  A captured RK4 graph of the handle is re-captured on its next

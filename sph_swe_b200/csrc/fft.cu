@@ -296,7 +296,7 @@ constexpr int fixed_p() { return V == 0 ? fftx::seqs<N>() : fftx::seqs<N>() / 2;
 
 template <int N, int P>
 static size_t fixed_smem() {
-    return (size_t)P * fftx::stride<N>() * sizeof(double2);
+    return (size_t)P * N * sizeof(double2);
 }
 
 template <int N, int P>
@@ -314,18 +314,23 @@ static int fixed_attr() {
     return fixed_attr_p<N, fixed_p<N, 1>()>();
 }
 
+// every (longitude, ring pair) of every field is an aligned 16-byte chunk
+static int rows16(const Handle* h, const double* spat, long long ld_spat) {
+    return (h->nlat % 2 == 0 && ld_spat % 2 == 0 && reinterpret_cast<uintptr_t>(spat) % 16 == 0) ? 1 : 0;
+}
+
 template <int N, int P>
 static void launch_ra(const Handle* h, const double* spat, long long ld_spat, double2* F, long long ldF, int mF, int batch,
                       cudaStream_t s) {
     k_ring_analysis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::NT, fixed_smem<N, P>(), s>>>(
-        spat, ld_spat, F, ldF, mF, h->L, h->nlat, h->fft.tw);
+        spat, ld_spat, F, ldF, mF, h->L, h->nlat, h->fft.tw, rows16(h, spat, ld_spat));
 }
 
 template <int N, int P>
 static void launch_rs(const Handle* h, const double2* F, long long ldF, int mF, double* spat, long long ld_spat, int batch,
                       const RingMap& map, cudaStream_t s) {
     k_ring_synthesis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::NT, fixed_smem<N, P>(), s>>>(
-        F, ldF, mF, h->L, spat, ld_spat, h->nlat, h->fft.tw, map);
+        F, ldF, mF, h->L, spat, ld_spat, h->nlat, h->fft.tw, map, rows16(h, spat, ld_spat));
 }
 
 int fft_kernels_init() {

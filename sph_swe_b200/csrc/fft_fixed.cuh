@@ -7,12 +7,16 @@
 // of the theta-contiguous grid; P is a template parameter so that the
 // autotuner can trade tile width for CTAs per SM), i.e. 2P consecutive
 // latitude rings of one field packed in pairs (ring 2q real part, ring 2q+1
-// imaginary part).  Sequence rows are
-// padded by one element so that the tile loads hit distinct banks.  The Stockham passes (radix 3 first, then
-// 8, 4, 2; all radices and strides compile-time) run in place in a single
-// shared-memory buffer: each pass reads its butterfly inputs into registers,
-// synchronises, and writes the outputs, so only P * (N + 1) * 16 bytes of
-// shared memory are needed.
+// imaginary part).  Shared memory holds the tile element-major with the
+// sequences innermost, buf[i * P + q]: element i of all P sequences is the
+// 16 P bytes that longitude i of the 2P rings occupies in the grid, so the
+// grid tile is copied in (analysis) and out (synthesis) as 16-byte chunks
+// without rearrangement, by asynchronous copies (cp.async) on the way in.
+// The Stockham passes (radix 3 first, then 8, 4, 2; all radices and strides
+// compile-time) run in place in that one buffer, the sequence index fastest
+// across threads so that every quarter-warp touches one contiguous row: each
+// pass reads its butterfly inputs into registers, synchronises, and writes
+// the outputs, so only P * N * 16 bytes of shared memory are needed.
 #pragma once
 
 // needs FFTPlan / RingMap of fft.cu (included from there)
@@ -24,8 +28,16 @@ constexpr int NT = 256;     // threads per CTA
 // default complex sequences per CTA (2 P real rings) and the padded row stride
 template <int N>
 constexpr int seqs() { return N <= 768 ? 8 : (N == 1536 ? 4 : 2); }
-template <int N>
-constexpr int stride() { return N + 1; }
+
+// 16-byte asynchronous global -> shared copy; bytes = 0 writes zeros
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, int bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -122,12 +134,12 @@ constexpr int ls_at(int N, int q) {
 // One Stockham pass on P sequences in place: butterflies t = (f, j), j < N/R,
 // inputs s[j + r N/R] times w^(r k N/(Ls R)), k = j mod Ls, outputs to
 // d[(j - k) R + k + r Ls]; w = exp(SIGN 2 pi i / N) from the table tw[t] = exp(-2 pi i t / N).
+// Element e of sequence f is buf[e * P + f]; f = t mod P.
 template <int N, int P, int Q, int SIGN>
 __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ tw) {
     constexpr int R = radix_at(N, Q);
     constexpr int Ls = ls_at(N, Q);
     constexpr int NR = N / R;
-    constexpr int SN = stride<N>();
     constexpr int TOT = P * NR;
     constexpr int IT = (TOT + NT - 1) / NT;
     constexpr int TS = N / (Ls * R);
@@ -136,14 +148,14 @@ __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ t
     for (int it = 0; it < IT; it++) {
         const int t = threadIdx.x + NT * it;
         if (TOT % NT == 0 || t < TOT) {
-            const int f = t / NR, j = t - f * NR, k = j % Ls;
-            const double2* s = buf + f * SN;
-            v[it][0] = s[j];
+            const int f = t % P, j = t / P, k = j % Ls;
+            const double2* s = buf + f;
+            v[it][0] = s[j * P];
 #pragma unroll
             for (int r = 1; r < R; r++) {
                 double2 w = __ldg(&tw[(r * k * TS) % N]);
                 if (SIGN > 0) w.y = -w.y;
-                v[it][r] = cmul(s[j + r * NR], w);
+                v[it][r] = cmul(s[(j + r * NR) * P], w);
             }
             dft<R, SIGN>(v[it]);
         }
@@ -153,10 +165,10 @@ __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ t
     for (int it = 0; it < IT; it++) {
         const int t = threadIdx.x + NT * it;
         if (TOT % NT == 0 || t < TOT) {
-            const int f = t / NR, j = t - f * NR, k = j % Ls;
-            double2* d = buf + f * SN + (j - k) * R + k;
+            const int f = t % P, j = t / P, k = j % Ls;
+            double2* d = buf + ((j - k) * R + k) * P + f;
 #pragma unroll
-            for (int r = 0; r < R; r++) d[r * Ls] = v[it][r];
+            for (int r = 0; r < R; r++) d[r * Ls * P] = v[it][r];
         }
     }
     __syncthreads();
@@ -176,32 +188,43 @@ __device__ __forceinline__ void passes(double2* buf, const double2* __restrict__
 namespace sphgpu {
 
 // grid tile (2P rings, pairs packed) -> F[b][m][j], m = 0..mF-1 (m > L zero),
-// scaled by 2 pi / N (quadrature weight in longitude)
+// scaled by 2 pi / N (quadrature weight in longitude).  vec != 0: nlat even and
+// the field rows 16-byte aligned, so each (longitude, ring pair) is one
+// aligned 16-byte chunk copied by cp.async.
 template <int N, int P>
 __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const double* __restrict__ spat, long long ld_spat,
                                                                     double2* __restrict__ F, long long ldF, int mF, int L,
-                                                                    int nlat, const double2* __restrict__ tw) {
-    constexpr int SN = fftx::stride<N>(), JT = 2 * P;
+                                                                    int nlat, const double2* __restrict__ tw, int vec) {
+    constexpr int JT = 2 * P;
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
     const double* src = spat + (long long)blockIdx.y * ld_spat;
-    // tile load in batches of U independent loads per thread
-    constexpr int PER = N * JT / fftx::NT;
-    constexpr int U = PER <= 12 ? PER : 8;
-    static_assert((N * JT) % fftx::NT == 0 && PER % U == 0, "tile divides into batches");
-    for (int base = 0; base < N * JT; base += U * fftx::NT) {
-        double v[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int idx = base + threadIdx.x + u * fftx::NT;
-            const int i = idx / JT, j = j0 + idx % JT;
-            v[u] = (j < nlat) ? __ldg(&src[(long long)i * nlat + j]) : 0.0;
+    if (vec) {
+        for (int idx = threadIdx.x; idx < N * P; idx += fftx::NT) {
+            const int i = idx / P, j = j0 + 2 * (idx % P);
+            const bool in = j < nlat;
+            fftx::cp_async16(&fbuf[idx], src + (long long)i * nlat + (in ? j : 0), in ? 16 : 0);
         }
+        fftx::cp_async_wait_all();
+    } else {
+        // tile load in batches of U independent loads per thread
+        constexpr int PER = N * JT / fftx::NT;
+        constexpr int U = PER <= 12 ? PER : 8;
+        static_assert((N * JT) % fftx::NT == 0 && PER % U == 0, "tile divides into batches");
+        for (int base = 0; base < N * JT; base += U * fftx::NT) {
+            double v[U];
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int idx = base + threadIdx.x + u * fftx::NT;
-            const int i = idx / JT, jj = idx % JT;
-            reinterpret_cast<double*>(&fbuf[(jj >> 1) * SN + i])[jj & 1] = v[u];
+            for (int u = 0; u < U; u++) {
+                const int idx = base + threadIdx.x + u * fftx::NT;
+                const int i = idx / JT, j = j0 + idx % JT;
+                v[u] = (j < nlat) ? __ldg(&src[(long long)i * nlat + j]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int idx = base + threadIdx.x + u * fftx::NT;
+                const int i = idx / JT, jj = idx % JT;
+                reinterpret_cast<double*>(&fbuf[i * P + (jj >> 1)])[jj & 1] = v[u];
+            }
         }
     }
     __syncthreads();
@@ -214,8 +237,8 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const doub
         if (j >= nlat) continue;
         double2 X = make_double2(0, 0), Y = make_double2(0, 0);
         if (m <= L) {
-            const double2 a = fbuf[q * SN + m];
-            const double2 c = fbuf[q * SN + (N - m) % N];
+            const double2 a = fbuf[m * P + q];
+            const double2 c = fbuf[((N - m) % N) * P + q];
             X = make_double2(0.5 * (a.x + c.x) * scale, 0.5 * (a.y - c.y) * scale);
             Y = make_double2(0.5 * (a.y + c.y) * scale, -0.5 * (a.x - c.x) * scale);
         }
@@ -224,13 +247,14 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const doub
     }
 }
 
-// F[fs][m][j] (optionally times i*m) -> grid k; m = 0 contributes its real part
+// F[fs][m][j] (optionally times i*m) -> grid k; m = 0 contributes its real part.
+// vec != 0: nlat even and the field rows 16-byte aligned (16-byte stores).
 template <int N, int P>
 __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const double2* __restrict__ F, long long ldF, int mF,
                                                                      int L, double* __restrict__ spat, long long ld_spat,
                                                                      int nlat, const double2* __restrict__ tw,
-                                                                     RingMap map) {
-    constexpr int SN = fftx::stride<N>(), JT = 2 * P;
+                                                                     RingMap map, int vec) {
+    constexpr int JT = 2 * P;
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
     const int k = blockIdx.y;
@@ -241,36 +265,56 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const dou
         mod = map.mod[r];
     }
     const double2* in = F + (long long)fs * ldF;
-    for (int idx = threadIdx.x; idx < P * SN; idx += fftx::NT) fbuf[idx] = make_double2(0, 0);
-    __syncthreads();
     const int mm = min(min(mF - 1, L), (N - 1) / 2);
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < (mm + 1) * P; idx += fftx::NT) {
-        const int m = idx / P, q = idx % P;
-        const int j = j0 + 2 * q;
-        double2 X = make_double2(0, 0), Y = make_double2(0, 0);
-        if (j < nlat) X = __ldg(&in[(long long)m * nlat + j]);
-        if (j + 1 < nlat) Y = __ldg(&in[(long long)m * nlat + j + 1]);
-        if (mod) {  // d/dlambda: times i*m
-            X = make_double2(-m * X.y, m * X.x);
-            Y = make_double2(-m * Y.y, m * Y.x);
+    // rows mm+1 .. N-mm-1 are zero; rows 0..mm and N-mm..N-1 are written below
+    for (int idx = (mm + 1) * P + threadIdx.x; idx < (N - mm) * P; idx += fftx::NT) fbuf[idx] = make_double2(0, 0);
+    constexpr int U = 8;
+    const int tot = (mm + 1) * P;
+    for (int base = threadIdx.x; base < tot; base += U * fftx::NT) {
+        double2 X[U], Y[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int idx = base + u * fftx::NT;
+            const int m = idx / P, j = j0 + 2 * (idx % P);
+            X[u] = Y[u] = make_double2(0, 0);
+            if (idx < tot && j < nlat) X[u] = __ldg(&in[(long long)m * nlat + j]);
+            if (idx < tot && j + 1 < nlat) Y[u] = __ldg(&in[(long long)m * nlat + j + 1]);
         }
-        if (m == 0) {
-            fbuf[q * SN] = make_double2(X.x, Y.x);
-        } else {
-            fbuf[q * SN + m] = make_double2(X.x - Y.y, X.y + Y.x);       // X + iY
-            fbuf[q * SN + N - m] = make_double2(X.x + Y.y, -X.y + Y.x);  // conj(X) + i conj(Y)
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int idx = base + u * fftx::NT;
+            if (idx >= tot) break;
+            const int m = idx / P, q = idx % P;
+            double2 x = X[u], y = Y[u];
+            if (mod) {  // d/dlambda: times i*m
+                x = make_double2(-m * x.y, m * x.x);
+                y = make_double2(-m * y.y, m * y.x);
+            }
+            if (m == 0) {
+                fbuf[q] = make_double2(x.x, y.x);
+            } else {
+                fbuf[m * P + q] = make_double2(x.x - y.y, x.y + y.x);        // X + iY
+                fbuf[(N - m) * P + q] = make_double2(x.x + y.y, -x.y + y.x);  // conj(X) + i conj(Y)
+            }
         }
     }
     __syncthreads();
     fftx::passes<N, P, 0, +1>(fbuf, tw);
     double* out = spat + (long long)k * ld_spat;
+    if (vec) {
 #pragma unroll 8
-    for (int idx = threadIdx.x; idx < N * JT; idx += fftx::NT) {
-        const int i = idx / JT, jj = idx % JT;
-        const int j = j0 + jj;
-        const double2 z = fbuf[(jj >> 1) * SN + i];
-        if (j < nlat) out[(long long)i * nlat + j] = (jj & 1) ? z.y : z.x;
+        for (int idx = threadIdx.x; idx < N * P; idx += fftx::NT) {
+            const int i = idx / P, j = j0 + 2 * (idx % P);
+            if (j < nlat) *reinterpret_cast<double2*>(&out[(long long)i * nlat + j]) = fbuf[idx];
+        }
+    } else {
+#pragma unroll 8
+        for (int idx = threadIdx.x; idx < N * JT; idx += fftx::NT) {
+            const int i = idx / JT, jj = idx % JT;
+            const int j = j0 + jj;
+            const double2 z = fbuf[i * P + (jj >> 1)];
+            if (j < nlat) out[(long long)i * nlat + j] = (jj & 1) ? z.y : z.x;
+        }
     }
 }
 

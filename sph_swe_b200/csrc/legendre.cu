@@ -166,6 +166,241 @@ __global__ void __launch_bounds__(NT) k_legendre_analysis(const double* __restri
     }
 }
 
+// Wide-tile variants for larger batches: CTA tile 64 rows x 64 real columns
+// (32 fields), 128 threads with 8 rows x 4 columns each (64 / 32 FP64
+// accumulators), contraction chunks of 16 double-buffered in shared memory
+// with the next chunk's global loads issued before the current chunk's FMAs.
+// Per k step a thread loads 4 + 2 (+2) double2 from shared memory for 32 FMAs.
+namespace {
+constexpr int WR = 64;        // rows per CTA (latitudes, or degrees in the analysis)
+constexpr int WC = 64;        // real columns per CTA
+constexpr int WK = 16;        // contraction chunk
+constexpr int WNT = 128;      // threads
+constexpr int WP = WR + 2;    // padded shared-memory row (16-byte aligned, spreads banks)
+constexpr int WSMEM_ANA = 3 * 2 * WK * WP * (int)sizeof(double);  // analysis: P, sum, difference tiles
+}  // namespace
+
+__global__ void __launch_bounds__(WNT) k_legendre_synthesis_w(const double* __restrict__ plm,
+                                                                   const long long* __restrict__ poff, int nh, int nlat,
+                                                                   const double2* __restrict__ spec, SpecMap sm,
+                                                                   double2* __restrict__ F, long long ldF, int batch) {
+    __shared__ __align__(16) double As[2][WK][WP];
+    __shared__ __align__(16) double Bs[2][WK][WP];
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int j0 = blockIdx.x * WR;
+    const int f0 = blockIdx.y * (WC / 2);
+    const int tid = threadIdx.x;
+    const int tx = tid & 15;  // columns 4 tx .. 4 tx + 3 (fields f0 + 2 tx, f0 + 2 tx + 1)
+    const int ty = tid >> 4;  // rows 8 ty .. 8 ty + 7
+    const double* P = plm + poff[am];
+
+    double ra[8];
+    double2 rb[4];
+    auto fetch = [&](int l0) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int idx = tid + WNT * i, kk = idx / WR, jj = idx % WR;
+            const int l = l0 + kk, j = j0 + jj;
+            ra[i] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
+            const int l = l0 + kk, f = f0 + ff;
+            rb[i] = (l <= lmax && f < batch) ? spec[(long long)f * sm.ld + spec_index(sm, l, m)] : make_double2(0, 0);
+        }
+    };
+    auto stash = [&](int b) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int idx = tid + WNT * i;
+            As[b][idx / WR][idx % WR] = ra[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
+            *reinterpret_cast<double2*>(&Bs[b][kk][2 * ff]) = rb[i];
+        }
+    };
+
+    double E[8][4], O[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) E[r][c] = O[r][c] = 0.0;
+
+    fetch(am);
+    stash(0);
+    __syncthreads();
+    int cur = 0;
+    for (int l0 = am; l0 <= lmax; l0 += WK) {
+        const bool more = l0 + WK <= lmax;
+        if (more) fetch(l0 + WK);
+#pragma unroll
+        for (int kk = 0; kk < WK; kk++) {
+            double a[8], b[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const double2 v = *reinterpret_cast<const double2*>(&As[cur][kk][8 * ty + 2 * q]);
+                a[2 * q] = v.x;
+                a[2 * q + 1] = v.y;
+            }
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const double2 v = *reinterpret_cast<const double2*>(&Bs[cur][kk][4 * tx + 2 * q]);
+                b[2 * q] = v.x;
+                b[2 * q + 1] = v.y;
+            }
+            // degree l0 + kk has the parity of kk (l0 - am is a multiple of 16)
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    if (kk & 1) O[r][c] = fma(a[r], b[c], O[r][c]);
+                    else E[r][c] = fma(a[r], b[c], E[r][c]);
+                }
+        }
+        if (more) stash(cur ^ 1);
+        __syncthreads();
+        cur ^= 1;
+    }
+    double2* outm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const int f = f0 + 2 * tx + c;
+        if (f >= batch) continue;
+        double2* out = outm + (long long)f * ldF;
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int j = j0 + 8 * ty + r;
+            if (j >= nh) continue;
+            out[j] = make_double2(E[r][2 * c] + O[r][2 * c], E[r][2 * c + 1] + O[r][2 * c + 1]);
+            out[nlat - 1 - j] = make_double2(E[r][2 * c] - O[r][2 * c], E[r][2 * c + 1] - O[r][2 * c + 1]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(WNT) k_legendre_analysis_w(const double* __restrict__ plm,
+                                                                  const long long* __restrict__ poff, int nh, int nlat,
+                                                                  const double* __restrict__ w,
+                                                                  const double2* __restrict__ F, long long ldF,
+                                                                  double2* __restrict__ spec, SpecMap sm, int batch) {
+    extern __shared__ __align__(16) double wsm[];
+    double(*Ps)[WK][WP] = reinterpret_cast<double(*)[WK][WP]>(wsm);
+    double(*Ss)[WK][WP] = Ps + 2;
+    double(*Ds)[WK][WP] = Ps + 4;
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int lbase = am + blockIdx.x * WR;
+    if (lbase > lmax) return;
+    const int f0 = blockIdx.y * (WC / 2);
+    const int tid = threadIdx.x;
+    const int tx = tid & 15;
+    const int ty = tid >> 4;
+    // the 64 degrees of the tile by parity (lbase - am is a multiple of 64):
+    // degree lbase + 2 e + par is shared-memory row par * 32 + e; a thread
+    // takes 8 degrees of one parity, e = e0 .. e0 + 7, and so needs only the
+    // sum (even) or the difference (odd) columns
+    const int par = ty >> 2, e0 = 8 * (ty & 3);
+    const double* P = plm + poff[am];
+    const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+
+    double rp[8];
+    double2 rs[4], rd[4];
+    auto fetch = [&](int j0) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int idx = tid + WNT * i, kk = idx & 15, ll = idx >> 4;
+            const int l = lbase + ll, j = j0 + kk;
+            rp[i] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
+            const int j = j0 + kk, f = f0 + ff;
+            double2 sv = make_double2(0, 0), dv = make_double2(0, 0);
+            if (j < nh && f < batch) {
+                const double2* Ff = Fm + (long long)f * ldF;
+                const double2 n = Ff[j], so = Ff[nlat - 1 - j];
+                const double wj = w[j];
+                sv = make_double2(wj * (n.x + so.x), wj * (n.y + so.y));
+                dv = make_double2(wj * (n.x - so.x), wj * (n.y - so.y));
+            }
+            rs[i] = sv;
+            rd[i] = dv;
+        }
+    };
+    auto stash = [&](int b) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int idx = tid + WNT * i;
+            const int ll = idx >> 4;
+            Ps[b][idx & 15][(ll & 1) * 32 + (ll >> 1)] = rp[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
+            *reinterpret_cast<double2*>(&Ss[b][kk][2 * ff]) = rs[i];
+            *reinterpret_cast<double2*>(&Ds[b][kk][2 * ff]) = rd[i];
+        }
+    };
+
+    double acc[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
+
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    int cur = 0;
+    for (int j0 = 0; j0 < nh; j0 += WK) {
+        const bool more = j0 + WK < nh;
+        if (more) fetch(j0 + WK);
+        const double(*G)[WK][WP] = par ? Ds : Ss;
+#pragma unroll
+        for (int kk = 0; kk < WK; kk++) {
+            double p[8], g[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const double2 v = *reinterpret_cast<const double2*>(&Ps[cur][kk][par * 32 + e0 + 2 * q]);
+                p[2 * q] = v.x;
+                p[2 * q + 1] = v.y;
+            }
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const double2 u = *reinterpret_cast<const double2*>(&G[cur][kk][4 * tx + 2 * q]);
+                g[2 * q] = u.x;
+                g[2 * q + 1] = u.y;
+            }
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[r][c] = fma(p[r], g[c], acc[r][c]);
+        }
+        if (more) stash(cur ^ 1);
+        __syncthreads();
+        cur ^= 1;
+    }
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const int f = f0 + 2 * tx + c;
+        if (f >= batch) continue;
+        double2* out = spec + (long long)f * sm.ld;
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int l = lbase + 2 * (e0 + r) + par;
+            if (l <= lmax) out[spec_index(sm, l, m)] = make_double2(acc[r][2 * c], acc[r][2 * c + 1]);
+        }
+    }
+}
+
 // zero the m = L+1 column of a degree-(L+1) packed spectrum (no wavenumber L+1 exists)
 __global__ void k_zero_top(double2* spec, long long ld, int lmax, int batch) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -176,6 +411,12 @@ static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double
                         cudaStream_t s) {
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
+    if (batch > 16) {
+        dim3 grid((h->nh + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
+        k_legendre_synthesis_w<<<grid, WNT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
+        SPH_CUDA_TRY(cudaGetLastError());
+        return SPH_OK;
+    }
     dim3 grid((h->nh + TJ - 1) / TJ, (batch + TC / 2 - 1) / (TC / 2), nm);
     k_legendre_synthesis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
     SPH_CUDA_TRY(cudaGetLastError());
@@ -186,8 +427,20 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
                        cudaStream_t s) {
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
-    dim3 grid((sm.lmax + 1 + TLT - 1) / TLT, (batch + TC / 2 - 1) / (TC / 2), nm);
-    k_legendre_analysis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, h->w, F, ldF, spec, sm, batch);
+    if (batch > 16) {
+        static bool attr = false;
+        if (!attr) {
+            SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_w, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              WSMEM_ANA));
+            attr = true;
+        }
+        dim3 grid((sm.lmax + 1 + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
+        k_legendre_analysis_w<<<grid, WNT, WSMEM_ANA, s>>>(h->plm, h->poff, h->nh, h->nlat, h->w, F, ldF, spec, sm,
+                                                        batch);
+    } else {
+        dim3 grid((sm.lmax + 1 + TLT - 1) / TLT, (batch + TC / 2 - 1) / (TC / 2), nm);
+        k_legendre_analysis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, h->w, F, ldF, spec, sm, batch);
+    }
     SPH_CUDA_TRY(cudaGetLastError());
     if (!sm.cplx && sm.lmax > h->L) {
         k_zero_top<<<(batch + 127) / 128, 128, 0, s>>>(spec, sm.ld, sm.lmax, batch);
@@ -198,14 +451,16 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
 
 int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
                             long long ldF, int batch, cudaStream_t s) {
-    if (h->flags & SPH_PREC_MIXED) return legendre_synthesis_tc(h, spec, ld_spec, lmax, F, ldF, batch, s);
+    // mixed handles: the tensor-core kernels unless the autotuner found the FP64 kernel faster (variant bit 16)
+    if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_SYNTHESIS, batch, 0) & 16))
+        return legendre_synthesis_tc(h, spec, ld_spec, lmax, F, ldF, batch, s);
     SpecMap sm{0, lmax, h->L, ld_spec};
     return launch_synth(h, spec, sm, F, ldF, batch, s);
 }
 
 int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
                            int lmax, int batch, cudaStream_t s) {
-    if (h->flags & SPH_PREC_MIXED) {
+    if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_ANALYSIS, batch, 0) & 16)) {
         if (int rc = legendre_analysis_tc(h, F, ldF, spec, ld_spec, lmax, batch, s)) return rc;
         if (lmax > h->L) {
             k_zero_top<<<(batch + 127) / 128, 128, 0, s>>>(spec, ld_spec, lmax, batch);

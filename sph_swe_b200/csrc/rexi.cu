@@ -34,6 +34,7 @@
 
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 
 struct sph_rexi;
@@ -55,13 +56,36 @@ struct RexiPlan {
     double2* Xr = nullptr;      // nlm
     double2* F = nullptr;       // (L+1)*nlat
     int* flag = nullptr;        // bit0 non-finite h, bit1 singular pivot
+    // factors of the banded systems, computed once at plan creation (FP64 form,
+    // Coriolis case): planes of [ngroups][ncplx][32 lanes]
+    double2* fphi = nullptr;    // 7 planes
+    double2* fvel = nullptr;    // 4 planes
+    signed char* pphi = nullptr;
+    signed char* pvel = nullptr;
+    long long plane = 0;
+    bool singular = false;      // a zero pivot met while factoring
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double* state = nullptr;
     cudaStream_t stream = nullptr;
 };
 
-template <int MAXN, bool MIXED>
+// factor every (pole, m-block, parity) system once into the stored planes
+__global__ void __launch_bounds__(64) k_rexi_factor(RexiDev d) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int nblk = 2 * d.L + 1;
+    if (warp >= nblk * d.ngroups) return;
+    const int g = warp % d.ngroups, kk = warp / d.ngroups;
+    const int m = (kk & 1) ? -((kk + 1) >> 1) : (kk >> 1);
+    const int pole = g * 32 + lane;
+    const bool valid = pole < d.npoles;
+    const double2 a = d.alpha[valid ? pole : 0];
+    const long long gl = (long long)g * d.ncplx * 32 + lane;
+    if (!rexi_factor_lane(d, m, a, gl) && valid) atomicOr(d.flag, 2);
+}
+
+template <int MAXN, bool MIXED, bool STORED>
 __global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -78,7 +102,8 @@ __global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
     const double2 a = d.alpha[valid ? pole : 0];
     const double2 bt = valid ? d.beta[pole] : make_double2(0, 0);
     double2 phi[MAXN], ra[MAXN], rb[MAXN];
-    const bool ok = rexi_lane<MAXN, MIXED>(d, m, a, phi, ra, rb);
+    const long long gl = (long long)g * nc * 32 + lane;
+    const bool ok = rexi_lane<MAXN, MIXED, STORED>(d, m, a, phi, ra, rb, gl);
     if (!ok && valid) atomicOr(d.flag, 2);
     // beta scaling and reduction over the 32 poles of this warp
     double2* outp = d.part + (size_t)g * 3 * nc;
@@ -199,6 +224,37 @@ __global__ void k_rx_finish(const double2* __restrict__ part, int ngroups, int n
     }
 }
 
+static RexiDev rexi_dev(const RexiPlan* R) {
+    const Handle* h = R->h;
+    RexiDev d{};
+    d.L = h->L;
+    d.npoles = R->npoles;
+    d.ngroups = R->ngroups;
+    d.ncplx = h->ncplx;
+    d.coriolis = (R->p.coriolis && R->p.omega != 0.0) ? 1 : 0;
+    // mixed form: complex FP32 factorisation and solves, two FP64 refinement steps
+    d.refine = R->p.precision == SPH_PREC_MIXED ? 2 : 0;
+    d.r = R->p.radius;
+    d.ir = 1.0 / R->p.radius;
+    d.T = 2.0 * R->p.omega;
+    d.P = R->p.h0 * R->p.gravity;
+    d.alpha = R->alpha;
+    d.beta = R->beta;
+    d.Cphi = R->Cphi;
+    d.Cvel = R->Cvel;
+    d.coef = R->coef;
+    d.V = R->V;
+    d.part = R->part;
+    d.flag = R->flag;
+    d.fphi = R->fphi;
+    d.pphi = R->pphi;
+    d.fvel = R->fvel;
+    d.pvel = R->pvel;
+    d.plane = R->plane;
+    d.lanes = 32;
+    return d;
+}
+
 static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     Handle* h = R->h;
     const int L = h->L, nlm = h->nlm, nc = h->ncplx, nlat = h->nlat, mF = L + 1;
@@ -238,36 +294,21 @@ static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     k_rx_block_op<<<gc, 64, 0, s>>>(3, Vs(12), Vs(17), Vs(9), L, ir);
     SPH_CUDA_TRY(cudaGetLastError());
     // all poles x all m x both parities
-    RexiDev d;
-    d.L = L;
-    d.npoles = R->npoles;
-    d.ngroups = R->ngroups;
-    d.ncplx = nc;
-    d.coriolis = (R->p.coriolis && R->p.omega != 0.0) ? 1 : 0;
-    // mixed form: complex FP32 factorisation and solves, two FP64 refinement steps
-    d.refine = R->p.precision == SPH_PREC_MIXED ? 2 : 0;
-    d.r = R->p.radius;
-    d.ir = ir;
-    d.T = 2.0 * R->p.omega;
-    d.P = R->p.h0 * R->p.gravity;
-    d.alpha = R->alpha;
-    d.beta = R->beta;
-    d.Cphi = R->Cphi;
-    d.Cvel = R->Cvel;
-    d.coef = R->coef;
-    d.V = R->V;
-    d.part = R->part;
-    d.flag = R->flag;
+    const RexiDev d = rexi_dev(R);
     const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
     const unsigned nb = (unsigned)((nthreads + 63) / 64);
-    if (d.refine > 0) {
-        if (L + 1 <= 64) k_rexi_solve<64, true><<<nb, 64, 0, s>>>(d);
-        else if (L + 1 <= 128) k_rexi_solve<128, true><<<nb, 64, 0, s>>>(d);
-        else k_rexi_solve<256, true><<<nb, 64, 0, s>>>(d);
+    if (d.fphi) {  // factors stored at plan creation: substitutions only
+        if (L + 1 <= 64) k_rexi_solve<64, false, true><<<nb, 64, 0, s>>>(d);
+        else if (L + 1 <= 128) k_rexi_solve<128, false, true><<<nb, 64, 0, s>>>(d);
+        else k_rexi_solve<256, false, true><<<nb, 64, 0, s>>>(d);
+    } else if (d.refine > 0) {
+        if (L + 1 <= 64) k_rexi_solve<64, true, false><<<nb, 64, 0, s>>>(d);
+        else if (L + 1 <= 128) k_rexi_solve<128, true, false><<<nb, 64, 0, s>>>(d);
+        else k_rexi_solve<256, true, false><<<nb, 64, 0, s>>>(d);
     } else {
-        if (L + 1 <= 64) k_rexi_solve<64, false><<<nb, 64, 0, s>>>(d);
-        else if (L + 1 <= 128) k_rexi_solve<128, false><<<nb, 64, 0, s>>>(d);
-        else k_rexi_solve<256, false><<<nb, 64, 0, s>>>(d);
+        if (L + 1 <= 64) k_rexi_solve<64, false, false><<<nb, 64, 0, s>>>(d);
+        else if (L + 1 <= 128) k_rexi_solve<128, false, false><<<nb, 64, 0, s>>>(d);
+        else k_rexi_solve<256, false, false><<<nb, 64, 0, s>>>(d);
     }
     SPH_CUDA_TRY(cudaGetLastError());
     const double visc_fac = R->p.viscosity * R->p.tau / (R->p.radius * R->p.radius);
@@ -280,7 +321,8 @@ static void rexi_free(RexiPlan* R) {
     if (!R) return;
     if (R->exec) cudaGraphExecDestroy(R->exec);
     if (R->graph) cudaGraphDestroy(R->graph);
-    void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V, R->part, R->X, R->Xr, R->F, R->flag};
+    void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V,    R->part, R->X,
+                    R->Xr,    R->F,    R->flag, R->fphi, R->fvel, R->pphi, R->pvel};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete R;
@@ -389,6 +431,30 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
     RX_TRY(cudaMemcpy(R->coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice));
     RX_TRY(cudaMemset(R->V, 0, sizeof(double2) * 18 * (size_t)nc));
     RX_TRY(cudaMemset(R->flag, 0, sizeof(int)));
+    // FP64 form with Coriolis: factor every banded system once (the matrices
+    // depend on the pole and m only), if the factors fit in half the free
+    // device memory; every step then runs the substitutions alone
+    const char* store_env = std::getenv("SPH_REXI_STORE");  // "0": factor on the fly every step
+    if (cor && p->precision == SPH_PREC_FP64 && !(store_env && store_env[0] == '0')) {
+        const long long plane = (long long)R->ngroups * nc * 32;
+        const size_t bytes = (size_t)plane * (11 * sizeof(double2) + 2);
+        size_t free_b = 0, total_b = 0;
+        RX_TRY(cudaMemGetInfo(&free_b, &total_b));
+        if (bytes <= free_b / 2) {
+            RX_TRY(cudaMalloc(&R->fphi, sizeof(double2) * 7 * (size_t)plane));
+            RX_TRY(cudaMalloc(&R->fvel, sizeof(double2) * 4 * (size_t)plane));
+            RX_TRY(cudaMalloc(&R->pphi, (size_t)plane));
+            RX_TRY(cudaMalloc(&R->pvel, (size_t)plane));
+            R->plane = plane;
+            const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
+            k_rexi_factor<<<(unsigned)((nthreads + 63) / 64), 64>>>(rexi_dev(R));
+            RX_TRY(cudaGetLastError());
+            int flag = 0;
+            RX_TRY(cudaMemcpy(&flag, R->flag, sizeof(int), cudaMemcpyDeviceToHost));
+            R->singular = (flag & 2) != 0;
+            RX_TRY(cudaMemset(R->flag, 0, sizeof(int)));
+        }
+    }
 #undef RX_TRY
     *out = R;
     return SPH_OK;
@@ -429,6 +495,7 @@ int sph_rexi_step(sph_rexi* R, double* state, int nsteps, void* stream) {
     int flag = 0;
     SPH_CUDA_TRY(cudaMemcpyAsync(&flag, R->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     SPH_CUDA_TRY(cudaStreamSynchronize(s));
+    if (R->singular && nsteps > 0) flag |= 2;
     if (flag & 2) {
         set_error("sph_rexi_step: zero pivot in a banded solve (zgbsv INFO > 0)");
         return SPH_ERR_SINGULAR;

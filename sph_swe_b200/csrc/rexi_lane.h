@@ -30,6 +30,23 @@ struct RexiDev {
     const double2* V;
     double2* part;
     int* flag;
+    // stored factors of the banded systems (nullptr: factor on the fly), see BandRef
+    double2* fphi;       // [7 planes][plane]: 1/U_kk, U_k,k+1..k+4, multipliers 1..2
+    signed char* pphi;   // [plane] pivot offsets
+    double2* fvel;       // [4 planes][plane]: 1/U_kk, U_k,k+1..k+2, multiplier
+    signed char* pvel;   // [plane]
+    long long plane;     // ngroups * ncplx * lanes
+    int lanes;           // poles per group (32 on the device, 1 on the host)
+};
+
+// Row k of one stored banded system: plane q at f[q * plane + i0 + k * lanes].
+// Rows of parity par of the m-block at block row `base` (N rows), pole group
+// g, lane `lane`: i0 = ((g * ncplx + base + (par ? (N + 1) / 2 : 0)) * lanes + lane.
+struct BandRef {
+    double2* f;
+    signed char* pv;
+    long long plane, i0;
+    int lanes;
 };
 
 __host__ __device__ inline double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
@@ -151,6 +168,138 @@ __host__ __device__ bool band_solve(int Np, Entry entry, Rhs rhs, Out out) {
         }
     }
     return ok;
+}
+
+// The factorisation of band_solve alone, stored: per row 1/U_kk, the U row's
+// 2H off-diagonal entries, the H multipliers and the pivot offset.  The same
+// operations in the same order as band_solve, so that band_solve_stored
+// reproduces its results.  Returns false on a zero pivot.
+template <int H, class Entry>
+__host__ __device__ bool band_factor_store(int Np, Entry entry, const BandRef& st) {
+    constexpr int W = 2 * H + 1;
+    double2 win[H + 1][W];
+#pragma unroll
+    for (int i = 0; i <= H; i++)
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - i;
+            win[i][j] = (i < Np && d >= -H && d <= H && j < Np) ? entry(i, d) : make_double2(0, 0);
+        }
+    bool ok = true;
+    for (int k = 0; k < Np; k++) {
+        int p = 0;
+        double best = c_abs1(win[0][0]);
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const double v = (k + i < Np) ? c_abs1(win[i][0]) : -1.0;
+            if (v > best) {
+                best = v;
+                p = i;
+            }
+        }
+        if (best == 0.0) ok = false;
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < W; j++) {
+                const double2 t0 = win[0][j], ti = win[i][j];
+                win[0][j] = sw ? ti : t0;
+                win[i][j] = sw ? t0 : ti;
+            }
+        }
+        const double2 rp = best == 0.0 ? make_double2(0, 0) : c_div(make_double2(1, 0), win[0][0]);
+        const long long e = st.i0 + (long long)k * st.lanes;
+        st.pv[e] = (signed char)p;
+        st.f[e] = rp;
+#pragma unroll
+        for (int j = 1; j < W; j++) st.f[j * st.plane + e] = win[0][j];
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const double2 l = c_mul(win[i][0], rp);
+            st.f[(2 * H + i) * st.plane + e] = l;
+#pragma unroll
+            for (int j = 1; j < W; j++) win[i][j] = c_sub(win[i][j], c_mul(l, win[0][j]));
+        }
+#pragma unroll
+        for (int i = 0; i < H; i++) {
+#pragma unroll
+            for (int j = 0; j < W - 1; j++) win[i][j] = win[i + 1][j + 1];
+            win[i][W - 1] = make_double2(0, 0);
+        }
+        const int rn = k + 1 + H;
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - H;
+            win[H][j] = (rn < Np && k + 1 + j < Np) ? entry(rn, d) : make_double2(0, 0);
+        }
+    }
+    return ok;
+}
+
+// Forward elimination and back substitution of band_solve with the factors
+// that band_factor_store wrote.
+template <int H, int MAXR, int NR, class Rhs, class Out>
+__host__ __device__ void band_solve_stored(int Np, const BandRef& st, Rhs rhs, Out out) {
+    constexpr int W = 2 * H + 1;
+    double2 y[MAXR][NR];
+    double2 wr[H + 1][NR];
+#pragma unroll
+    for (int i = 0; i <= H; i++)
+#pragma unroll
+        for (int r = 0; r < NR; r++) wr[i][r] = i < Np ? rhs(i, r) : make_double2(0, 0);
+    for (int k = 0; k < Np; k++) {
+        const long long e = st.i0 + (long long)k * st.lanes;
+        const int p = RX_LDG(&st.pv[e]);
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const double2 t0 = wr[0][r], ti = wr[i][r];
+                wr[0][r] = sw ? ti : t0;
+                wr[i][r] = sw ? t0 : ti;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) y[k][r] = wr[0][r];
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const double2 l = ld(&st.f[(2 * H + i) * st.plane + e]);
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[i][r] = c_sub(wr[i][r], c_mul(l, wr[0][r]));
+        }
+#pragma unroll
+        for (int i = 0; i < H; i++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[i][r] = wr[i + 1][r];
+        const int rn = k + 1 + H;
+#pragma unroll
+        for (int r = 0; r < NR; r++) wr[H][r] = rn < Np ? rhs(rn, r) : make_double2(0, 0);
+    }
+    double2 x[W][NR];
+#pragma unroll
+    for (int j = 0; j < W; j++)
+#pragma unroll
+        for (int r = 0; r < NR; r++) x[j][r] = make_double2(0, 0);
+    for (int k = Np - 1; k >= 0; k--) {
+        const long long e = st.i0 + (long long)k * st.lanes;
+        const double2 rd = ld(&st.f[e]);
+        double2 u[W];
+#pragma unroll
+        for (int j = 1; j < W; j++) u[j] = ld(&st.f[j * st.plane + e]);
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            double2 s = y[k][r];
+#pragma unroll
+            for (int j = 1; j < W; j++) s = c_sub(s, c_mul(u[j], x[j - 1][r]));
+            const double2 xk = c_mul(s, rd);
+#pragma unroll
+            for (int j = W - 1; j > 0; j--) x[j][r] = x[j - 1][r];
+            x[0][r] = xk;
+            out(k, r, xk);
+        }
+    }
 }
 
 __host__ __device__ inline float2 f_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -306,11 +455,63 @@ __host__ __device__ bool band_solve_mixed(int Np, int refine, Entry entry, Rhs r
     return ok;
 }
 
+// Entry (k, dd) of the parity-`par` Phi system of the m-block at block row
+// base: alpha^4 I + alpha^2 C2 + alpha C1 + alpha^-1 Cm1 + C0 (rows par + 2k).
+__host__ __device__ inline double2 phi_entry(const RexiDev& d, int base, int par, double2 a, double2 a2, double2 ainv,
+                                             double2 a4, int k, int dd) {
+    const size_t nc5 = (size_t)d.ncplx * 5;
+    const int row = base + par + 2 * k;
+    const double2* c = d.Cphi + (size_t)row * 5 + (dd + 2);
+    double2 v = c_mul(a2, ld(c));
+    v = c_add(v, c_mul(a, ld(c + nc5)));
+    v = c_add(v, c_mul(ainv, ld(c + 2 * nc5)));
+    v = c_add(v, ld(c + 3 * nc5));
+    if (dd == 0) v = c_add(v, a4);
+    return v;
+}
+// Entry (k, dd) of the parity-`par` velocity system: alpha^2 I + Cvel.
+__host__ __device__ inline double2 vel_entry(const RexiDev& d, int base, int par, double2 a2, int k, int dd) {
+    const int row = base + par + 2 * k;
+    double2 v = ld(&d.Cvel[(size_t)row * 3 + dd + 1]);
+    if (dd == 0) v = c_add(v, a2);
+    return v;
+}
+__host__ __device__ inline BandRef band_ref(double2* f, signed char* pv, const RexiDev& d, long long gl, int base,
+                                            int N, int par) {
+    return BandRef{f, pv, d.plane, gl + (long long)(base + (par ? (N + 1) / 2 : 0)) * d.lanes, d.lanes};
+}
+
+// Factor the Phi and velocity systems of one pole and one m-block (both
+// parities) into the stored planes of d; gl = g * ncplx * lanes + lane.
+// Returns false on a zero pivot.  Only the Coriolis case has banded systems.
+__host__ __device__ inline bool rexi_factor_lane(const RexiDev& d, int m, double2 a, long long gl) {
+    const int am = m < 0 ? -m : m;
+    const int N = d.L + 1 - am;
+    const int base = block_off(d.L, m);
+    const double2 a2 = c_mul(a, a), a4 = c_mul(a2, a2);
+    const double2 ainv = c_div(make_double2(1, 0), a);
+    bool ok = true;
+    for (int par = 0; par < 2; par++) {
+        const int Np = (N - par + 1) >> 1;
+        if (Np <= 0) continue;
+        ok = band_factor_store<2>(
+                 Np, [&](int k, int dd) { return phi_entry(d, base, par, a, a2, ainv, a4, k, dd); },
+                 band_ref(d.fphi, d.pphi, d, gl, base, N, par)) && ok;
+        ok = band_factor_store<1>(
+                 Np, [&](int k, int dd) { return vel_entry(d, base, par, a2, k, dd); },
+                 band_ref(d.fvel, d.pvel, d, gl, base, N, par)) && ok;
+    }
+    return ok;
+}
+
 // One pole, one m-block: Phi solve (both l-parities), velocity right-hand
 // sides and the two velocity solves.  Writes the unscaled phi, u, v of the
 // block's N = L+1-|m| rows to phi / ra / rb; returns false on a zero pivot.
-template <int MAXN, bool MIXED = false>
-__host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* phi, double2* ra, double2* rb) {
+// STORED: substitutions only, with the factors rexi_factor_lane stored
+// (gl as there).
+template <int MAXN, bool MIXED = false, bool STORED = false>
+__host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* phi, double2* ra, double2* rb,
+                                   long long gl = 0) {
     const int L = d.L;
     const int am = m < 0 ? -m : m;
     const int N = L + 1 - am;
@@ -339,16 +540,7 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
         for (int par = 0; par < 2; par++) {
             const int Np = (N - par + 1) >> 1;
             if (Np <= 0) continue;
-            auto entry = [&](int k, int dd) -> double2 {
-                const int row = base + par + 2 * k;
-                const double2* c = d.Cphi + (size_t)row * 5 + (dd + 2);
-                double2 v = c_mul(a2, ld(c));
-                v = c_add(v, c_mul(a, ld(c + (size_t)nc * 5)));
-                v = c_add(v, c_mul(ainv, ld(c + (size_t)2 * nc * 5)));
-                v = c_add(v, ld(c + (size_t)3 * nc * 5));
-                if (dd == 0) v = c_add(v, a4);
-                return v;
-            };
+            auto entry = [&](int k, int dd) -> double2 { return phi_entry(d, base, par, a, a2, ainv, a4, k, dd); };
             auto rhs = [&](int k, int) -> double2 {
                 const int row = base + par + 2 * k;
                 double2 v = make_double2(0, 0);
@@ -357,7 +549,9 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
                 return v;
             };
             auto out = [&](int k, int, double2 x) { phi[par + 2 * k] = x; };
-            if constexpr (MIXED)
+            if constexpr (STORED)
+                band_solve_stored<2, (MAXN + 1) / 2, 1>(Np, band_ref(d.fphi, d.pphi, d, gl, base, N, par), rhs, out);
+            else if constexpr (MIXED)
                 ok = band_solve_mixed<2, (MAXN + 1) / 2, 1>(Np, d.refine, entry, rhs, out) && ok;
             else
                 ok = band_solve<2, (MAXN + 1) / 2, 1>(Np, entry, rhs, out) && ok;
@@ -399,19 +593,16 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
         for (int par = 0; par < 2; par++) {
             const int Np = (N - par + 1) >> 1;
             if (Np <= 0) continue;
-            auto entry = [&](int k, int dd) -> double2 {
-                const int row = base + par + 2 * k;
-                double2 v = ld(&d.Cvel[(size_t)row * 3 + dd + 1]);
-                if (dd == 0) v = c_add(v, a2);
-                return v;
-            };
+            auto entry = [&](int k, int dd) -> double2 { return vel_entry(d, base, par, a2, k, dd); };
             // u and v share the matrix: one factorisation, two right-hand sides
             auto rhs2 = [&](int k, int r) -> double2 { return r == 0 ? ra[par + 2 * k] : rb[par + 2 * k]; };
             auto out2 = [&](int k, int r, double2 x) {
                 if (r == 0) ra[par + 2 * k] = x;
                 else rb[par + 2 * k] = x;
             };
-            if constexpr (MIXED)
+            if constexpr (STORED)
+                band_solve_stored<1, (MAXN + 1) / 2, 2>(Np, band_ref(d.fvel, d.pvel, d, gl, base, N, par), rhs2, out2);
+            else if constexpr (MIXED)
                 ok = band_solve_mixed<1, (MAXN + 1) / 2, 2>(Np, d.refine, entry, rhs2, out2) && ok;
             else
                 ok = band_solve<1, (MAXN + 1) / 2, 2>(Np, entry, rhs2, out2) && ok;

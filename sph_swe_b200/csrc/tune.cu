@@ -5,7 +5,8 @@
 //     tile of 16, 32 or 64 real columns per CTA (8, 16, 32 fields) x kernel:
 //     P loaded by the TMA unit and B staged by producer warps, both operands
 //     loaded by the TMA unit (B prepared once per call), or P regenerated from
-//     recurrence checkpoints;
+//     recurrence checkpoints; and the FP64 CUDA-core kernel of the plain form
+//     (variant 16: more accurate than the mixed form needs, taken when faster);
 //   - the fixed-length ring FFTs (automatic grids): 2P rings per CTA with the
 //     default P or half of it (more CTAs per SM, shorter tiles);
 // with CUDA events on the caller's stream (one warm-up launch, then the mean
@@ -89,6 +90,7 @@ static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
             // B staged by producer warps (0), both operands loaded by the TMA unit (8), P regenerated (4)
             for (int src : {0, 8, 4})
                 for (int c = 1; c <= 3; c++) cand.push_back(src | c);
+            cand.push_back(16);  // FP64 CUDA-core kernel
         } else {
             if (!fixed_ring(h->nphi)) continue;
             cand = {0, 1};
@@ -103,8 +105,8 @@ static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
             float us = 0.f;
             auto run = [&]() -> int {
                 switch (kind) {
-                    case TUNE_TC_SYNTHESIS: return legendre_synthesis_tc(h, spec, h->nlm, L, F, fou, batch, s);
-                    case TUNE_TC_ANALYSIS: return legendre_analysis_tc(h, F, fou, spec, h->nlm, L, batch, s);
+                    case TUNE_TC_SYNTHESIS: return legendre_synthesis_real(h, spec, h->nlm, L, F, fou, batch, s);
+                    case TUNE_TC_ANALYSIS: return legendre_analysis_real(h, F, fou, spec, h->nlm, L, batch, s);
                     case TUNE_RING_ANALYSIS: return ring_analysis_real(h, grid, h->nspat, F, fou, mF, batch, s);
                     default: return ring_synthesis_real(h, F, fou, mF, grid, h->nspat, batch, nullptr, nullptr, 0, 0, s);
                 }
@@ -152,7 +154,7 @@ static int tune_load(Handle* h, const char* json) {
         if (!b || !v) break;
         batch = std::atoi(b + 8);
         var = std::atoi(v + 10);
-        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 15) {
+        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 31) {
             set_error("sph_tune_load: malformed entry");
             return SPH_ERR_ARG;
         }

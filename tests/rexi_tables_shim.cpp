@@ -4,6 +4,7 @@
 #include "../sph_swe_b200/csrc/rexi_lane.h"
 
 #include <cstring>
+#include <vector>
 
 using namespace sphgpu;
 
@@ -35,6 +36,56 @@ extern "C" int shim_rexi_pole(int L, int coriolis, double r, double T, double P,
     for (int m = -L; m <= L; m++) {
         const bool ok = rexi_lane<512>(d, m, make_double2(a_re, a_im), phi.data(), ra.data(), rb.data());
         if (!ok) rc = 1;
+        const int base = block_off(L, m), N = L + 1 - (m < 0 ? -m : m);
+        for (int i = 0; i < N; i++) {
+            o[base + i] = phi[i];
+            o[nc + base + i] = ra[i];
+            o[2 * nc + base + i] = rb[i];
+        }
+    }
+    return rc;
+}
+
+// The same pole with the banded systems factored once into stored planes
+// (rexi_factor_lane) and solved from them (rexi_lane<.., STORED>), as the
+// CUDA kernels do when the factors are kept between steps.
+extern "C" int shim_rexi_pole_stored(int L, int coriolis, double r, double T, double P, double a_re, double a_im,
+                                     const double* cphi, const double* cvel, const double* coef, const double* V,
+                                     double* out) {
+    const int nc = (L + 1) * (L + 1);
+    RexiDev d{};
+    d.L = L;
+    d.npoles = 1;
+    d.ngroups = 1;
+    d.ncplx = nc;
+    d.coriolis = coriolis;
+    d.r = r;
+    d.ir = 1.0 / r;
+    d.T = T;
+    d.P = P;
+    d.Cphi = reinterpret_cast<const double2*>(cphi);
+    d.Cvel = reinterpret_cast<const double2*>(cvel);
+    d.coef = coef;
+    d.V = reinterpret_cast<const double2*>(V);
+    std::vector<double2> fphi((size_t)7 * nc), fvel((size_t)4 * nc);
+    std::vector<signed char> pphi(nc, -1), pvel(nc, -1);
+    d.fphi = fphi.data();
+    d.pphi = pphi.data();
+    d.fvel = fvel.data();
+    d.pvel = pvel.data();
+    d.plane = nc;
+    d.lanes = 1;
+    const double2 a = make_double2(a_re, a_im);
+    int rc = 0;
+    for (int m = -L; m <= L; m++)
+        if (coriolis && !rexi_factor_lane(d, m, a, 0)) rc = 1;
+    // every row of every block has its pivot offset (0..H) written exactly once
+    for (int i = 0; i < nc && coriolis; i++)
+        if (pphi[i] < 0 || pphi[i] > 2 || pvel[i] < 0 || pvel[i] > 1) rc = 2;
+    std::vector<double2> phi(L + 1), ra(L + 1), rb(L + 1);
+    double2* o = reinterpret_cast<double2*>(out);
+    for (int m = -L; m <= L; m++) {
+        rexi_lane<512, false, true>(d, m, a, phi.data(), ra.data(), rb.data(), 0);
         const int base = block_off(L, m), N = L + 1 - (m < 0 ? -m : m);
         for (int i = 0; i < N; i++) {
             o[base + i] = phi[i];

@@ -49,6 +49,29 @@ def test_rexi_matches_oracle(gpu, oracle_mod, L, M, half, coriolis, fix, visc, s
         assert rel_l2(out[q], ref[q]) < 1e-10, q
 
 
+def test_rexi_stored_factors_match_on_the_fly(gpu, oracle_mod, monkeypatch):
+    """FP64 plans factor every banded system once at creation and only
+    substitute per step; SPH_REXI_STORE=0 factors on the fly every step.  Same
+    operations in the same order: the two agree to rounding over 4 steps."""
+    from sph_swe_b200.sph import Sph
+
+    L = 63
+    s, g = Sph(L), oracle_mod.Grid(L)
+    a, br, _ = oracle_mod.rexi_coeffs(0.2, 64, half=False)
+    h = g.spat_to_SH(bump_state(g))
+    u, v = random_spec(L, 2, seed=8, decay=3.0) * 5.0
+    outs = []
+    for store in ("1", "0"):
+        monkeypatch.setenv("SPH_REXI_STORE", store)
+        rx = s.rexi(a, br, radius=P6[0], gravity=P6[1], omega=P6[2], h0=P6[3], tau=P6[5])
+        st = torch.from_numpy(np.stack([h, u, v])).cuda()
+        rx.step(st, 4)
+        outs.append(st.cpu().numpy())
+        rx.close()
+    for q in range(3):
+        assert rel_l2(outs[0][q], outs[1][q]) < 1e-14, q
+
+
 def test_rexi_config2_t127_full_poles(gpu, oracle_mod):
     """REXI config: T127 192x384, Robert, h=0.2, M=256, full pole set (535 poles), tau = 3600 s."""
     from sph_swe_b200.sph import Sph

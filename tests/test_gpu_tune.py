@@ -1,7 +1,8 @@
 """The autotuner (sph_autotune / sph_tune_load / sph_tune_clear): every
 candidate variant runs, the chosen table re-applies, and the transforms give
 the same results with any variant (column tiles are exact alternatives; the
-two P_l^m sources agree to the mixed-form tolerance)."""
+two P_l^m sources agree to the mixed-form tolerance, and so does the FP64
+kernel that a mixed handle may take instead)."""
 import numpy as np
 import pytest
 import torch
@@ -28,23 +29,26 @@ def test_autotune_table_and_results(gpu, oracle_mod, L, prec):
     if prec == capi.SPH_PREC_MIXED:
         assert {"legendre_synthesis_tc", "legendre_analysis_tc"} <= names
         tc = [k for k in table["kernels"] if k["name"].endswith("_tc")]
-        assert all(len(k["candidates"]) == 9 for k in tc)
+        assert all(len(k["candidates"]) == 10 for k in tc)
     for k in table["kernels"]:
         assert k["us"] > 0 and k["us"] == min(c["us"] for c in k["candidates"])
     grid1 = s.SH_to_spat(spec)
     back1 = s.spat_to_SH(grid1)
     capi.check(capi.lib().sph_sync(s.h, None))
     tol = 1e-15 if prec == 0 else 1e-7
-    assert rel_l2(grid1.cpu().numpy(), grid0.cpu().numpy()) < tol
-    assert rel_l2(back1.cpu().numpy(), back0.cpu().numpy()) < tol
+    # a mixed handle's tuner may pick the FP64 kernel: within the mixed form's 1e-6
+    tuned_tol = tol if prec == 0 else 1e-6
+    assert rel_l2(grid1.cpu().numpy(), grid0.cpu().numpy()) < tuned_tol
+    assert rel_l2(back1.cpu().numpy(), back0.cpu().numpy()) < tuned_tol
     # every variant forced through a loaded table gives the same transforms
-    variants = [0, 1] if prec == 0 else [1, 2, 3, 5, 6, 7, 9, 10, 11]
+    variants = [0, 1] if prec == 0 else [1, 2, 3, 5, 6, 7, 9, 10, 11, 16]
     for v in variants:
         forced = {"lmax": L, "nphi": s.nphi, "kernels": [
             {"kind": kind, "batch": nb, "variant": (v if kind < 2 else v & 1)} for kind in range(4)]}
         s.tune_load(forced)
         g = s.SH_to_spat(spec)
-        assert rel_l2(g.cpu().numpy(), grid0.cpu().numpy()) < tol, v
+        # variant 16 is the FP64 kernel: it differs from the split-TF32 form by that form's error
+        assert rel_l2(g.cpu().numpy(), grid0.cpu().numpy()) < (tuned_tol if v == 16 else tol), v
     s.tune_clear()
     with pytest.raises(capi.SphError):
         s.tune_load({"lmax": L + 1, "nphi": s.nphi, "kernels": [{"kind": 0, "batch": 1, "variant": 1}]})
@@ -75,5 +79,7 @@ def test_autotuned_rk4_matches_untuned(gpu, oracle_mod):
             st = st0.clone()
             s.swe_rk4(p, st, 5)
         out.append(st.cpu().numpy())
+    # the tuned handle may run some stages on the FP64 kernel: the two runs then
+    # differ by the mixed form's error (h 2.6e-8 after 200 steps at T63)
     for q in range(3):
-        assert rel_l2(out[1][q], out[0][q]) < 1e-6 if q else rel_l2(out[1][q], out[0][q]) < 1e-9
+        assert rel_l2(out[1][q], out[0][q]) < (1e-6 if q else 1e-8)

@@ -150,6 +150,15 @@ def test_rexi_lane_matches_oracle_pole(shim, oracle_mod):
                                  x.dtype == np.complex128 else x.ctypes.data_as(dp) for x in (cphi, cvel, coef, Vst)],
                                  out.view(np.float64).ctypes.data_as(dp))
         assert rc == 0
+        # factors stored once, substitutions from the stored planes: the same numbers
+        outs = np.zeros((3, nc), np.complex128)
+        shim.shim_rexi_pole_stored.restype = ctypes.c_int
+        shim.shim_rexi_pole_stored.argtypes = shim.shim_rexi_pole.argtypes
+        rc = shim.shim_rexi_pole_stored(L, 1, r, T, P, a.real, a.imag, *[
+            x.view(np.float64).ctypes.data_as(dp) if x.dtype == np.complex128 else x.ctypes.data_as(dp)
+            for x in (cphi, cvel, coef, Vst)], outs.view(np.float64).ctypes.data_as(dp))
+        assert rc == 0
+        assert np.abs(outs - out).max() <= 1e-14 * np.abs(out).max(), k
         ref = g.rexi_pole((a_, g_, om, h0, 0.0, tau), alpha[k], br[k], phi0, u, v)
         for q in range(3):
             c = to_cidx(b * out[q])
