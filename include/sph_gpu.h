@@ -238,7 +238,13 @@ typedef struct sph_rexi_params {
 
 /* Prepare a REXI integrator for npoles poles alpha[k], beta[k] (host arrays of
  * interleaved complex).  Replaces the per-pole SWERexiSPH[Robert]::setup loop
- * (AppSWE.hpp:381-412, SWERexiSPHRobert.hpp:68-132). */
+ * (AppSWE.hpp:381-412, SWERexiSPHRobert.hpp:68-132).  With SPH_PREC_FP64 and
+ * the Coriolis term, every banded system (pole x m x parity) is factored here
+ * once and its factors are kept on the device (178 bytes per block row and
+ * pole: 1.6 GB at T127 with 535 poles) if they fit in half the free device
+ * memory; each sph_rexi_step then only substitutes.  A zero pivot met while
+ * factoring is reported by the first sph_rexi_step (SPH_ERR_SINGULAR), as when
+ * factoring per step.  Environment SPH_REXI_STORE=0: factor every step. */
 int sph_rexi_create(sph_handle* h, const double* alpha, const double* beta, int npoles, const sph_rexi_params* p,
                     sph_rexi** out);
 int sph_rexi_destroy(sph_rexi* r);
