@@ -107,7 +107,11 @@ int sph_SH_to_spat(sph_handle* h, const double* spec, double* spat, int batch, l
  * batches fail with SPH_ERR_ARG.  The first call on each device looks up the
  * array's device address; make that first call before any stream capture.
  * Calls that overlap on the GPU (other streams, other host threads) race on
- * the shared array: serialise them. */
+ * the shared array: serialise them.  A mixed handle whose autotuned synthesis
+ * variant for this batch is the loader-only tensor-core kernel needs a
+ * per-handle operand buffer that only an allocating call grows: until one
+ * sph_SH_to_spat with this batch has run, the call fails with SPH_ERR_ARG
+ * rather than allocate. */
 int sph_SH_to_spat_noalloc(sph_handle* h, const double* spec, double* spat, int batch, void* stream);
 
 /* Complex analysis / synthesis on complex grids (double2[nphi*nlat]) and

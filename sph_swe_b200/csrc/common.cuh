@@ -121,6 +121,7 @@ int tc_check(const Handle* h);
 // reserve the tensor-core operand workspace for calls of up to `batch` fields
 // (before a stream capture, which cannot allocate)
 int tc_reserve(const Handle* h, int batch);
+bool tc_synthesis_needs_alloc(const Handle* h, int lmax, int batch);
 int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F, long long ldF,
                           int batch, cudaStream_t s);
 int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec, int lmax,

@@ -1230,6 +1230,19 @@ static int tcb_ensure(MixedTables* T, size_t bytes, cudaStream_t s) {
     return SPH_OK;
 }
 
+// true if a synthesis of `batch` fields up to degree lmax would grow the
+// prepared-B buffer (the loader-only variant chosen by the autotuner for this
+// batch, and the buffer not yet large enough)
+bool tc_synthesis_needs_alloc(const Handle* h, int lmax, int batch) {
+    const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
+    if (!T || !T->streamed || batch <= 0) return false;
+    const int var = tune_get(h, TUNE_TC_SYNTHESIS, batch, 0);
+    if ((var & 16) || (var & 4) || !(var & 8)) return false;
+    const int nc = tc_cols_v(batch, var);
+    const int nct = (2 * batch + nc - 1) / nc;
+    return tcb_bytes(h, true, lmax, nct * nc) > T->Bcap;
+}
+
 int tc_reserve(const Handle* h, int batch) {
     MixedTables* T = static_cast<MixedTables*>(h->mixed);
     if (!T || !T->streamed || batch <= 0) return SPH_OK;

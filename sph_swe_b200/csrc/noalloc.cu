@@ -79,6 +79,16 @@ extern "C" int sph_SH_to_spat_noalloc(sph_handle* hh, const double* spec, double
         set_error("sph_SH_to_spat_noalloc: the current device is not the handle's device");
         return SPH_ERR_ARG;
     }
+    // a mixed handle whose autotuned synthesis variant for this batch is the
+    // loader-only kernel needs the handle's prepared-operand buffer; if that
+    // buffer has not been grown yet (by an allocating call with this batch),
+    // using the variant here would allocate, so refuse instead
+    if ((h->flags & SPH_PREC_MIXED) && tc_synthesis_needs_alloc(h, h->L, batch)) {
+        set_error("sph_SH_to_spat_noalloc: the autotuned tensor-core variant for " + std::to_string(batch) +
+                  " fields needs a workspace this handle has not reserved; make one allocating call "
+                  "(sph_SH_to_spat) with this batch first, or clear the tuning (sph_tune_clear)");
+        return SPH_ERR_ARG;
+    }
     void* scratch = nullptr;
     if (int rc = noalloc_scratch(dev, &scratch)) return rc;
     double2* F = static_cast<double2*>(scratch);

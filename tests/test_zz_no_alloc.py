@@ -50,3 +50,27 @@ def test_noalloc_rejects_batches_beyond_the_fixed_scratch(gpu):
     out = torch.empty(6, s.nphi, s.nlat, dtype=torch.float64, device="cuda")
     assert _noalloc(s, spec, out) == capi.SPH_ERR_ARG
     assert "at most 5 fields" in capi.last_error()
+
+
+def test_noalloc_refuses_an_unreserved_tuned_workspace(gpu):
+    """A mixed handle tuned to the loader-only tensor-core variant needs a
+    prepared-operand buffer that only an allocating call grows: until one has
+    run with that batch the no-allocation entry point refuses, afterwards it
+    runs and matches."""
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+    from tests.helpers import random_spec, rel_l2
+
+    L, batch = 63, 5
+    s = Sph(L, precision=capi.SPH_PREC_MIXED)
+    s.tune_load({"lmax": L, "nphi": s.nphi, "kernels": [{"kind": 0, "batch": batch, "variant": 9}]})
+    spec = torch.from_numpy(random_spec(L, batch, seed=321)).cuda()
+    out = torch.empty(batch, s.nphi, s.nlat, dtype=torch.float64, device="cuda")
+    assert _noalloc(s, spec, out) == capi.SPH_ERR_ARG
+    assert "workspace" in capi.last_error()
+    ref = s.SH_to_spat(spec).cpu().numpy()  # allocating call: grows the buffer
+    for _ in range(2):
+        out.fill_(float("nan"))
+        assert _noalloc(s, spec, out) == capi.SPH_OK, capi.last_error()
+        torch.cuda.synchronize()
+        assert rel_l2(out.cpu().numpy(), ref) < 1e-12
