@@ -13,6 +13,8 @@
 // Columns of the GEMM are (field, re/im) pairs.
 #include "common.cuh"
 
+#include <atomic>
+
 namespace sphgpu {
 
 namespace {
@@ -428,11 +430,13 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
     if (batch > 16) {
-        static bool attr = false;
-        if (!attr) {
+        // the shared-memory opt-in is a per-device attribute: once per device
+        static std::atomic<unsigned long long> attr_done{0};
+        const unsigned long long bit = h->device >= 0 && h->device < 64 ? 1ull << h->device : 0ull;
+        if (!bit || !(attr_done.load() & bit)) {
             SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_w, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               WSMEM_ANA));
-            attr = true;
+            attr_done.fetch_or(bit);
         }
         dim3 grid((sm.lmax + 1 + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
         k_legendre_analysis_w<<<grid, WNT, WSMEM_ANA, s>>>(h->plm, h->poff, h->nh, h->nlat, h->w, F, ldF, spec, sm,
