@@ -147,6 +147,15 @@ int sph_vec_spat_to_SH(sph_handle* h, const double* u, const double* v, double* 
 int sph_legendre_synthesis(sph_handle* h, const double* spec, double* four, int batch, void* stream);
 int sph_legendre_analysis(sph_handle* h, const double* four, double* spec, int batch, void* stream);
 
+/* Copy batch real packed spectra of handle hs (truncation Ls) into the layout
+ * of handle hd (truncation Ld): coefficients with n <= min(Ls, Ld) are
+ * copied, the rest of dst is zero.  Dense batches (nlm of each handle per
+ * field).  Replaces SPHData::spec_copyToDifferentModes (SPHData.hpp:108-187),
+ * which the REXI extended-modes option (sh_example X<k>, AppSWE.hpp:338-350,
+ * 434-445, 524-535) uses to run the REXI step at truncation L+k. */
+int sph_spec_copy_modes(const sph_handle* hs, const double* src, const sph_handle* hd, double* dst, int batch,
+                        void* stream);
+
 /* ---------------------------------------------------------------- spectral operators */
 
 enum sph_spec_op_id {

@@ -116,6 +116,15 @@ class SPHConfig {
         if (o_nlat) *o_nlat = spat_num_lat;
     }
 
+    // SPHConfig::setupAdditionalModes (SPHConfig.hpp:403-417): the
+    // quadratic-rule grid of base's truncation plus the added modes (the
+    // REXI extended-modes option); one truncation for n and m, as sph_create
+    void setupAdditionalModes(const SPHConfig* base, int added_lon, int added_lat, int precision = SPH_PREC_FP64) {
+        if (added_lon != added_lat)
+            throw std::runtime_error("setupAdditionalModes: the same number of modes in longitude and latitude");
+        create(base->spec_m_max + added_lon, base->spec_n_max + added_lat, 0, 0, precision);
+    }
+
     void shutdown() {
         free_grids();
         if (h_) sph_destroy(h_);
@@ -305,6 +314,20 @@ class SPHData {
               "sph_spec_op");
         out.data_spec_valid = true;
         return out;
+    }
+
+    // SPHData::spec_copyToDifferentModes (SPHData.hpp:108-187): this field's
+    // spectrum in o's truncation (shared modes copied, the others zero)
+    const SPHData& spec_copyToDifferentModes(SPHData& o) const {
+        if (o.sphConfig == sphConfig) throw std::runtime_error("spec_copyToDifferentModes: same configuration");
+        request_data_spectral();
+        if (sphConfig->stream != o.sphConfig->stream) cuda_check(cudaStreamSynchronize(sphConfig->stream), "sync");
+        check(sph_spec_copy_modes(h(), reinterpret_cast<const double*>(data_spec), o.h(),
+                                  reinterpret_cast<double*>(o.data_spec), 1, o.sphConfig->s()),
+              "sph_spec_copy_modes");
+        o.data_spec_valid = true;
+        o.data_spat_valid = false;
+        return *this;
     }
 
     void spec_set_zero() {

@@ -21,6 +21,7 @@ EXPORTS = (
     "sph_create", "sph_destroy", "sph_info", "sph_grid",
     "sph_spat_to_SH", "sph_SH_to_spat", "sph_SH_to_spat_noalloc", "sph_cplx_spat_to_SH", "sph_cplx_SH_to_spat",
     "sph_vec_SH_to_spat", "sph_vec_spat_to_SH", "sph_legendre_synthesis", "sph_legendre_analysis", "sph_spec_op",
+    "sph_spec_copy_modes",
     "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched", "sph_swe_rk4_launches",
     "sph_ensemble_create", "sph_ensemble_step", "sph_ensemble_launches", "sph_ensemble_destroy",
     "sph_autotune", "sph_tune_load", "sph_tune_clear",
@@ -69,6 +70,7 @@ def lib():
         for n in ("sph_vec_SH_to_spat", "sph_vec_spat_to_SH"):
             getattr(L, n).argtypes = [vp, vp, vp, vp, vp, i, i, vp]
         L.sph_spec_op.argtypes = [vp, i, vp, vp, d, d, d, d, i, i, vp]
+        L.sph_spec_copy_modes.argtypes = [vp, vp, vp, vp, i, vp]
         L.sph_SH_to_spat_noalloc.argtypes = [vp, vp, vp, i, vp]
         L.sph_legendre_synthesis.argtypes = [vp, vp, vp, i, vp]
         L.sph_legendre_analysis.argtypes = [vp, vp, vp, i, vp]

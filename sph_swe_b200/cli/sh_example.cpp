@@ -1,7 +1,7 @@
 // sh_example: the reference's command-line driver (main.cpp:37-210, AppSWE.hpp)
 // on top of libsphgpu.so through the C++ class surface of sph_swe.hpp.
 //
-//   sh_example T<n> P0 N<0|1> M<rexiM> H<h> I<halfpoles> R<dt> S<robert>
+//   sh_example T<n> P0 N<0|1> M<rexiM> H<h> I<halfpoles> X<added modes> R<dt> S<robert>
 //              Q<scenario> E<tend> V<visc> O<outdt> F<omega> W<M> [K<precision>] [C<file>] [D<file>]
 //   sh_example <n> [<m> [<nlon> <nlat>]] <flags...>
 //
@@ -64,6 +64,7 @@ struct Vars {
     double radius = 6.37122e6;
     double h0 = 10000.0;
     int precision = SPH_PREC_FP64;
+    int rexi_ext = 0;  // X<k>: REXI at truncation L + k (rexi_use_extended_modes)
     std::string dump;
     std::string resume;
 };
@@ -104,6 +105,7 @@ int parse(int argc, char** argv, Vars& v) {
             case 'O': v.out_dt = std::atof(a); break;
             case 'W': v.rexi_M = std::atoi(a); break;
             case 'K': v.precision = std::atoi(a); break;
+            case 'X': v.rexi_ext = std::atoi(a); break;
             case 'D': v.dump = a; break;
             case 'C': v.resume = a; break;
             default: break;  // unknown letters (and a trailing T<k>) are ignored, as in the reference
@@ -333,11 +335,35 @@ int main(int argc, char** argv) {
             REXI rexi;
             rexi.setup(v.rexi_h, v.rexi_M, 0, v.half_poles);
             std::printf(" + REXI poles: %zu\n", rexi.alpha.size());
-            SWERexiRobert stepper(&cfg, p, rexi, v.dt, false, v.precision);
-            while (done < nsteps) {
-                const long long k = steps_to_output(done);
-                stepper.run(h, u, w, (int)k);
-                done += k;
+            if (v.rexi_ext > 0) {
+                // AppSWE.hpp:338-350, 434-445, 524-535: every step copies the state up to
+                // truncation L + X, integrates there and copies it back down
+                SPHConfig cfg_ext;
+                cfg_ext.setupAdditionalModes(&cfg, v.rexi_ext, v.rexi_ext, v.precision);
+                std::printf(" + REXI additional modes: %d (T%d on %d x %d)\n", v.rexi_ext, cfg_ext.spec_n_max,
+                            cfg_ext.spat_num_lat, cfg_ext.spat_num_lon);
+                SWERexiRobert stepper(&cfg_ext, p, rexi, v.dt, false, v.precision);
+                SPHData he(&cfg_ext), ue(&cfg_ext), we(&cfg_ext);
+                while (done < nsteps) {
+                    const long long k = steps_to_output(done);
+                    for (long long i = 0; i < k; i++) {
+                        h.spec_copyToDifferentModes(he);
+                        u.spec_copyToDifferentModes(ue);
+                        w.spec_copyToDifferentModes(we);
+                        stepper.run(he, ue, we, 1);
+                        he.spec_copyToDifferentModes(h);
+                        ue.spec_copyToDifferentModes(u);
+                        we.spec_copyToDifferentModes(w);
+                    }
+                    done += k;
+                }
+            } else {
+                SWERexiRobert stepper(&cfg, p, rexi, v.dt, false, v.precision);
+                while (done < nsteps) {
+                    const long long k = steps_to_output(done);
+                    stepper.run(h, u, w, (int)k);
+                    done += k;
+                }
             }
         } else {
             SWERK4 stepper(&cfg, p);

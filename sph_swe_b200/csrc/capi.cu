@@ -255,4 +255,22 @@ int sph_spec_op(sph_handle* h, int op, const double* in, double* out, double a_r
                    make_double2(a_re, a_im), make_double2(b_re, b_im), batch, cplx ? 1 : 0, S(stream));
 }
 
+int sph_spec_copy_modes(const sph_handle* hs, const double* src, const sph_handle* hd, double* dst, int batch,
+                        void* stream) {
+    if (!hs || !hd || batch < 0 || (batch > 0 && (!src || !dst))) {
+        set_error("sph_spec_copy_modes: bad arguments");
+        return SPH_ERR_ARG;
+    }
+    if (hs->device != hd->device) {
+        set_error("sph_spec_copy_modes: the two handles are on different devices");
+        return SPH_ERR_ARG;
+    }
+    if (batch > 0 && src == dst) {
+        set_error("sph_spec_copy_modes: source and destination must not be the same array");
+        return SPH_ERR_ARG;
+    }
+    return spec_copy_modes(hs, reinterpret_cast<const double2*>(src), hs->nlm, hd, reinterpret_cast<double2*>(dst),
+                           hd->nlm, batch, S(stream));
+}
+
 }  // extern "C"

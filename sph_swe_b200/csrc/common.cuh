@@ -128,6 +128,8 @@ int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, doubl
                          int batch, cudaStream_t s);
 
 // spectral operators (packed real or complex layout)
+int spec_copy_modes(const Handle* hs, const double2* src, long long lds, const Handle* hd, double2* dst,
+                    long long ldd, int batch, cudaStream_t s);
 int spec_op(const Handle* h, int op, const double2* in, long long ld_in, double2* out, long long ld_out, double2 a,
             double2 b, int batch, int cplx, cudaStream_t s);
 

@@ -98,4 +98,29 @@ int spec_op(const Handle* h, int op, const double2* in, long long ld_in, double2
     return SPH_OK;
 }
 
+// Real packed spectra of truncation Ls -> truncation Ld, field by field
+// (SPHData::spec_copyToDifferentModes, SPHData.hpp:108-187): coefficients
+// with n <= min(Ls, Ld) are copied, the others of the output are zero.  Grid
+// (m of the output, field); threads along n.
+__global__ void k_spec_copy_modes(const double2* __restrict__ src, int Ls, long long lds, double2* __restrict__ dst,
+                                  int Ld, long long ldd) {
+    const int m = blockIdx.x;
+    const double2* x = src + (long long)blockIdx.y * lds;
+    double2* y = dst + (long long)blockIdx.y * ldd;
+    for (int n = m + threadIdx.x; n <= Ld; n += blockDim.x)
+        y[pidx(Ld, n, m)] = (n <= Ls) ? x[pidx(Ls, n, m)] : make_double2(0, 0);
+}
+
+int spec_copy_modes(const Handle* hs, const double2* src, long long lds, const Handle* hd, double2* dst,
+                    long long ldd, int batch, cudaStream_t s) {
+    if (batch <= 0) return SPH_OK;
+    if (batch > 65535) {
+        set_error("sph_spec_copy_modes: batch too large");
+        return SPH_ERR_ARG;
+    }
+    k_spec_copy_modes<<<dim3(hd->L + 1, batch), 128, 0, s>>>(src, hs->L, lds, dst, hd->L, ldd);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
 }  // namespace sphgpu

@@ -138,6 +138,15 @@ class Sph:
                                           int(cplx), _stream()))
         return out
 
+    def spec_copy_modes(self, x: torch.Tensor, dst: "Sph") -> torch.Tensor:
+        """Real spectra of this handle's truncation re-laid out for `dst`'s
+        truncation: shared coefficients copied, the rest zero
+        (SPHData::spec_copyToDifferentModes; see sph_spec_copy_modes)."""
+        batch = x.numel() // self.nlm
+        out = torch.empty(x.shape[:-1] + (dst.nlm,), dtype=torch.complex128, device=x.device)
+        capi.check(capi.lib().sph_spec_copy_modes(self.h, _ptr(x), dst.h, _ptr(out), batch, _stream()))
+        return out
+
     # ------------------------------------------------------------ autotuner
     def autotune(self, batch: int) -> dict:
         """Time the kernel variants for `batch` fields per launch, keep the

@@ -112,6 +112,31 @@ def test_sh_example_rexi_matches_oracle(gpu, oracle_mod, tmp_path):
         assert rel_l2(st[q * g.nlm:(q + 1) * g.nlm], ref) < 1e-10, q
 
 
+def test_sh_example_rexi_extended_modes_matches_oracle(gpu, oracle_mod, tmp_path):
+    """sh_example ... X2: every REXI step runs at T33 on its own grid, the state
+    copied up (zero-padded) before and truncated to T31 after it
+    (rexi_use_extended_modes, AppSWE.hpp:338-350, 434-445, 524-535)."""
+    st, out = _run_cli(["T31", "P0", "N0", "S1", "M64", "H0.2", "I0", "X2", "R3600", "E7200", "O1e9", "Q10"], tmp_path)
+    assert "REXI additional modes: 2 (T33" in out
+    g, ge = oracle_mod.Grid(31), oracle_mod.Grid(33)
+    pairs = [(g.idx(n, m), ge.idx(n, m)) for m in range(32) for n in range(m, 32)]
+    small, big = (np.array(x) for x in zip(*pairs))
+    state = [g.spat_to_SH(bump_state(g)), np.zeros(g.nlm, complex), np.zeros(g.nlm, complex)]
+    for _ in range(2):
+        ext = []
+        for q in range(3):
+            e = np.zeros(ge.nlm, complex)
+            e[big] = state[q][small]
+            ext.append(e)
+        rh, ru, rv, _ = ge.rexi_run((6.37122e6, 9.80616, 7.292e-5, 1e4, 1e5, 3600.0), *ext, 1, rexi_h=0.2, rexi_M=64,
+                                    half=False, robert=1)
+        for q, r in enumerate((rh, ru, rv)):
+            state[q] = np.zeros(g.nlm, complex)
+            state[q][small] = r[big]
+    for q in range(3):
+        assert rel_l2(st[q * g.nlm:(q + 1) * g.nlm], state[q]) < 1e-10, q
+
+
 def test_sh_example_writes_reference_csv(gpu, oracle_mod, tmp_path):
     """Output as AppSWE::write_output: files at t = 0, every O seconds and at the
     end, in the reference's CSV layout; the final h grid equals the synthesis of

@@ -166,3 +166,28 @@ def test_bad_arguments_fail_loudly(gpu):
     x = torch.zeros(s.nlm, dtype=torch.complex128, device="cuda")
     with pytest.raises(capi.SphError):
         s.spec_op("mu", x, out=x)
+
+
+def test_spec_copy_modes_between_truncations(gpu, oracle_mod):
+    """sph_spec_copy_modes (SPHData::spec_copyToDifferentModes): T31 -> T33
+    zero-pads, T33 -> T31 truncates, both exact."""
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+
+    s31, s33 = Sph(31), Sph(33)
+    g31, g33 = oracle_mod.Grid(31), oracle_mod.Grid(33)
+    x = random_spec(31, 3, seed=41)
+    up = s31.spec_copy_modes(torch.from_numpy(x).cuda(), s33).cpu().numpy()
+    want = np.zeros((3, g33.nlm), complex)
+    for m in range(32):
+        for n in range(m, 32):
+            want[:, g33.idx(n, m)] = x[:, g31.idx(n, m)]
+    assert np.array_equal(up, want)
+    y = random_spec(33, 2, seed=42)
+    down = s33.spec_copy_modes(torch.from_numpy(y).cuda(), s31).cpu().numpy()
+    want = np.array([[y[b, g33.idx(n, m)] for m in range(32) for n in range(m, 32)] for b in range(2)])
+    order = [g31.idx(n, m) for m in range(32) for n in range(m, 32)]
+    assert np.array_equal(down[:, order], want)
+    t = torch.from_numpy(x).cuda()
+    with pytest.raises(capi.SphError):
+        capi.check(capi.lib().sph_spec_copy_modes(s31.h, t.data_ptr(), s31.h, t.data_ptr(), 3, None))
