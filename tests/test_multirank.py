@@ -33,7 +33,7 @@ def _rank(rank, world, port, out):
 def test_max_over_ranks_gloo():
     world = 2
     port = _free_port()
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this (threaded) process
     out = mgr.dict()
     mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
     assert out[0] == out[1] == 3.0
