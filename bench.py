@@ -201,6 +201,15 @@ def _per_field_rel(a, b):
     return {"max": float(r.max()), "median": float(r.median()), "fields": int(r.numel())}
 
 
+def _per_field_rel_area(a, b, w):
+    """relL2 per field of grids [field][lon][lat] with every point weighted by
+    the Gauss weight of its latitude (the area-weighted variant)"""
+    import torch
+
+    sw = torch.as_tensor(w, dtype=a.dtype, device=a.device).sqrt()
+    return _per_field_rel(a * sw, b * sw)
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -234,6 +243,9 @@ def run_ours(args, rank, world):
         "divergence_roundtrip_vs_input": _per_field_rel(mx.d, div),
         "fp64_scalar_roundtrip_vs_input": _per_field_rel(f64.spec_out, spec),
         "fp64_vorticity_roundtrip_vs_input": _per_field_rel(f64.z, vort),
+        "scalar_synthesis_vs_fp64_area_weighted": _per_field_rel_area(mx.grid, f64.grid, mx.s.w),
+        "vector_u_vs_fp64_area_weighted": _per_field_rel_area(mx.u, f64.u, mx.s.w),
+        "vector_v_vs_fp64_area_weighted": _per_field_rel_area(mx.v, f64.v, mx.s.w),
     }
 
     ms = {}
