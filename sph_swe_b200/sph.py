@@ -247,6 +247,66 @@ class Rexi:
             pass
 
 
+
+class ShardedRexi:
+    """REXI with its poles split across the ranks of a torch.distributed
+    process group, one GPU per rank (the reference loops over all poles one
+    after another, AppSWE.hpp:452-523).  Rank r keeps poles r, r + W, r + 2W,
+    ... of the W ranks and each step sums only those; one all-reduce (sum) of
+    the state [h, u, v] per step then adds the ranks' parts.  The split is
+    exact: everything after the per-pole solves (the beta-weighted sum, the
+    real-part extraction, the implicit viscosity factor) is linear in the
+    poles' contributions.  Every rank takes the same collectives in the same
+    order, also when its own step fails; a failure on any rank (or a
+    non-finite h after the sum) raises SphError on all of them.
+
+    make_rexi(alpha_part, beta_part) builds the per-rank integrator (an
+    object with step(state, nsteps)); ShardedRexi.on(...) uses Rexi."""
+
+    def __init__(self, alpha, beta, make_rexi, group=None):
+        import torch.distributed as dist
+
+        self.group = group
+        rank, world = dist.get_rank(group), dist.get_world_size(group)
+        a = np.asarray(alpha, np.complex128)[rank::world]
+        b = np.asarray(beta, np.complex128)[rank::world]
+        self.npoles = len(a)
+        self.rx = make_rexi(a, b) if len(a) else None
+
+    @classmethod
+    def on(cls, sph: Sph, alpha, beta, params: capi.RexiParams, group=None) -> "ShardedRexi":
+        return cls(alpha, beta, lambda a, b: Rexi(sph, a, b, params), group)
+
+    def step(self, state: torch.Tensor, nsteps: int = 1) -> torch.Tensor:
+        """In place on state (3, nlm) complex128 = [h, u, v], on every rank."""
+        import torch.distributed as dist
+
+        for _ in range(nsteps):
+            err = None
+            try:
+                if self.rx is None:
+                    state.zero_()
+                else:
+                    self.rx.step(state, 1)
+            except capi.SphError as e:
+                err = e
+                state.zero_()
+            dist.all_reduce(torch.view_as_real(state), group=self.group)
+            code = torch.tensor([0.0 if err is None else float(err.code)], dtype=torch.float64, device=state.device)
+            dist.all_reduce(code, op=dist.ReduceOp.MAX, group=self.group)
+            if code.item() != 0.0:
+                if err is not None:
+                    raise err
+                raise capi.SphError(int(code.item()), "REXI step failed on another rank")
+            if not bool(torch.isfinite(torch.view_as_real(state[0])).all()):
+                raise capi.SphError(capi.SPH_ERR_NAN, "REXI step: instability detected (non-finite value in h)")
+        return state
+
+    def close(self):
+        if self.rx is not None and hasattr(self.rx, "close"):
+            self.rx.close()
+        self.rx = None
+
 class Ensemble:
     """Members of several truncations advanced by one CUDA graph.
 
