@@ -672,6 +672,25 @@ class SPHOperators {
         cx.data_spat_valid = true;
         return grid_div(spec_one_minus_mu_squared_diff_lat_mu(cx), x.sphConfig->inv_cos2());
     }
+    // d/dmu: I(D x) / (1 - mu^2) (SPHOperators.hpp:63-78); d/dphi is grad_lat (:86-91)
+    static SPHData diff_lat_mu(const SPHData& x) {
+        return grid_div(spec_one_minus_mu_squared_diff_lat_mu(x), x.sphConfig->inv_cos2());
+    }
+    static SPHData diff_lat_phi(const SPHData& x) { return grad_lat(x); }
+    // the truncated (1 - mu^2) d/dmu under its other two names (SPHOperators.hpp:224-230)
+    static SPHData spec_cosphi_squared_diff_lat_mu(const SPHData& x) { return spec_one_minus_mu_squared_diff_lat_mu(x); }
+    static SPHData spec_one_minus_sinphi_squared_diff_lat_mu(const SPHData& x) {
+        return spec_one_minus_mu_squared_diff_lat_mu(x);
+    }
+    // Robert-variable operators, U = u cos(phi) (SPHOperators.hpp:129-210):
+    // I(i m U) / cos^2, I(D V) / cos^2, i m Phi and D Phi (spectral)
+    static SPHData robert_div_lon(const SPHData& x) { return grid_div(diff_lon(x), x.sphConfig->inv_cos2()); }
+    static SPHData robert_div_lat(const SPHData& x) {
+        return grid_div(spec_cosphi_squared_diff_lat_mu(x), x.sphConfig->inv_cos2());
+    }
+    static SPHData robert_grad_lon(const SPHData& x) { return diff_lon(x); }
+    static SPHData robert_grad_lat(const SPHData& x) { return spec_one_minus_mu_squared_diff_lat_mu(x); }
+
     // vorticity grad_lon(v) - grad_lat(u) and divergence div_lon(u) + div_lat(v)
     // (SPHOperators.hpp:507-529); the sums are spectral, as SPHData's operators are
     static SPHData vort(const SPHData& u, const SPHData& v) { return grad_lon(v) - grad_lat(u); }

@@ -57,6 +57,11 @@ int main(int argc, char** argv) {
         SPHData g(&cfg);
         g.spat_update_lambda_gaussian_grid([](double lon, double mu, double& o) { o = mu * std::cos(lon) + 2.0; });
         put_spec(out, g);                                                // 15
+        put_spat(out, SPHOperators::diff_lat_mu(x));                     // 16 grid
+        put_spat(out, SPHOperators::robert_div_lon(x));                  // 17 grid
+        put_spat(out, SPHOperators::robert_div_lat(x));                  // 18 grid
+        put_spec(out, SPHOperators::robert_grad_lat(x));                 // 19
+        put_spec(out, SPHOperators::robert_grad_lon(x));                 // 20
         std::printf("nan %d absmax %.17g\n", (int)x.isAnyNaNorInf(), x.spat_reduce_abs_max());
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());

@@ -38,7 +38,7 @@ def test_class_operators_match_oracle(classes_bin, oracle_mod, tmp_path, L):
     nphi, nlat, nlm, ncplx = map(int, r.stdout.split()[:4])
     assert (nphi, nlat, nlm) == (g.nphi, g.nlat, g.nlm)
     raw = np.fromfile(outp, np.uint8)
-    kinds = "sssssgggsssgsss" + "s"
+    kinds = "sssssgggsssgsss" + "s" + "gggss"
     blocks, off = [], 0
     for k in kinds:
         n = nlm * 16 if k == "s" else nphi * nlat * 8
@@ -62,6 +62,13 @@ def test_class_operators_match_oracle(classes_bin, oracle_mod, tmp_path, L):
     assert rel_l2(blocks[13], vort) < 1e-12
     assert rel_l2(blocks[14], div) < 1e-12
     assert rel_l2(blocks[15], g.spat_to_SH(g.grid_from(lambda lon, mu: mu * np.cos(lon) + 2.0))) < 1e-13
+    # d/dmu and the Robert-variable operators (SPHOperators.hpp:63-78, 129-210)
+    for i, op in zip((16, 17, 18), ("diff_lat_mu", "robert_div_lon", "robert_div_lat")):
+        kind, r = g.real_op(op, x, kind="spec")
+        assert kind == "spat"
+        assert rel_l2(blocks[i].reshape(nphi, nlat), r) < 1e-12, op
+    assert rel_l2(blocks[19], g.real_op("d1mu2", x, kind="spec")[1]) < 1e-12
+    assert rel_l2(blocks[20], g.real_op("diff_lon", x, kind="spec")[1]) < 1e-12
     assert "nan 0" in r.stdout
 
 
