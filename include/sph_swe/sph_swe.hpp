@@ -155,6 +155,19 @@ class SPHConfig {
         grids();
         return cos_;
     }
+    // the same weights with every value twice, for complex grids (re, im)
+    const double* inv_cos_c() const {
+        grids();
+        return inv_cos_c_;
+    }
+    const double* inv_cos2_c() const {
+        grids();
+        return inv_cos2_c_;
+    }
+    const double* cos_grid_c() const {
+        grids();
+        return cos_c_;
+    }
 
   private:
     sph_handle* h_ = nullptr;
@@ -162,6 +175,9 @@ class SPHConfig {
     mutable double* inv_cos_ = nullptr;
     mutable double* inv_cos2_ = nullptr;
     mutable double* cos_ = nullptr;
+    mutable double* inv_cos_c_ = nullptr;
+    mutable double* inv_cos2_c_ = nullptr;
+    mutable double* cos_c_ = nullptr;
 
     void create(int mmax, int nmax, int nlat, int nphi, int precision) {
         shutdown();
@@ -199,9 +215,21 @@ class SPHConfig {
         cuda_check(cudaMemcpy(inv_cos_, a.data(), n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
         cuda_check(cudaMemcpy(inv_cos2_, b.data(), n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
         cuda_check(cudaMemcpy(cos_, c.data(), n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+        std::vector<double> a2(2 * n), b2(2 * n), c2(2 * n);
+        for (size_t k = 0; k < n; k++) {
+            a2[2 * k] = a2[2 * k + 1] = a[k];
+            b2[2 * k] = b2[2 * k + 1] = b[k];
+            c2[2 * k] = c2[2 * k + 1] = c[k];
+        }
+        cuda_check(cudaMalloc(&inv_cos_c_, 2 * n * 8), "cudaMalloc");
+        cuda_check(cudaMalloc(&inv_cos2_c_, 2 * n * 8), "cudaMalloc");
+        cuda_check(cudaMalloc(&cos_c_, 2 * n * 8), "cudaMalloc");
+        cuda_check(cudaMemcpy(inv_cos_c_, a2.data(), 2 * n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+        cuda_check(cudaMemcpy(inv_cos2_c_, b2.data(), 2 * n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+        cuda_check(cudaMemcpy(cos_c_, c2.data(), 2 * n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
     }
     void free_grids() {
-        for (double** p : {&inv_cos_, &inv_cos2_, &cos_})
+        for (double** p : {&inv_cos_, &inv_cos2_, &cos_, &inv_cos_c_, &inv_cos2_c_, &cos_c_})
             if (*p) {
                 cudaFree(*p);
                 *p = nullptr;
@@ -602,6 +630,34 @@ class SPHDataComplex {
     SPHDataComplex operator-(const SPHDataComplex& b) const { return axpby(1.0, *this, -1.0, b); }
     SPHDataComplex operator*(double v) const { return axpby(v, *this, 0.0, *this); }
 
+    // host spectrum (layout n*n+n+m) -> this field's spectrum
+    void spec_from_host(const std::vector<cplx>& v) {
+        if (v.size() != (size_t)sphConfig->cplx_spec_num_elems) throw std::runtime_error("spec_from_host: wrong size");
+        cuda_check(cudaMemcpyAsync(data_spec, v.data(), spec_bytes(), cudaMemcpyHostToDevice, sphConfig->stream), "ul");
+        cuda_check(cudaStreamSynchronize(sphConfig->stream), "sync");
+        data_spec_valid = true;
+        data_spat_valid = false;
+    }
+    std::vector<cplx> spat_to_host() const {
+        request_data_physical();
+        std::vector<cplx> v((size_t)sphConfig->spat_num_elems);
+        cuda_check(cudaMemcpyAsync(v.data(), data_spat, spat_bytes(), cudaMemcpyDeviceToHost, sphConfig->stream), "dl");
+        cuda_check(cudaStreamSynchronize(sphConfig->stream), "sync");
+        return v;
+    }
+    // x / (a - (b / r^2) n(n+1)) (SPHDataComplex.hpp:523-545)
+    SPHDataComplex spec_solve_helmholtz(cplx a, cplx b, double r) const {
+        request_data_spectral();
+        SPHDataComplex out(sphConfig);
+        const cplx br = b / (r * r);
+        check(sph_spec_op(h(), SPH_OP_HELMHOLTZ, reinterpret_cast<const double*>(data_spec),
+                          reinterpret_cast<double*>(out.data_spec), a.real(), a.imag(), br.real(), br.imag(), 1, 1,
+                          sphConfig->s()),
+              "sph_spec_op");
+        out.data_spec_valid = true;
+        return out;
+    }
+
     std::vector<cplx> spec_to_host() const {
         request_data_spectral();
         std::vector<cplx> v((size_t)sphConfig->cplx_spec_num_elems);
@@ -710,6 +766,87 @@ class SPHOperators {
         y.request_data_physical();
         SPHData out(y.sphConfig);
         check(sph_spat_op(y.h(), SPH_SPAT_MUL, y.data_spat, w, out.data_spat, 1.0, 0.0, y.sphConfig->spat_num_elems,
+                          y.sphConfig->s()),
+              "sph_spat_op");
+        out.data_spat_valid = true;
+        return out;
+    }
+};
+
+// ------------------------------------------------------------------ SPHOperatorsComplex
+// Replaces SPHOperatorsComplex (SPHOperatorsComplex.hpp): the same operators on
+// complex fields (m = -L..L); grid-valued ones divide on the grid after one
+// complex synthesis, as the reference does.
+class SPHOperatorsComplex {
+  public:
+    // x i m, truncated (1 - mu^2) d/dmu under its three names, mu x, mu^2 x,
+    // -n(n+1) x (SPHOperatorsComplex.hpp:27-50, 119-222, 430-470)
+    static SPHDataComplex diff_lon(const SPHDataComplex& x) { return spec(SPH_OP_DIFF_LON, x); }
+    static SPHDataComplex spec_one_minus_mu_squared_diff_lat_mu(const SPHDataComplex& x) { return spec(SPH_OP_D1MU2, x); }
+    static SPHDataComplex spec_cosphi_squared_diff_lat_mu(const SPHDataComplex& x) { return spec(SPH_OP_D1MU2, x); }
+    static SPHDataComplex spec_one_minus_sinphi_squared_diff_lat_mu(const SPHDataComplex& x) {
+        return spec(SPH_OP_D1MU2, x);
+    }
+    static SPHDataComplex mu(const SPHDataComplex& x) { return spec(SPH_OP_MU, x); }
+    static SPHDataComplex mu2(const SPHDataComplex& x) { return spec(SPH_OP_MU2, x); }
+    static SPHDataComplex laplace(const SPHDataComplex& x) { return spec(SPH_OP_LAPLACE, x); }
+
+    // I(i m x) / cos, I(D x) / cos, I(D x) / cos^2 (SPHOperatorsComplex.hpp:62-116, 224-282)
+    static SPHDataComplex grad_lon(const SPHDataComplex& x) { return grid_mul(diff_lon(x), x.sphConfig->inv_cos_c()); }
+    static SPHDataComplex grad_lat(const SPHDataComplex& x) {
+        return grid_mul(spec_one_minus_mu_squared_diff_lat_mu(x), x.sphConfig->inv_cos_c());
+    }
+    static SPHDataComplex diff_lat_mu(const SPHDataComplex& x) {
+        return grid_mul(spec_one_minus_mu_squared_diff_lat_mu(x), x.sphConfig->inv_cos2_c());
+    }
+    static SPHDataComplex diff_lat_phi(const SPHDataComplex& x) { return grad_lat(x); }
+    // div_lon = grad_lon; div_lat = I(D F(cos x)) / cos^2 (SPHOperatorsComplex.hpp:284-344)
+    static SPHDataComplex div_lon(const SPHDataComplex& x) { return grad_lon(x); }
+    static SPHDataComplex div_lat(const SPHDataComplex& x) {
+        const SPHDataComplex cx = grid_mul(x, x.sphConfig->cos_grid_c());
+        return grid_mul(spec_one_minus_mu_squared_diff_lat_mu(cx), x.sphConfig->inv_cos2_c());
+    }
+    // Robert-variable operators (SPHOperatorsComplex.hpp:347-428)
+    static SPHDataComplex robert_div_lon(const SPHDataComplex& x) {
+        return grid_mul(diff_lon(x), x.sphConfig->inv_cos2_c());
+    }
+    static SPHDataComplex robert_div_lat(const SPHDataComplex& x) {
+        return grid_mul(spec_cosphi_squared_diff_lat_mu(x), x.sphConfig->inv_cos2_c());
+    }
+    static SPHDataComplex robert_grad_lon(const SPHDataComplex& x) { return diff_lon(x); }
+    static SPHDataComplex robert_grad_lat(const SPHDataComplex& x) { return spec_cosphi_squared_diff_lat_mu(x); }
+
+    // vorticity and divergence (SPHOperatorsComplex.hpp:480-550); sums are spectral
+    static SPHDataComplex vort(const SPHDataComplex& lon, const SPHDataComplex& lat) {
+        return grad_lon(lat) - grad_lat(lon);
+    }
+    static SPHDataComplex robert_vort(const SPHDataComplex& lon, const SPHDataComplex& lat) {
+        return robert_grad_lon(lat) - robert_grad_lat(lon);
+    }
+    static SPHDataComplex div(const SPHDataComplex& lon, const SPHDataComplex& lat) {
+        return div_lon(lon) + div_lat(lat);
+    }
+    // one division: I(i m U + D V) / cos^2
+    static SPHDataComplex robert_div(const SPHDataComplex& lon, const SPHDataComplex& lat) {
+        return grid_mul(diff_lon(lon) + spec_cosphi_squared_diff_lat_mu(lat), lon.sphConfig->inv_cos2_c());
+    }
+
+  private:
+    static SPHDataComplex spec(int op, const SPHDataComplex& x) {
+        x.request_data_spectral();
+        SPHDataComplex out(x.sphConfig);
+        check(sph_spec_op(x.h(), op, reinterpret_cast<const double*>(x.data_spec),
+                          reinterpret_cast<double*>(out.data_spec), 0.0, 0.0, 0.0, 0.0, 1, 1, x.sphConfig->s()),
+              "sph_spec_op");
+        out.data_spec_valid = true;
+        return out;
+    }
+    // y times a real weight per grid point (w: the doubled grids of SPHConfig)
+    static SPHDataComplex grid_mul(const SPHDataComplex& y, const double* w) {
+        y.request_data_physical();
+        SPHDataComplex out(y.sphConfig);
+        check(sph_spat_op(y.h(), SPH_SPAT_MUL, reinterpret_cast<const double*>(y.data_spat), w,
+                          reinterpret_cast<double*>(out.data_spat), 1.0, 0.0, 2LL * y.sphConfig->spat_num_elems,
                           y.sphConfig->s()),
               "sph_spat_op");
         out.data_spat_valid = true;

@@ -26,6 +26,51 @@ def classes_bin(gpu, tmp_path_factory):
     return out
 
 
+@pytest.fixture(scope="module")
+def classes_cplx_bin(gpu, tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("cppc") / "classes_check_cplx")
+    cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "cpp", "classes_check_cplx.cpp"), "-o", out, "-L", PKG, "-lsphgpu",
+           "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath," + PKG, "-Wl,-rpath,/usr/local/cuda/lib64"]
+    subprocess.run(cmd, check=True)
+    return out
+
+
+def test_complex_class_operators_match_oracle(classes_cplx_bin, oracle_mod, tmp_path):
+    """SPHDataComplex / SPHOperatorsComplex (SPHOperatorsComplex.hpp) against the
+    oracle's complex operators; the compositions the oracle lacks (Helmholtz,
+    robert_vort, robert_div, diff_lat_mu) against the same compositions of
+    oracle pieces."""
+    L = 31
+    g = oracle_mod.Grid(L)
+    x, y = random_spec(L, 2, seed=77, cplx=True)
+    inp = tmp_path / "in.bin"
+    np.concatenate([x, y]).astype(np.complex128).tofile(inp)
+    outp = tmp_path / "out.bin"
+    r = subprocess.run([classes_cplx_bin, str(L), str(inp), str(outp)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    nphi, nlat, ncplx = map(int, r.stdout.split()[:3])
+    assert (nphi, nlat, ncplx) == (g.nphi, g.nlat, g.ncplx)
+    kinds = "cccccgggccgg"
+    raw = np.fromfile(outp, np.complex128)
+    blocks, off = [], 0
+    for k in kinds:
+        n = ncplx if k == "c" else nphi * nlat
+        blocks.append(raw[off:off + n] if k == "c" else raw[off:off + n].reshape(nphi, nlat))
+        off += n
+    assert off == raw.size
+    op = lambda name, v: g.cplx_op(name, v, kind="spec")[1]
+    for i, name in enumerate(["diff_lon", "d1mu2", "mu", "mu2", "laplace", "grad_lon", "grad_lat", "div_lat"]):
+        assert rel_l2(blocks[i], op(name, x)) < 1e-12, name
+    n = np.concatenate([np.full(2 * l + 1, l) for l in range(L + 1)]).astype(float)
+    a, b = 1.5 + 0.5j, (2.0e-3 + 1.0e-3j) / 9.0
+    assert rel_l2(blocks[8], x / (a - b * n * (n + 1))) < 1e-14
+    assert rel_l2(blocks[9], op("diff_lon", y) - op("d1mu2", x)) < 1e-13
+    c2 = g.cosphi[None, :] ** 2
+    assert rel_l2(blocks[10], g.cplx_SH_to_spat(op("diff_lon", x) + op("d1mu2", y)) / c2) < 1e-12
+    assert rel_l2(blocks[11], g.cplx_SH_to_spat(op("d1mu2", x)) / c2) < 1e-12
+
+
 @pytest.mark.parametrize("L", [31, 63])
 def test_class_operators_match_oracle(classes_bin, oracle_mod, tmp_path, L):
     g = oracle_mod.Grid(L)
