@@ -247,6 +247,12 @@ typedef struct sph_rexi_params {
     int fix_z5robert;  /* 0: reproduce SPHSolverComplex.hpp:305-309 as written */
     int precision;     /* SPH_PREC_FP64 direct, SPH_PREC_MIXED (complex FP32
                           factor/solve + FP64 iterative refinement)          */
+    int factor_each_step; /* 1: never keep the factors of the banded systems
+                          (FP64 form) but factor them in every step, as the
+                          reference does; for plans of one or a few poles,
+                          whose stored factors would cost more memory than
+                          their steps cost time.  0 (zero-initialised): keep
+                          them when they fit (see sph_rexi_create)          */
 } sph_rexi_params;
 
 /* Prepare a REXI integrator for npoles poles alpha[k], beta[k] (host arrays of

@@ -968,4 +968,89 @@ class SWERexiRobert : public SWERK4 {
     sph_rexi* r_ = nullptr;
 };
 
+// One pole of the REXI sum, SWERexiSPHRobert (SWERexiSPHRobert.hpp:68-258):
+// setup takes the pole alpha, weight beta (both divided by the time step
+// here, as there) and the physical constants; solve returns this pole's
+// Re(I(beta x)) for the geopotential phi0 and the Robert velocities u0, v0,
+// which the caller sums over the poles as AppSWE::run does.  Each object is a
+// one-pole plan of sph_rexi that factors its banded systems in every solve
+// (sph_rexi_params.factor_each_step).  SWERexiRobert runs all poles of a step
+// in one launch instead.
+class SWERexiSPHRobert {
+  public:
+    SWERexiSPHRobert() = default;
+    SWERexiSPHRobert(const SWERexiSPHRobert&) = delete;
+    SWERexiSPHRobert& operator=(const SWERexiSPHRobert&) = delete;
+    SWERexiSPHRobert(SWERexiSPHRobert&& o) noexcept { swap(o); }
+    SWERexiSPHRobert& operator=(SWERexiSPHRobert&& o) noexcept {
+        swap(o);
+        return *this;
+    }
+    ~SWERexiSPHRobert() { release(); }
+
+    void setup(SPHConfig* cfg, const cplx& alpha, const cplx& beta, double radius, double coriolis_omega,
+               double avg_geopotential, double timestep_size, bool include_coriolis_effect = true) {
+        release();
+        cfg_ = cfg;
+        sph_rexi_params rp{};
+        rp.radius = radius;
+        rp.gravity = 1.0;  // the state is the geopotential itself
+        rp.omega = coriolis_omega;
+        rp.h0 = avg_geopotential;
+        rp.viscosity = 0.0;  // AppSWE applies viscosity after the pole sum
+        rp.tau = timestep_size;
+        rp.robert = 1;
+        rp.coriolis = include_coriolis_effect ? 1 : 0;
+        rp.fix_z5robert = 0;
+        rp.precision = SPH_PREC_FP64;
+        rp.factor_each_step = 1;
+        const double ab[4] = {alpha.real(), alpha.imag(), beta.real(), beta.imag()};
+        check(sph_rexi_create(cfg->handle(), ab, ab + 2, 1, &rp, &r_), "sph_rexi_create");
+        cuda_check(cudaMalloc(&state_, 3 * sizeof(cplx) * (size_t)cfg->spec_num_elems), "cudaMalloc");
+    }
+
+    void solve(const SPHData& phi0, const SPHData& u0, const SPHData& v0, SPHData& o_phi, SPHData& o_u,
+               SPHData& o_v) {
+        if (!r_) throw std::runtime_error("SWERexiSPHRobert: solve before setup");
+        const size_t n = (size_t)cfg_->spec_num_elems;
+        const SPHData* in[3] = {&phi0, &u0, &v0};
+        for (int k = 0; k < 3; k++) {
+            in[k]->request_data_spectral();
+            cuda_check(cudaMemcpyAsync(state_ + k * n, in[k]->data_spec, n * sizeof(cplx), cudaMemcpyDeviceToDevice,
+                                       cfg_->stream),
+                       "copy");
+        }
+        check(sph_rexi_step(r_, reinterpret_cast<double*>(state_), 1, cfg_->s()), "sph_rexi_step");
+        SPHData* out[3] = {&o_phi, &o_u, &o_v};
+        for (int k = 0; k < 3; k++) {
+            if (out[k]->sphConfig != cfg_) *out[k] = SPHData(cfg_);
+            cuda_check(cudaMemcpyAsync(out[k]->data_spec, state_ + k * n, n * sizeof(cplx), cudaMemcpyDeviceToDevice,
+                                       cfg_->stream),
+                       "copy");
+            out[k]->mark_spectral();
+        }
+    }
+    // the reference's signature also passes its operator object, which holds no state
+    void solve(const SPHData& phi0, const SPHData& u0, const SPHData& v0, SPHData& o_phi, SPHData& o_u, SPHData& o_v,
+               const SPHOperatorsComplex&) {
+        solve(phi0, u0, v0, o_phi, o_u, o_v);
+    }
+
+  private:
+    SPHConfig* cfg_ = nullptr;
+    sph_rexi* r_ = nullptr;
+    cplx* state_ = nullptr;
+    void swap(SWERexiSPHRobert& o) noexcept {
+        std::swap(cfg_, o.cfg_);
+        std::swap(r_, o.r_);
+        std::swap(state_, o.state_);
+    }
+    void release() {
+        if (r_) sph_rexi_destroy(r_);
+        if (state_) cudaFree(state_);
+        r_ = nullptr;
+        state_ = nullptr;
+    }
+};
+
 }  // namespace sph_swe

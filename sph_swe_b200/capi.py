@@ -45,7 +45,7 @@ class RexiParams(ctypes.Structure):
     _fields_ = [("radius", ctypes.c_double), ("gravity", ctypes.c_double), ("omega", ctypes.c_double),
                 ("h0", ctypes.c_double), ("viscosity", ctypes.c_double), ("tau", ctypes.c_double),
                 ("robert", ctypes.c_int), ("coriolis", ctypes.c_int), ("fix_z5robert", ctypes.c_int),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("factor_each_step", ctypes.c_int)]
 
 
 _lib = None

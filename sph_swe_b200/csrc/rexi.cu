@@ -435,7 +435,7 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
     // depend on the pole and m only), if the factors fit in half the free
     // device memory; every step then runs the substitutions alone
     const char* store_env = std::getenv("SPH_REXI_STORE");  // "0": factor on the fly every step
-    if (cor && p->precision == SPH_PREC_FP64 && !(store_env && store_env[0] == '0')) {
+    if (cor && p->precision == SPH_PREC_FP64 && !p->factor_each_step && !(store_env && store_env[0] == '0')) {
         const long long plane = (long long)R->ngroups * nc * 32;
         const size_t bytes = (size_t)plane * (11 * sizeof(double2) + 2);
         size_t free_b = 0, total_b = 0;

@@ -71,6 +71,31 @@ def test_complex_class_operators_match_oracle(classes_cplx_bin, oracle_mod, tmp_
     assert rel_l2(blocks[11], g.cplx_SH_to_spat(op("d1mu2", x)) / c2) < 1e-12
 
 
+def test_per_pole_rexi_class_matches_oracle(gpu, oracle_mod, tmp_path):
+    """SWERexiSPHRobert used as AppSWE::run uses it (one object per pole,
+    solve, sum over the poles, divide by g) equals one SWERexiRobert step over
+    all poles and the oracle's REXI step (T31, M = 16, full pole set)."""
+    exe = str(tmp_path / "rexi_pole_check")
+    subprocess.run(["/usr/bin/g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-I",
+                    "/usr/local/cuda/include", os.path.join(ROOT, "tests", "cpp", "rexi_pole_check.cpp"), "-o", exe,
+                    "-L", PKG, "-lsphgpu", "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath," + PKG,
+                    "-Wl,-rpath,/usr/local/cuda/lib64"], check=True)
+    outp = tmp_path / "out.bin"
+    r = subprocess.run([exe, "31", str(outp)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    nlm, npoles = map(int, r.stdout.split()[:2])
+    assert npoles == 55
+    loop, full = np.fromfile(outp, np.complex128).reshape(2, 3, nlm)
+    g = oracle_mod.Grid(31)
+    h = g.spat_to_SH(bump_state(g))
+    z = np.zeros(g.nlm, complex)
+    ref = g.rexi_run((6.371e6, 9.80616, 7.292e-5, 1e4, 0.0, 3600.0), h, z, z, 1, rexi_h=0.2, rexi_M=16, half=False,
+                     robert=1)[:3]
+    for q in range(3):
+        assert rel_l2(loop[q], full[q]) < 1e-12, q
+        assert rel_l2(loop[q], ref[q]) < 1e-10, q
+
+
 @pytest.mark.parametrize("L", [31, 63])
 def test_class_operators_match_oracle(classes_bin, oracle_mod, tmp_path, L):
     g = oracle_mod.Grid(L)
