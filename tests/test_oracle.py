@@ -287,7 +287,7 @@ def test_config0_rounding_noise_floor(oracle_mod):
     """The T63 200-step nonlinear run amplifies rounding noise: a perturbation of
     the initial h coefficients by 1e-16 relative (below one ulp of the state)
     changes u and v by ~1e-10 relative L2 after 200 steps.  This is the floor
-    against which GPU-vs-oracle parity of u, v is judged."""
+    against which GPU-vs-oracle parity of u, v is measured."""
     from tests.helpers import bump_state
 
     g = oracle_mod.Grid(63)
