@@ -56,6 +56,17 @@ def test_error_reporting_without_gpu(lib):
     assert lib.sph_ensemble_step(None, 1, None) == capi.SPH_ERR_ARG
     assert lib.sph_ensemble_launches(None) == 0
     assert lib.sph_ensemble_destroy(None) == capi.SPH_OK
+    # argument checks of the other entry points come before any device call
+    assert lib.sph_spec_copy_modes(None, None, None, None, 1, None) == capi.SPH_ERR_ARG
+    assert "sph_spec_copy_modes" in capi.last_error()
+    assert lib.sph_SH_to_spat_noalloc(None, None, None, 1, None) == capi.SPH_ERR_ARG
+    assert "sph_SH_to_spat_noalloc" in capi.last_error()
+    r = ctypes.c_void_p()
+    assert lib.sph_rexi_create(None, None, None, 0, None, ctypes.byref(r)) == capi.SPH_ERR_ARG
+    assert lib.sph_rexi_step(None, None, 1, None) == capi.SPH_ERR_ARG
+    assert lib.sph_autotune(None, 8, None, 0, None) == capi.SPH_ERR_ARG
+    assert lib.sph_tune_load(None, b"{}") == capi.SPH_ERR_ARG
+    assert lib.sph_tune_clear(None) == capi.SPH_ERR_ARG
 
 
 @pytest.mark.parametrize("M,half", [(64, False), (256, False), (256, True), (32, True)])
