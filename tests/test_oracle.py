@@ -121,6 +121,39 @@ def test_p1_operator_kat(g63, op, ref, tol):
     assert np.abs(out - g63.grid_from(ref)).max() < tol
 
 
+# ------------------------------------------------------------------ P2 (AppTestSPHOperatorsComplex.hpp)
+@pytest.mark.parametrize("op,ref,tol", [
+    ("diff_lon", ga_dlambda, 1e-12),
+    ("grad_lon", lambda l, m: ga_dlambda(l, m) / np.sqrt(1 - m * m), 1e-11),
+    ("grad_lat", ga_dphi, 1e-10),
+    ("mu", lambda l, m: ga_f(l, m) * m, 1e-13),
+    ("mu2", lambda l, m: ga_f(l, m) * m * m, 1e-13),
+    ("d1mu2", lambda l, m: ga_dphi(l, m) * np.sqrt(1 - m * m), 1e-11),
+])
+def test_p2_complex_operator_kat(g63, op, ref, tol):
+    """The complex operators (the reference's P2 checks on the Gaussian test
+    function, AppTestSPHOperatorsComplex.hpp:229-490) on (1 + 2i) f, so that
+    the imaginary parts are exercised too."""
+    s = 1.0 + 2.0j
+    h = s * g63.grid_from(ga_f)
+    kind, out = g63.cplx_op(op, h)
+    if kind == "spec":
+        out = g63.cplx_SH_to_spat(out)
+    assert np.abs(out - s * g63.grid_from(ref)).max() < tol * abs(s)
+
+
+def test_p2_complex_identity_and_sph_basis(g63):
+    """Complex round trip of the test function and the Y_2^1 check of
+    AppTestSPHOperatorsComplex.hpp:33-78 ((1 - mu^2) d/dmu of the basis function)."""
+    f = g63.grid_from(ga_f) * (0.5 - 1.5j)
+    assert np.abs(g63.cplx_SH_to_spat(g63.cplx_spat_to_SH(f)) - f).max() < 1e-11
+    y21 = g63.grid_from(lambda lon, mu: -mu / 2.0 * np.sqrt(-15.0 * mu * mu + 15.0) * np.cos(lon) / np.sqrt(2 * np.pi))
+    kind, out = g63.cplx_op("d1mu2", y21.astype(complex))
+    ref = g63.grid_from(lambda lon, mu: (15.0 * mu * mu - 7.5) / (np.sqrt(15.0) * np.sqrt(1.0 - mu * mu)) *
+                        np.cos(lon) * (1.0 - mu * mu) / np.sqrt(2 * np.pi))
+    assert np.abs(g63.cplx_SH_to_spat(out) - ref).max() < 1e-13
+
+
 def test_p1_div_lat_reference_behaviour(g63):
     # div_lat = (1/c) d(c f)/dphi through spectral grad_lat of c f; the reference
     # prints this error without a threshold (AppTestSPHOperators.hpp:424-448);
