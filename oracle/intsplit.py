@@ -88,3 +88,31 @@ def synthesis(P, nh: int, nlat: int, L: int, spec: np.ndarray, S: int):
         F[:, m, :nh] = (north[:, :nb] + 1j * north[:, nb:]).T
         F[:, m, nlat - nh:] = (south[:, :nb] + 1j * south[:, nb:]).T[:, ::-1]
     return F, gmax
+
+
+def analysis(P, nh: int, nlat: int, L: int, F: np.ndarray, w: np.ndarray, S: int):
+    """Packed real spectra spec[b][nlm] from Fourier coefficients F[b][m][j]
+    (analysis convention F_m = (2 pi / nphi) sum_i f e^{-i m lambda_i}) with
+    the Gauss weights w[j] of the northern latitudes: per m and parity the
+    product of P^T (rows: degrees) with the weighted north +/- south sums
+    (K: latitudes).  Returns (spec, largest group sum)."""
+    nb = F.shape[0]
+    nlm = (L + 1) * (L + 2) // 2
+    spec = np.zeros((nb, nlm), complex)
+    gmax = 0
+    for m in range(L + 1):
+        Pm = P(m)
+        north = F[:, m, :nh]
+        south = F[:, m, nlat - nh:][:, ::-1]
+        base = m * (2 * L - m + 1) // 2 + m
+        for par in (0, 1):
+            A = Pm[par::2]  # K_par x nh: rows are degrees l = m + par + 2k
+            if A.shape[0] == 0:
+                continue
+            G = (north + south) if par == 0 else (north - south)
+            G = G * w[None, :nh]
+            B = np.concatenate([G.real.T, G.imag.T], axis=1)  # nh x 2 nb
+            C, g = matmul(A, B, S)
+            gmax = max(gmax, g)
+            spec[:, base + par: base + L - m + 1: 2] = (C[:, :nb] + 1j * C[:, nb:]).T
+    return spec, gmax

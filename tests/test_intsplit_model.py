@@ -51,3 +51,17 @@ def test_intsplit_matmul_is_exact_integer_arithmetic():
     C, gmax = intsplit.matmul(A, B, 5)
     assert gmax < 2 ** 31
     assert rel_l2(C, A @ B) < 1e-10
+
+
+@pytest.mark.parametrize("L", [31, 63])
+def test_intsplit_analysis_accuracy(oracle_mod, L):
+    g = oracle_mod.Grid(L)
+    P, nh = _plm(g)
+    spec = random_spec(L, 3, seed=L + 5)
+    grid = g.SH_to_spat(spec)
+    ref = g.spat_to_SH(grid)
+    nphi = g.nphi
+    F = (2 * np.pi / nphi) * np.fft.fft(grid, axis=1)[:, : L + 1, :]  # [b][m][j]
+    out, gmax = intsplit.analysis(P, nh, g.nlat, L, F, np.asarray(g.w), 4)
+    assert gmax < 2 ** 31
+    assert rel_l2(out, ref) < 1e-7, rel_l2(out, ref)
