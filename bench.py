@@ -74,14 +74,41 @@ def random_spec(L, n, seed, zero_mean=False):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons sampled DURING the timed region.
 
-    def __init__(self, index=0):
+    NVML (nvidia-ml-py) is polled every ~2 ms from a host thread, so even a
+    timed region of a few tens of milliseconds gets samples; nvidia-smi
+    (100 ms interval) is the fallback where NVML cannot be loaded."""
+
+    # NVML clocks-event-reason bits by their pynvml names
+    REASON_NAMES = (("nvmlClocksEventReasonHwSlowdown", "hw_slowdown"),
+                    ("nvmlClocksEventReasonHwThermalSlowdown", "hw_thermal_slowdown"),
+                    ("nvmlClocksEventReasonHwPowerBrakeSlowdown", "hw_power_brake_slowdown"),
+                    ("nvmlClocksEventReasonSwThermalSlowdown", "sw_thermal_slowdown"),
+                    ("nvmlClocksEventReasonSwPowerCap", "sw_power_cap"))
+
+    def __init__(self, index=0, period_s=0.002):
         self.index = index
-        self.samples = []
+        self.period = period_s
+        self.samples = []  # (sm_mhz, max_mhz, [reasons])
         self.proc = None
+        self.nvml = None
+        self._stop = threading.Event()
 
     def __enter__(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.dev = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.dev, pynvml.NVML_CLOCK_SM))
+            self.bits = [(int(getattr(pynvml, a)), n) for a, n in self.REASON_NAMES if hasattr(pynvml, a)]
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -95,11 +122,35 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv = self.nvml
+        while not self._stop.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.dev, nv.NVML_CLOCK_SM))
+                bits = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.dev))
+                self.samples.append((mhz, self.max_mhz, [n for b, n in self.bits if bits & b]))
+            except Exception:
+                return
+            time.sleep(self.period)
+
     def _read(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            f = [x.strip() for x in line.split(",")]
+            try:
+                self.samples.append((float(f[0]), float(f[1]),
+                                     [names[k] for k in range(4) if len(f) > 3 + k and f[3 + k] == "Active"]))
+            except ValueError:
+                pass
 
     def __exit__(self, *a):
+        self._stop.set()
+        if self.nvml is not None:
+            self.thread.join(timeout=2)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -109,13 +160,11 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 3 + k and s[3 + k] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [x[0] for x in self.samples]
+        reasons = sorted({r for x in self.samples for r in x[2]})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(x[1] for x in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def measured_peaks():
@@ -565,28 +614,56 @@ def ensemble_rates(dev, args):
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle port)
-def cpu_baseline(min_seconds=10.0, max_reps=50):
-    """Oracle restatement of the same transforms on the host cores: repeated
-    inverse + forward of the 64 scalar T255 fields until >= min_seconds."""
-    from oracle import oracle as O
+class OracleCfg1:
+    """The transform-throughput step on the host cores through the oracle
+    (C++/OpenMP FP64 restatement of the reference's transforms; its vector
+    pair through the oracle's restatement of the exact vector transforms):
+    synthesis + analysis of the 64 scalar fields, vector synthesis of the 32
+    vorticity/divergence pairs to (u, v) and vector analysis back, i.e. the
+    same work and the same algorithmic flop count as one GPU step."""
 
-    g = O.Grid(L_CFG1)
-    spec = random_spec(L_CFG1, N_SCALAR, 7)
-    _, _, per_contr = cfg1_flops()
-    fft_per_field = 2.5 * g.nphi * math.log2(g.nphi) * g.nlat
-    g.spat_to_SH(g.SH_to_spat(spec[:2]))
-    reps = 0
+    def __init__(self):
+        from oracle import oracle as O
+        from oracle.vortdiv import VortDiv
+
+        O.build()
+        self.O = O
+        self.g = O.Grid(L_CFG1)
+        self.vd = VortDiv(self.g)
+        self.cos = np.sqrt(self.vd.c2)[None, :]
+        self.spec = random_spec(L_CFG1, N_SCALAR, 1)
+        self.vort = random_spec(L_CFG1, N_PAIRS, 1001, zero_mean=True)
+        self.div = random_spec(L_CFG1, N_PAIRS, 2001, zero_mean=True)
+
+    def step(self):
+        g, vd = self.g, self.vd
+        g.spat_to_SH(g.SH_to_spat(self.spec))
+        for k in range(N_PAIRS):
+            U, V = vd.vec_synthesis(self.vort[k], self.div[k])
+            u, v = U / self.cos, V / self.cos
+            vd.vec_analysis(u * self.cos, v * self.cos)
+
+    def cores(self):
+        return self.O.num_threads()
+
+
+def cpu_baseline(min_seconds=12.0, max_steps=40):
+    """Oracle restatement of the same step on the host cores, repeated until
+    >= min_seconds (a bounded sample of the headline workload)."""
+    c = OracleCfg1()
+    c.step()
+    steps = 0
     t0 = time.perf_counter()
-    while reps < max_reps:
-        g.spat_to_SH(g.SH_to_spat(spec))
-        reps += 1
+    while steps < max_steps:
+        c.step()
+        steps += 1
         if time.perf_counter() - t0 >= min_seconds:
             break
     dt = time.perf_counter() - t0
-    flops = reps * N_SCALAR * 2 * (per_contr + fft_per_field)
-    return {"value": flops / dt / 1e9, "unit": "GFLOP/s", "cores": O.num_threads(), "kind": "port",
-            "sample": f"{reps} x (inverse + forward) of the {N_SCALAR} scalar T255 fields "
-                      f"(oracle C++/OpenMP FP64, {dt:.1f} s)"}
+    flops = steps * sum(cfg1_flops()[:2])
+    return {"value": flops / dt / 1e9, "unit": "GFLOP/s", "cores": c.cores(), "kind": "port",
+            "sample": f"{steps} steps of the same workload (64 scalar fields + 32 vort/div pairs, inverse + forward, "
+                      f"T255) through the oracle (C++/OpenMP FP64), {dt:.1f} s"}
 
 
 def profile_case():
@@ -627,38 +704,70 @@ def profile_case():
 
 def run_reference(args, rank, world):
     """CPU arm: the oracle (C++/OpenMP FP64 restatement; the reference's own
-    SHTNS/FFTW/LAPACK build is unavailable on this machine) on all host cores.
-    One step: inverse + forward of 128 scalar T255 fields (the 64 scalar fields
-    and the 32 vector pairs counted as two scalar fields each)."""
+    SHTNS/FFTW/LAPACK build is unavailable on this machine) on all host cores,
+    on the same step as our arm: 64 scalar T255 fields and 32 vort/div pairs,
+    inverse + forward (the vector pair through the oracle's exact vector
+    transforms)."""
     if rank != 0:
         return None
-    from oracle import oracle as O
-
-    O.build()
-    g = O.Grid(L_CFG1)
-    spec = random_spec(L_CFG1, N_SCALAR + 2 * N_PAIRS, 7)
-    _, _, per_contr = cfg1_flops()
-    fft_per_field = 2.5 * g.nphi * math.log2(g.nphi) * g.nlat
+    c = OracleCfg1()
     for _ in range(args.warmup):
-        g.spat_to_SH(g.SH_to_spat(spec[:4]))
+        c.step()
     ts = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        g.spat_to_SH(g.SH_to_spat(spec))
+        c.step()
         ts.append(time.perf_counter() - t0)
     dt = float(np.mean(ts))
-    flops = spec.shape[0] * 2 * (per_contr + fft_per_field)
-    value = flops / dt / 1e9
-    sample = (f"per step inverse + forward of {spec.shape[0]} scalar T255 fields (oracle C++/OpenMP FP64; the "
-              "reference's SHTNS/FFTW/LAPACK build is unavailable on this machine)")
+    value = sum(cfg1_flops()[:2]) / dt / 1e9
+    sample = ("per step inverse + forward of the 64 scalar T255 fields and the 32 vort/div pairs (oracle C++/OpenMP "
+              "FP64; the reference's SHTNS/FFTW/LAPACK build is unavailable on this machine)")
     return {"metric": METRIC, "value": value, "unit": "GFLOP/s", "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "SHT throughput: T255 384x768 Gauss grid, 64 scalar fields + 32 vort/div pairs, "
-                                   "inverse + forward per step", "lmax": L_CFG1, "nlat": 384, "nphi": 768},
-            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": O.num_threads(), "kind": "port",
+                                   "inverse + forward per step", "lmax": L_CFG1, "nlat": 384, "nphi": 768,
+                       "fields": N_SCALAR, "vector_pairs": N_PAIRS, "gflop_per_step": sum(cfg1_flops()[:2]) / 1e9},
+            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": c.cores(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def _sig(x, n=3):
+    return float(f"{x:.{n}g}") if isinstance(x, (int, float)) and x == x else x
+
+
+def summary(line):
+    """The figures a reader needs, in a compact object printed LAST in the
+    line (the driver keeps the tail of the output): the FP64 form of the
+    headline step, every mixed/FP64 speed ratio, the worst per-field relative
+    L2 of the mixed form, and the Legendre kernel times."""
+    out = {"fp64_form_gflops": _sig(line.get("fp64_form", {}).get("value", float("nan")), 5),
+           "fp64_form_ms": _sig(line.get("fp64_form", {}).get("ms_per_step", float("nan")), 4),
+           "mixed_ms": _sig(line["ms_per_step"], 4)}
+    ratios = {"cfg1": line.get("mixed_over_fp64")}
+    for k, v in line.get("rk4", {}).items():
+        ratios["rk4_" + k] = v.get("mixed_over_fp64")
+    for k, v in line.get("rexi", {}).items():
+        ratios["rexi_" + k] = v.get("mixed_over_fp64")
+    if "ensemble" in line:
+        ratios["ensemble"] = line["ensemble"].get("mixed_over_fp64")
+    if "T1023" in line:
+        ratios["T1023"] = line["T1023"].get("mixed_over_fp64")
+    out["mixed_over_fp64"] = {k: _sig(v) for k, v in ratios.items() if v is not None}
+    acc = line.get("accuracy", {})
+    out["mixed_cfg1_max_rel_l2"] = {k.replace("_vs_fp64", "").replace("_vs_input", ""): _sig(v["max"], 2)
+                                    for k, v in acc.items() if not k.startswith("fp64") and "area" not in k}
+    runs = {}
+    for k, v in line.get("rk4", {}).items():
+        runs["rk4_" + k] = v.get("mixed_rel_l2_vs_fp64_after_nsteps")
+    if "T1023" in line:
+        runs["T1023"] = line["T1023"].get("mixed_rel_l2_vs_fp64_after_nsteps")
+    out["mixed_run_rel_l2"] = {k: {q: _sig(x, 2) for q, x in v.items()} for k, v in runs.items() if v}
+    leg = line.get("roofline", {}).get("legendre", {})
+    out["legendre_us_syn_ana"] = {k: [_sig(v["synthesis_us"]), _sig(v["analysis_us"])] for k, v in leg.items()}
+    out["roofline_frac"] = _sig(line.get("roofline", {}).get("frac", float("nan")))
+    return out
 
 
 def main():
@@ -713,6 +822,7 @@ def main():
         if not args.quick:
             line["cpu_baseline"] = cpu_baseline()
         line.update(r["extra"])
+        line["summary"] = summary(line)
         print(json.dumps(line))
     if world > 1:
         import torch

@@ -101,11 +101,12 @@ int sph_SH_to_spat(sph_handle* h, const double* spec, double* spat, int batch, l
  * cudaMalloc/cudaFree synchronisation would break their latency budget).
  * Same result as sph_SH_to_spat on dense arrays (spec: batch*nlm complex,
  * spat: batch*nphi*nlat doubles).  The Fourier intermediate lives in a fixed
- * 8 MiB device array inside the library, shared by all calls and kept by
- * every GPU that loads the library until the process exits: batch is limited
- * to 8 MiB / ((L+1)*nlat*16 bytes) fields (5 at T255, 85 at T63) and larger
- * batches fail with SPH_ERR_ARG.  The first call on each device looks up the
- * array's device address; make that first call before any stream capture.
+ * 8 MiB device array inside the library, shared by all calls: batch is
+ * limited to 8 MiB / ((L+1)*nlat*16 bytes) fields (5 at T255, 85 at T63) and
+ * larger batches fail with SPH_ERR_ARG.  The array is reserved on a device,
+ * and its device address looked up, when the first handle is created on that
+ * device (sph_create, where allocating is still allowed); the device keeps it
+ * until the process exits, and this entry point only reuses it.
  * Calls that overlap on the GPU (other streams, other host threads) race on
  * the shared array: serialise them.  A mixed handle whose autotuned synthesis
  * variant for this batch is the loader-only tensor-core kernel needs a
@@ -330,6 +331,15 @@ int sph_tune_clear(sph_handle* h);
  * (a bounded wait inside a tensor-core kernel that gave up: SPH_ERR_TIMEOUT).
  * No counterpart in the reference, whose CPU path has no asynchronous errors. */
 int sph_sync(sph_handle* h, void* stream);
+
+/* Diagnostic of the failure path of the bounded device-side waits (mixed
+ * handles only): launches one block that waits, with the same bounded wait as
+ * the tensor-core Legendre kernels, for a barrier that nothing completes.  The
+ * wait gives up after `seconds` (0 < seconds <= 10) and records the failure
+ * in the handle exactly as a timed-out kernel would, so the next sph_sync
+ * returns SPH_ERR_TIMEOUT (once: the record is then cleared) and the CUDA
+ * context stays usable.  No counterpart in the reference. */
+int sph_wait_selftest(sph_handle* h, double seconds, void* stream);
 
 /* Copy the message of the last error into buf (NUL terminated); returns its length. */
 int sph_last_error(char* buf, int n);

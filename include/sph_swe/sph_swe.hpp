@@ -581,7 +581,17 @@ class SPHDataComplex {
         return *this;
     }
     // complex field from a real one through the grid (SPHDataComplex.hpp:67-77)
-    explicit SPHDataComplex(const SPHData& r) : SPHDataComplex(r.sphConfig) {
+    explicit SPHDataComplex(const SPHData& r) : SPHDataComplex(r.sphConfig) { spat_fromSPHData(r); }
+    // SPHDataComplex.hpp:93-104: assignment from a real field goes through the grid
+    SPHDataComplex& operator=(const SPHData& r) {
+        if (sphConfig != r.sphConfig) setup(r.sphConfig);
+        spat_fromSPHData(r);
+        return *this;
+    }
+    // grid of the real field as the real part, imaginary part zero; only the
+    // grid is valid afterwards (SPHDataComplex.hpp:162-175)
+    void spat_fromSPHData(const SPHData& r) {
+        if (r.sphConfig != sphConfig) throw std::runtime_error("spat_fromSPHData: fields of different configurations");
         r.request_data_physical();
         check(sph_spat_op(h(), SPH_SPAT_FILL, nullptr, nullptr, reinterpret_cast<double*>(data_spat), 0.0, 0.0,
                           2LL * sphConfig->spat_num_elems, sphConfig->s()),
@@ -589,8 +599,14 @@ class SPHDataComplex {
         cuda_check(cudaMemcpy2DAsync(data_spat, sizeof(cplx), r.data_spat, sizeof(double), sizeof(double),
                                      (size_t)sphConfig->spat_num_elems, cudaMemcpyDeviceToDevice, sphConfig->stream),
                    "copy");
+        data_spec_valid = false;
         data_spat_valid = true;
     }
+    // real part of this field's grid into o's grid; o becomes grid-valid only
+    // (SPHDataComplex.hpp:129-142)
+    void spat_RealToSPHData(SPHData& o) const { part_to(o, 0); }
+    // imaginary part likewise (SPHDataComplex.hpp:145-158)
+    void spat_ImagToSPHData(SPHData& o) const { part_to(o, 1); }
 
     void setup(SPHConfig* cfg) {
         release();
@@ -683,6 +699,16 @@ class SPHDataComplex {
     }
 
   private:
+    void part_to(SPHData& o, int part) const {
+        if (o.sphConfig != sphConfig) throw std::runtime_error("SPHDataComplex: fields of different configurations");
+        request_data_physical();
+        cuda_check(cudaMemcpy2DAsync(o.data_spat, sizeof(double), reinterpret_cast<const double*>(data_spat) + part,
+                                     sizeof(cplx), sizeof(double), (size_t)sphConfig->spat_num_elems,
+                                     cudaMemcpyDeviceToDevice, sphConfig->stream),
+                   "copy");
+        o.data_spec_valid = false;
+        o.data_spat_valid = true;
+    }
     void release() {
         if (sphConfig) {
             DeviceCache::put(data_spec, spec_bytes());

@@ -25,7 +25,8 @@ EXPORTS = (
     "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched", "sph_swe_rk4_launches",
     "sph_ensemble_create", "sph_ensemble_step", "sph_ensemble_launches", "sph_ensemble_destroy",
     "sph_autotune", "sph_tune_load", "sph_tune_clear",
-    "sph_spat_op", "sph_rexi_coefficients", "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_sync", "sph_last_error",
+    "sph_spat_op", "sph_rexi_coefficients", "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_sync", "sph_wait_selftest",
+    "sph_last_error",
 )
 
 
@@ -91,6 +92,7 @@ def lib():
         L.sph_rexi_coefficients.argtypes = [d, i, i, i, dp, dp, dp, ip]
         L.sph_rexi_step.argtypes = [vp, vp, i, vp]
         L.sph_sync.argtypes = [vp, vp]
+        L.sph_wait_selftest.argtypes = [vp, d, vp]
         L.sph_spat_op.argtypes = [vp, i, vp, vp, vp, d, d, ll, vp]
         L.sph_last_error.argtypes = [ctypes.c_char_p, i]
         for n in EXPORTS:

@@ -106,12 +106,17 @@ int sph_create(int lmax, int mmax, int nlat, int nphi, int flags, sph_handle** o
     h->flags = flags;
     h->device = dev;
     int rc = fft_kernels_init();
+    if (rc == SPH_OK) rc = legendre_kernels_init();
     if (rc == SPH_OK) rc = fft_plan_init(&h->fft, nphi);
     if (rc == SPH_OK) rc = setup_tables(h);
     if (rc == SPH_OK && (flags & SPH_PREC_MIXED)) {
         rc = tc_kernels_init();
         if (rc == SPH_OK) rc = tc_tables_build(h, lmax + 1);
     }
+    // reserve the fixed scratch of sph_SH_to_spat_noalloc on this device now,
+    // so that the no-allocation entry point never triggers the reservation
+    void* scratch = nullptr;
+    if (rc == SPH_OK) rc = noalloc_scratch(dev, &scratch);
     if (rc != SPH_OK) {
         sph_destroy(h);
         return rc;
@@ -164,6 +169,11 @@ int sph_sync(sph_handle* h, void* stream) {
     CHECK_H("sph_sync");
     SPH_CUDA_TRY(cudaStreamSynchronize(S(stream)));
     return tc_check(h);
+}
+
+int sph_wait_selftest(sph_handle* h, double seconds, void* stream) {
+    CHECK_H("sph_wait_selftest");
+    return tc_wait_selftest(h, seconds, S(stream));
 }
 
 int sph_spat_to_SH(sph_handle* h, const double* spat, double* spec, int batch, long long ld_spat, long long ld_spec,
@@ -265,8 +275,22 @@ int sph_spec_copy_modes(const sph_handle* hs, const double* src, const sph_handl
         set_error("sph_spec_copy_modes: the two handles are on different devices");
         return SPH_ERR_ARG;
     }
-    if (batch > 0 && src == dst) {
-        set_error("sph_spec_copy_modes: source and destination must not be the same array");
+    if (batch > 0) {
+        // blocks of the copy kernel read src while others write dst, so the
+        // two arrays must not share any byte
+        const char* s0 = reinterpret_cast<const char*>(src);
+        const char* s1 = s0 + sizeof(double2) * (size_t)hs->nlm * (size_t)batch;
+        const char* d0 = reinterpret_cast<const char*>(dst);
+        const char* d1 = d0 + sizeof(double2) * (size_t)hd->nlm * (size_t)batch;
+        if (s0 < d1 && d0 < s1) {
+            set_error("sph_spec_copy_modes: source and destination arrays overlap");
+            return SPH_ERR_ARG;
+        }
+    }
+    int dev = 0;
+    SPH_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != hs->device) {
+        set_error("sph_spec_copy_modes: the current device is not the handles' device");
         return SPH_ERR_ARG;
     }
     return spec_copy_modes(hs, reinterpret_cast<const double2*>(src), hs->nlm, hd, reinterpret_cast<double2*>(dst),

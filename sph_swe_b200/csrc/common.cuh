@@ -68,6 +68,10 @@ struct Handle {
 };
 
 int ensure_workspace(Handle* h, size_t bytes);
+// device address of the fixed scratch array of sph_SH_to_spat_noalloc on
+// device dev (the current device); the first call per device loads the
+// array's module, which reserves its memory (noalloc.cu)
+int noalloc_scratch(int dev, void** out);
 
 // kernel variants chosen by the autotuner (tune.cu); 0 = the built-in rule
 enum TuneKind { TUNE_TC_SYNTHESIS = 0, TUNE_TC_ANALYSIS = 1, TUNE_RING_ANALYSIS = 2, TUNE_RING_SYNTHESIS = 3 };
@@ -104,6 +108,7 @@ int ring_synthesis_cplx(const Handle* h, const double2* F, long long ldF, double
 
 // Legendre stage (FP64).  Real: spectral packed for degree lmax (L or L+1),
 // m = 0..min(lmax, L).  Complex: m = -L..L, layout n*n+n+m.
+int legendre_kernels_init();  // loads the FP64 Legendre kernels (lazy module loading)
 int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
                             long long ldF, int batch, cudaStream_t s);
 int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
@@ -118,6 +123,7 @@ int tc_kernels_init();
 int tc_tables_build(Handle* h, int lmax);
 void tc_tables_free(Handle* h);
 int tc_check(const Handle* h);
+int tc_wait_selftest(const Handle* h, double seconds, cudaStream_t s);
 // reserve the tensor-core operand workspace for calls of up to `batch` fields
 // (before a stream capture, which cannot allocate)
 int tc_reserve(const Handle* h, int batch);

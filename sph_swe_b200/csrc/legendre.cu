@@ -453,6 +453,20 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
     return SPH_OK;
 }
 
+// Query every FP64 Legendre kernel once.  Under lazy module loading (the
+// CUDA default) a kernel's code is loaded onto the device on first use; the
+// query loads it at handle creation instead, so that later calls (among them
+// the no-allocation synthesis) load nothing.
+int legendre_kernels_init() {
+    cudaFuncAttributes fa;
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_w));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_w));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_zero_top));
+    return SPH_OK;
+}
+
 int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
                             long long ldF, int batch, cudaStream_t s) {
     // mixed handles: the tensor-core kernels unless the autotuner found the FP64 kernel faster (variant bit 16)

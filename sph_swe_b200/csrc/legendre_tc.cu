@@ -164,19 +164,37 @@ __device__ __forceinline__ uint64_t globaltimer() {
 
 // Wait for a phase with a time limit; gives up early when another thread has
 // raised the CTA's abort flag, and raises it on its own timeout.
-__device__ __forceinline__ bool mbar_wait_abort(uint32_t mbar, uint32_t phase, volatile int* abort) {
+__device__ __forceinline__ bool mbar_wait_abort(uint32_t mbar, uint32_t phase, volatile int* abort,
+                                                unsigned long long limit_ns = tc::WAIT_NS) {
     if (mbar_try(mbar, phase)) return true;
     const uint64_t t0 = globaltimer();
     for (uint32_t i = 0;; i++) {
         if (mbar_try(mbar, phase)) return true;
         if ((i & 63) == 63) {
             if (*abort) return false;
-            if (globaltimer() - t0 > tc::WAIT_NS) {
+            if (globaltimer() - t0 > limit_ns) {
                 *abort = 1;
                 return false;
             }
         }
     }
+}
+
+// One CTA waits, with the bounded wait of the tensor-core kernels, for a
+// barrier phase that nothing completes: the wait gives up after limit_ns and
+// the CTA records the failure in the handle's flag exactly as a timed-out
+// tensor-core kernel does, then returns.  This exercises the SPH_ERR_TIMEOUT
+// path without a faulty kernel.
+__global__ void k_wait_selftest(unsigned long long limit_ns, int* flag) {
+    __shared__ __align__(8) unsigned long long bar;
+    __shared__ int abort;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar), 1);
+        abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !mbar_wait_abort(smem_u32(&bar), 0, &abort, limit_ns)) atomicOr(flag, 1);
 }
 
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -1351,9 +1369,26 @@ int tc_check(const Handle* h) {
     int flag = 0;
     SPH_CUDA_TRY(cudaMemcpy(&flag, T->flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
+        // reported once: the flag is cleared so that the handle stays usable
+        SPH_CUDA_TRY(cudaMemset(T->flag, 0, sizeof(int)));
         set_error("tensor-core Legendre stage: a bounded wait gave up");
         return SPH_ERR_TIMEOUT;
     }
+    return SPH_OK;
+}
+
+int tc_wait_selftest(const Handle* h, double seconds, cudaStream_t s) {
+    const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
+    if (!T) {
+        set_error("sph_wait_selftest: the bounded waits belong to the tensor-core kernels of a mixed handle");
+        return SPH_ERR_ARG;
+    }
+    if (!(seconds > 0.0 && seconds <= 10.0)) {
+        set_error("sph_wait_selftest: the limit must lie in (0, 10] seconds");
+        return SPH_ERR_ARG;
+    }
+    k_wait_selftest<<<1, 32, 0, s>>>((unsigned long long)(seconds * 1e9), T->flag);
+    SPH_CUDA_TRY(cudaGetLastError());
     return SPH_OK;
 }
 

@@ -16,16 +16,23 @@ namespace sphgpu {
 namespace {
 
 // 8 MiB of scratch: (L+1)*nlat*16 bytes per field, i.e. at most 5 fields at
-// T255 (384 latitudes), 85 at T63, 1 at T511.  Every GPU that loads the
-// library holds this array until the process exits.
+// T255 (384 latitudes), 85 at T63, 1 at T511.  The library is built without
+// relocatable device code, so this array sits in a device module of its own,
+// and with lazy module loading (the CUDA default) the driver reserves its
+// 8 MiB only when the module is first touched.  sph_create touches it (through
+// noalloc_scratch) on the handle's device, while allocating is still allowed;
+// from then on the device holds the array until the process exits.
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;
 __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double2)];
 
-// Device address of the array, looked up once per device (the symbol's name
-// in host code is only a host-side stand-in and must not reach a kernel).
+// Device address of the array, looked up once per device with that device
+// current (the symbol's name in host code is only a host-side stand-in and
+// must not reach a kernel).
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+}  // namespace
 
 int noalloc_scratch(int dev, void** out) {
     if (dev < 0 || dev >= kMaxDevices) {
@@ -46,7 +53,6 @@ int noalloc_scratch(int dev, void** out) {
     return SPH_OK;
 }
 
-}  // namespace
 }  // namespace sphgpu
 
 using namespace sphgpu;

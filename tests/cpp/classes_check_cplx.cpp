@@ -20,6 +20,10 @@ static void put_spat(std::ofstream& f, const SPHDataComplex& x) {
     const auto v = x.spat_to_host();
     f.write(reinterpret_cast<const char*>(v.data()), (std::streamsize)(v.size() * sizeof(cplx)));
 }
+static void put_real_spat(std::ofstream& f, const SPHData& x) {
+    const auto v = x.spat_to_host();
+    f.write(reinterpret_cast<const char*>(v.data()), (std::streamsize)(v.size() * sizeof(double)));
+}
 
 int main(int argc, char** argv) {
     if (argc < 4) return 1;
@@ -52,6 +56,23 @@ int main(int argc, char** argv) {
         put_spec(out, Op::robert_vort(x, y));                                       // 9
         put_spat(out, Op::robert_div(x, y));                                        // 10 grid
         put_spat(out, Op::diff_lat_mu(x));                                          // 11 grid
+        // real <-> complex through the grid (SPHDataComplex.hpp:93-175)
+        SPHData re(&cfg), im(&cfg);
+        x.spat_RealToSPHData(re);
+        x.spat_ImagToSPHData(im);
+        put_real_spat(out, re);                                                     // 12 real grid
+        put_real_spat(out, im);                                                     // 13 real grid
+        SPHDataComplex z(&cfg);
+        z = re;
+        put_spec(out, z);                                                           // 14
+        SPHDataComplex w(&cfg);
+        w.spat_fromSPHData(im);
+        put_spat(out, w);                                                           // 15 grid
+        SPHData q = re;
+        q.request_data_spectral();
+        q.data_spat_valid = false;  // spectral only: the conversion must synthesise
+        const SPHDataComplex c(q);
+        put_spat(out, c);                                                           // 16 grid
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 2;

@@ -62,7 +62,9 @@ def test_complex_class_operators_match_oracle(classes_cplx_bin, oracle_mod, tmp_
     """SPHDataComplex / SPHOperatorsComplex (SPHOperatorsComplex.hpp) against the
     oracle's complex operators; the compositions the oracle lacks (Helmholtz,
     robert_vort, robert_div, diff_lat_mu) against the same compositions of
-    oracle pieces."""
+    oracle pieces; the real <-> complex grid conversions (spat_RealToSPHData,
+    spat_ImagToSPHData, spat_fromSPHData, assignment from SPHData) against the
+    oracle's transforms of the parts."""
     L = 31
     g = oracle_mod.Grid(L)
     x, y = random_spec(L, 2, seed=77, cplx=True)
@@ -73,13 +75,15 @@ def test_complex_class_operators_match_oracle(classes_cplx_bin, oracle_mod, tmp_
     assert r.returncode == 0, r.stderr
     nphi, nlat, ncplx = map(int, r.stdout.split()[:3])
     assert (nphi, nlat, ncplx) == (g.nphi, g.nlat, g.ncplx)
-    kinds = "cccccgggccgg"
-    raw = np.fromfile(outp, np.complex128)
+    kinds = "cccccgggccggrrcgg"
+    raw = np.fromfile(outp, np.uint8)
     blocks, off = [], 0
     for k in kinds:
         n = ncplx if k == "c" else nphi * nlat
-        blocks.append(raw[off:off + n] if k == "c" else raw[off:off + n].reshape(nphi, nlat))
-        off += n
+        dt = np.float64 if k == "r" else np.complex128
+        v = raw[off:off + n * np.dtype(dt).itemsize].view(dt)
+        blocks.append(v if k == "c" else v.reshape(nphi, nlat))
+        off += n * np.dtype(dt).itemsize
     assert off == raw.size
     op = lambda name, v: g.cplx_op(name, v, kind="spec")[1]
     for i, name in enumerate(["diff_lon", "d1mu2", "mu", "mu2", "laplace", "grad_lon", "grad_lat", "div_lat"]):
@@ -91,6 +95,18 @@ def test_complex_class_operators_match_oracle(classes_cplx_bin, oracle_mod, tmp_
     c2 = g.cosphi[None, :] ** 2
     assert rel_l2(blocks[10], g.cplx_SH_to_spat(op("diff_lon", x) + op("d1mu2", y)) / c2) < 1e-12
     assert rel_l2(blocks[11], g.cplx_SH_to_spat(op("d1mu2", x)) / c2) < 1e-12
+    # real <-> complex through the grid: spat_RealToSPHData / spat_ImagToSPHData
+    # copy the parts of the synthesised grid exactly, operator= and
+    # spat_fromSPHData build (part, 0), and a spectral-only real field is
+    # synthesised first
+    gx = g.cplx_SH_to_spat(x)
+    assert rel_l2(blocks[12], gx.real) < 1e-12
+    assert rel_l2(blocks[13], gx.imag) < 1e-12
+    assert rel_l2(blocks[14], g.cplx_spat_to_SH(gx.real.astype(complex))) < 1e-12
+    assert np.array_equal(blocks[15].imag, np.zeros_like(blocks[13]))
+    assert np.array_equal(blocks[15].real, blocks[13])
+    assert np.array_equal(blocks[16].imag, np.zeros_like(blocks[12]))
+    assert rel_l2(blocks[16].real, g.SH_to_spat(g.spat_to_SH(gx.real))) < 1e-12
 
 
 def test_per_pole_rexi_class_matches_oracle(gpu, oracle_mod, tmp_path):

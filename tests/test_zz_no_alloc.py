@@ -22,6 +22,34 @@ def _noalloc(s, spec, out):
                                              batch, stream)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_noalloc_first_calls_reserve_no_device_memory(gpu, precision):
+    """On a fresh handle the no-allocation entry point runs before any
+    allocating call, and the device's free memory is the same before and
+    after two calls: neither the handle's workspace nor the library's scratch
+    array is reserved by the entry point (the scratch is reserved when the
+    handle is created)."""
+    from sph_swe_b200 import capi
+    from sph_swe_b200.sph import Sph
+    from tests.helpers import random_spec, rel_l2
+
+    L, batch = 127, 3
+    s = Sph(L, precision=precision)
+    specs = [torch.from_numpy(random_spec(L, batch, seed=700 + k)).cuda() for k in range(2)]
+    outs = [torch.full((batch, s.nphi, s.nlat), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for spec, out in zip(specs, outs):
+        assert _noalloc(s, spec, out) == capi.SPH_OK, capi.last_error()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0, f"the no-allocation calls changed free device memory by {free0 - free1} bytes"
+    tol = 1e-12 if precision == 0 else 1e-6
+    for spec, out in zip(specs, outs):
+        ref = s.SH_to_spat(spec).cpu().numpy()
+        assert rel_l2(out.cpu().numpy(), ref) < tol
+
+
 @pytest.mark.parametrize("L,batch", [(63, 7), (255, 5)])
 def test_noalloc_synthesis_matches_allocating_entry_point(gpu, L, batch):
     from sph_swe_b200 import capi
