@@ -666,11 +666,15 @@ def cpu_baseline(min_seconds=12.0, max_steps=40):
                       f"T255) through the oracle (C++/OpenMP FP64), {dt:.1f} s"}
 
 
-def profile_case():
+def profile_case(which="all"):
     """One small instance of each workload, for ncu captures of every kernel
     family (no timing): transforms of 64 scalar fields at T255 in both forms,
     one nonlinear RK4 step at T255 (advective and vorticity-divergence forms),
-    one REXI step at T127 (M = 64) and one spectral operator pass."""
+    one REXI step at T127 (M = 64) and one spectral operator pass.  which:
+    "all", or one workload alone: "mixed64" (two inverse + forward transforms
+    of the 64 scalar T255 fields in the mixed form), "rexi" (two REXI steps at
+    T127, M = 64, FP64 with stored factors, Robert form), "rexi_s0" (the same
+    in the non-Robert form)."""
     import torch
 
     from sph_swe_b200 import build as b
@@ -679,6 +683,25 @@ def profile_case():
     from sph_swe_b200.sph import Sph, rexi_coefficients
 
     dev = torch.device("cuda", 0)
+    if which == "mixed64":
+        s = Sph(L_CFG1, precision=capi.SPH_PREC_MIXED)
+        spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1)).to(dev)
+        for _ in range(2):
+            s.spat_to_SH(s.SH_to_spat(spec))
+        capi.check(capi.lib().sph_sync(s.h, None))
+        s.close()
+        print(json.dumps({"profile_case": which}))
+        return
+    if which in ("rexi", "rexi_s0"):
+        s = Sph(127)
+        a, br, _ = rexi_coefficients(0.2, 64, False)
+        rx = s.rexi(a, br, radius=6.371e6, tau=3600.0, robert=1 if which == "rexi" else 0)
+        rx.step(_bump_state(s, dev), 2)
+        torch.cuda.synchronize()
+        rx.close()
+        s.close()
+        print(json.dumps({"profile_case": which}))
+        return
     for prec in (capi.SPH_PREC_FP64, capi.SPH_PREC_MIXED):
         s = Sph(L_CFG1, precision=prec)
         spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1)).to(dev)
@@ -779,10 +802,11 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the RK4 side measurements")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel (default: the committed capture)")
-    ap.add_argument("--profile-case", action="store_true", help="run one small instance of each workload (for ncu)")
+    ap.add_argument("--profile-case", nargs="?", const="all", default=None,
+                    help="run one small instance of each workload (for ncu); optionally one of mixed64, rexi, rexi_s0")
     args = ap.parse_args()
     if args.profile_case:
-        profile_case()
+        profile_case(args.profile_case)
         return
     args.warmup = max(3, args.warmup)
 

@@ -258,7 +258,11 @@ typedef struct sph_rexi_params {
 
 /* Prepare a REXI integrator for npoles poles alpha[k], beta[k] (host arrays of
  * interleaved complex).  Replaces the per-pole SWERexiSPH[Robert]::setup loop
- * (AppSWE.hpp:381-412, SWERexiSPHRobert.hpp:68-132).  With SPH_PREC_FP64 and
+ * (AppSWE.hpp:381-412, SWERexiSPH.hpp:68-130, SWERexiSPHRobert.hpp:68-132).
+ * p->robert = 0 selects the non-Robert form (state [h | u | v]); it keeps, per
+ * pole, phi and the spectra of its two grid-valued gradients plus their
+ * Fourier buffer (about 16 * npoles * ((L+1)^2 * 3 + 2 (2L+1) nlat) bytes:
+ * 1.1 GB at T127 with 535 poles).  With SPH_PREC_FP64 and
  * the Coriolis term, every banded system (pole x m x parity) is factored here
  * once and its factors are kept on the device (178 bytes per block row and
  * pole: 1.6 GB at T127 with 535 poles) if they fit in half the free device
@@ -280,9 +284,11 @@ int sph_rexi_coefficients(double h, int M, int half, int cap, double* alpha, dou
                           int* npoles);
 
 /* nsteps REXI steps in place on state = [h | u | v] (3*nlm complex): all poles
- * x all m x both l-parities are solved in one launch per step; replaces the
- * serial pole loop of AppSWE::run (AppSWE.hpp:414-566) with
- * SWERexiSPH[Robert]::solve (SWERexiSPHRobert.hpp:139-258) and
+ * x all m x both l-parities are solved in one launch per step (the non-Robert
+ * form: one launch for phi, one batched transform pair for its gradients, one
+ * launch for the velocities); replaces the serial pole loop of AppSWE::run
+ * (AppSWE.hpp:414-566) with SWERexiSPH[Robert]::solve (SWERexiSPH.hpp:137-244,
+ * SWERexiSPHRobert.hpp:139-258) and
  * SPHSolverComplex::solve -> zgbsv (SPHSolverComplex.hpp:462-511,
  * BandedMatrixSolver.hpp:416-427). */
 int sph_rexi_step(sph_rexi* r, double* state, int nsteps, void* stream);

@@ -969,21 +969,26 @@ class SWERK4 {
 // REXI time stepping of AppSWE::run (AppSWE.hpp:337-568) with the Robert
 // formulation: the serial pole loop over SWERexiSPHRobert::setup/solve
 // (SWERexiSPHRobert.hpp:68-258) is one sph_rexi_step over all poles.
-class SWERexiRobert : public SWERK4 {
+// All poles of a REXI step in one launch per step: the pole loop of
+// AppSWE::run (AppSWE.hpp:368-566) over SWERexiSPH (robert = false,
+// SWERexiSPH.hpp) or SWERexiSPHRobert (robert = true, SWERexiSPHRobert.hpp);
+// the state is (h, u, v), with the Robert velocities u cos(phi), v cos(phi) in
+// the Robert form.
+class SWERexi : public SWERK4 {
   public:
-    SWERexiRobert(SPHConfig* cfg, const SWEParameters& p, const REXI& rexi, double tau, bool fix_z5robert = false,
-                  int precision = SPH_PREC_FP64)
+    SWERexi(SPHConfig* cfg, const SWEParameters& p, const REXI& rexi, double tau, bool robert,
+            bool fix_z5robert = false, int precision = SPH_PREC_FP64)
         : SWERK4(cfg, p) {
-        sph_rexi_params rp = {p.earth_radius, p.gravitation, p.coriolis_omega, p.h0, p.viscosity2, tau,
-                              1, p.coriolis_omega != 0.0 ? 1 : 0, fix_z5robert ? 1 : 0, precision};
+        sph_rexi_params rp = {p.earth_radius, p.gravitation,          p.coriolis_omega, p.h0, p.viscosity2, tau,
+                              robert ? 1 : 0, p.coriolis_omega != 0.0 ? 1 : 0, fix_z5robert ? 1 : 0, precision};
         check(sph_rexi_create(cfg->handle(), reinterpret_cast<const double*>(rexi.alpha.data()),
                               reinterpret_cast<const double*>(rexi.beta_re.data()), (int)rexi.alpha.size(), &rp, &r_),
               "sph_rexi_create");
     }
-    ~SWERexiRobert() {
+    ~SWERexi() {
         if (r_) sph_rexi_destroy(r_);
     }
-    // advance (h, U, V) by nsteps steps of tau
+    // advance (h, u, v) by nsteps steps of tau
     void run(SPHData& h, SPHData& u, SPHData& v, int nsteps) {
         pack(h, u, v);
         check(sph_rexi_step(r_, reinterpret_cast<double*>(state_), nsteps, cfg_->s()), "sph_rexi_step");
@@ -993,26 +998,35 @@ class SWERexiRobert : public SWERK4 {
   private:
     sph_rexi* r_ = nullptr;
 };
-
-// One pole of the REXI sum, SWERexiSPHRobert (SWERexiSPHRobert.hpp:68-258):
-// setup takes the pole alpha, weight beta (both divided by the time step
-// here, as there) and the physical constants; solve returns this pole's
-// Re(I(beta x)) for the geopotential phi0 and the Robert velocities u0, v0,
-// which the caller sums over the poles as AppSWE::run does.  Each object is a
-// one-pole plan of sph_rexi that factors its banded systems in every solve
-// (sph_rexi_params.factor_each_step).  SWERexiRobert runs all poles of a step
-// in one launch instead.
-class SWERexiSPHRobert {
+class SWERexiRobert : public SWERexi {
   public:
-    SWERexiSPHRobert() = default;
-    SWERexiSPHRobert(const SWERexiSPHRobert&) = delete;
-    SWERexiSPHRobert& operator=(const SWERexiSPHRobert&) = delete;
-    SWERexiSPHRobert(SWERexiSPHRobert&& o) noexcept { swap(o); }
-    SWERexiSPHRobert& operator=(SWERexiSPHRobert&& o) noexcept {
+    SWERexiRobert(SPHConfig* cfg, const SWEParameters& p, const REXI& rexi, double tau, bool fix_z5robert = false,
+                  int precision = SPH_PREC_FP64)
+        : SWERexi(cfg, p, rexi, tau, true, fix_z5robert, precision) {}
+};
+
+// One pole of the REXI sum: SWERexiSPH (SWERexiSPH.hpp:68-244) and
+// SWERexiSPHRobert (SWERexiSPHRobert.hpp:68-258) share this body.  setup takes
+// the pole alpha, weight beta (both divided by the time step here, as there)
+// and the physical constants; solve returns this pole's Re(I(beta x)) for the
+// geopotential phi0 and the velocities u0, v0 (the Robert velocities
+// u cos(phi), v cos(phi) in the Robert form), which the caller sums over the
+// poles as AppSWE::run does.  Each object is a one-pole plan of sph_rexi that
+// factors its banded systems in every solve
+// (sph_rexi_params.factor_each_step); SWERexi runs all poles of a step in one
+// launch instead.
+class SWERexiSPHPole {
+  public:
+    explicit SWERexiSPHPole(bool robert) : robert_(robert) {}
+    SWERexiSPHPole(const SWERexiSPHPole&) = delete;
+    SWERexiSPHPole& operator=(const SWERexiSPHPole&) = delete;
+    SWERexiSPHPole(SWERexiSPHPole&& o) noexcept : robert_(o.robert_) { swap(o); }
+    SWERexiSPHPole& operator=(SWERexiSPHPole&& o) noexcept {
+        std::swap(robert_, o.robert_);
         swap(o);
         return *this;
     }
-    ~SWERexiSPHRobert() { release(); }
+    ~SWERexiSPHPole() { release(); }
 
     void setup(SPHConfig* cfg, const cplx& alpha, const cplx& beta, double radius, double coriolis_omega,
                double avg_geopotential, double timestep_size, bool include_coriolis_effect = true) {
@@ -1025,7 +1039,7 @@ class SWERexiSPHRobert {
         rp.h0 = avg_geopotential;
         rp.viscosity = 0.0;  // AppSWE applies viscosity after the pole sum
         rp.tau = timestep_size;
-        rp.robert = 1;
+        rp.robert = robert_ ? 1 : 0;
         rp.coriolis = include_coriolis_effect ? 1 : 0;
         rp.fix_z5robert = 0;
         rp.precision = SPH_PREC_FP64;
@@ -1037,7 +1051,7 @@ class SWERexiSPHRobert {
 
     void solve(const SPHData& phi0, const SPHData& u0, const SPHData& v0, SPHData& o_phi, SPHData& o_u,
                SPHData& o_v) {
-        if (!r_) throw std::runtime_error("SWERexiSPHRobert: solve before setup");
+        if (!r_) throw std::runtime_error("SWERexiSPH: solve before setup");
         const size_t n = (size_t)cfg_->spec_num_elems;
         const SPHData* in[3] = {&phi0, &u0, &v0};
         for (int k = 0; k < 3; k++) {
@@ -1063,10 +1077,11 @@ class SWERexiSPHRobert {
     }
 
   private:
+    bool robert_;
     SPHConfig* cfg_ = nullptr;
     sph_rexi* r_ = nullptr;
     cplx* state_ = nullptr;
-    void swap(SWERexiSPHRobert& o) noexcept {
+    void swap(SWERexiSPHPole& o) noexcept {
         std::swap(cfg_, o.cfg_);
         std::swap(r_, o.r_);
         std::swap(state_, o.state_);
@@ -1077,6 +1092,17 @@ class SWERexiSPHRobert {
         r_ = nullptr;
         state_ = nullptr;
     }
+};
+
+// SWERexiSPH: the non-Robert form (velocities u, v; SWERexiSPH.hpp)
+class SWERexiSPH : public SWERexiSPHPole {
+  public:
+    SWERexiSPH() : SWERexiSPHPole(false) {}
+};
+// SWERexiSPHRobert: the Robert form (velocities u cos(phi), v cos(phi); SWERexiSPHRobert.hpp)
+class SWERexiSPHRobert : public SWERexiSPHPole {
+  public:
+    SWERexiSPHRobert() : SWERexiSPHPole(true) {}
 };
 
 }  // namespace sph_swe

@@ -330,7 +330,6 @@ int main(int argc, char** argv) {
         const auto t0 = std::chrono::steady_clock::now();
         long long done = 0;
         if (v.use_rexi) {
-            if (!v.robert) throw std::runtime_error("REXI needs the Robert formulation (S1)");
             if (v.nonlinear) throw std::runtime_error("REXI integrates the linear equations (N0)");
             REXI rexi;
             rexi.setup(v.rexi_h, v.rexi_M, 0, v.half_poles);
@@ -342,7 +341,8 @@ int main(int argc, char** argv) {
                 cfg_ext.setupAdditionalModes(&cfg, v.rexi_ext, v.rexi_ext, v.precision);
                 std::printf(" + REXI additional modes: %d (T%d on %d x %d)\n", v.rexi_ext, cfg_ext.spec_n_max,
                             cfg_ext.spat_num_lat, cfg_ext.spat_num_lon);
-                SWERexiRobert stepper(&cfg_ext, p, rexi, v.dt, false, v.precision);
+                // SWERexiSPH (S0) or SWERexiSPHRobert (S1) for every pole (AppSWE.hpp:368-414)
+                SWERexi stepper(&cfg_ext, p, rexi, v.dt, v.robert != 0, false, v.precision);
                 SPHData he(&cfg_ext), ue(&cfg_ext), we(&cfg_ext);
                 while (done < nsteps) {
                     const long long k = steps_to_output(done);
@@ -358,7 +358,7 @@ int main(int argc, char** argv) {
                     done += k;
                 }
             } else {
-                SWERexiRobert stepper(&cfg, p, rexi, v.dt, false, v.precision);
+                SWERexi stepper(&cfg, p, rexi, v.dt, v.robert != 0, false, v.precision);
                 while (done < nsteps) {
                     const long long k = steps_to_output(done);
                     stepper.run(h, u, w, (int)k);

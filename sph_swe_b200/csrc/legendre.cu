@@ -463,6 +463,9 @@ int legendre_kernels_init() {
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_w));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_w));
+    // the wide analysis needs its shared-memory opt-in on this device before any
+    // launch, also before launches inside a stream capture
+    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_w, cudaFuncAttributeMaxDynamicSharedMemorySize, WSMEM_ANA));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_zero_top));
     return SPH_OK;
 }

@@ -93,6 +93,17 @@ struct MixedTables {
     // B operand prepared by the loader-only kernel (legendre_tcb.cuh)
     float* Bbuf = nullptr;
     size_t Bcap = 0;
+    // int8 digit tables of the integer-split kernels (legendre_i8.cuh)
+    unsigned char* SY = nullptr;  // synthesis digit planes
+    unsigned char* AN = nullptr;  // analysis digit planes
+    int* esy = nullptr;           // synthesis row exponents [m][j]
+    int* ean = nullptr;           // analysis row exponents [pidx(lmax, l, m)]
+    long long* i8zoff = nullptr;  // [m] first z of order m in SY
+    long long* i8aoff = nullptr;  // [m] first row of order m in AN
+    long long zSY = 0, rowsAN = 0;
+    int zAN = 0;
+    bool i8 = false;
+    CUtensorMap mapSY, mapAN;
 };
 
 // Offsets of degree m's blocks in the coefficient and checkpoint tables of
@@ -366,7 +377,9 @@ __global__ void k_tc_ck(int nh, int nhp, int lmax, int mm, const double* __restr
 }
 
 static int tcs_tables_build(Handle* h, MixedTables* T);
+static int i8_tables_build(Handle* h, MixedTables* T);
 static bool g_tc_stream = true;
+static bool g_tc_i8 = true;
 
 int tc_tables_build(Handle* h, int lmax) {
     if (h->mixed) return SPH_OK;
@@ -389,6 +402,8 @@ int tc_tables_build(Handle* h, int lmax) {
     SPH_CUDA_TRY(cudaGetLastError());
     if (g_tc_stream)
         if (int rc = tcs_tables_build(h, T)) return rc;
+    if (g_tc_i8)
+        if (int rc = i8_tables_build(h, T)) return rc;
     SPH_CUDA_TRY(cudaDeviceSynchronize());
     return SPH_OK;
 }
@@ -396,7 +411,8 @@ int tc_tables_build(Handle* h, int lmax) {
 void tc_tables_free(Handle* h) {
     MixedTables* T = static_cast<MixedTables*>(h->mixed);
     if (!T) return;
-    void* bufs[] = {T->ab, T->ck, T->ckx, T->flag, T->S, T->A, T->soff, T->aoff, T->Bbuf};
+    void* bufs[] = {T->ab, T->ck,   T->ckx, T->flag,   T->S,      T->A,     T->soff,
+                    T->aoff, T->Bbuf, T->SY, T->AN, T->esy, T->ean, T->i8zoff, T->i8aoff};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete T;
@@ -1041,6 +1057,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
 
 #include "legendre_tcs.cuh"
 #include "legendre_tcb.cuh"
+#include "legendre_i8.cuh"
 
 // rows: padded row count (a multiple of 64), slices: z extent
 static int encode_map(CUtensorMap* map, float* base, unsigned long long rows, unsigned long long slices) {
@@ -1099,6 +1116,81 @@ static int tcs_tables_build(Handle* h, MixedTables* T) {
     return SPH_OK;
 }
 
+// tensor map of an int8 digit table seen as 32-bit words: dims (64 rows x 16 B,
+// row blocks, z, 4 digit planes), box {256, 2, 2, 4} = 128 rows x 32 K x 4 planes
+static int encode_map_i8(CUtensorMap* map, unsigned char* base, unsigned long long rows, unsigned long long zext) {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* f = nullptr;
+        SPH_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+        if (!f || q != cudaDriverEntryPointSuccess) {
+            set_error("cuTensorMapEncodeTiled is not available");
+            return SPH_ERR_CUDA;
+        }
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    const cuuint64_t dims[4] = {256, rows / 64, zext, 4};
+    const cuuint64_t strides[3] = {1024, 16ull * rows, 16ull * rows * zext};
+    const cuuint32_t box[4] = {256, 2, 2, 4};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (int8 tables) failed (" + std::to_string((int)r) + ")");
+        return SPH_ERR_CUDA;
+    }
+    return SPH_OK;
+}
+
+static int i8_tables_build(Handle* h, MixedTables* T) {
+    const int tl = T->lmax, nh = h->nh, mm = std::min(tl, h->L);
+    const int nhP = tcs_pad64(nh);
+    std::vector<long long> zo(mm + 2, 0), ao(mm + 2, 0);
+    for (int m = 0; m <= mm; m++) {
+        zo[m + 1] = zo[m] + 4LL * i8_nch(tl, m);
+        ao[m + 1] = ao[m] + tcs_pad64(i8_nlp(tl, m, 0)) + tcs_pad64(i8_nlp(tl, m, 1));
+    }
+    T->zSY = zo[mm + 1];
+    T->rowsAN = ao[mm + 1];
+    T->zAN = 2 * ((nh + li8::KC - 1) / li8::KC);
+    const long long nlmT = (long long)(tl + 1) * (tl + 2) / 2;
+    const size_t bs = (size_t)4 * T->zSY * nhP * 16, ba = (size_t)4 * T->zAN * T->rowsAN * 16;
+    SPH_CUDA_TRY(cudaMalloc(&T->SY, bs));
+    SPH_CUDA_TRY(cudaMalloc(&T->AN, ba));
+    SPH_CUDA_TRY(cudaMemset(T->SY, 0, bs));
+    SPH_CUDA_TRY(cudaMemset(T->AN, 0, ba));
+    SPH_CUDA_TRY(cudaMalloc(&T->esy, sizeof(int) * (size_t)(mm + 1) * nh));
+    SPH_CUDA_TRY(cudaMalloc(&T->ean, sizeof(int) * (size_t)nlmT));
+    SPH_CUDA_TRY(cudaMemset(T->ean, 0, sizeof(int) * (size_t)nlmT));
+    SPH_CUDA_TRY(cudaMalloc(&T->i8zoff, sizeof(long long) * (mm + 2)));
+    SPH_CUDA_TRY(cudaMalloc(&T->i8aoff, sizeof(long long) * (mm + 2)));
+    SPH_CUDA_TRY(cudaMemcpy(T->i8zoff, zo.data(), sizeof(long long) * (mm + 2), cudaMemcpyHostToDevice));
+    SPH_CUDA_TRY(cudaMemcpy(T->i8aoff, ao.data(), sizeof(long long) * (mm + 2), cudaMemcpyHostToDevice));
+    unsigned long long* amax = nullptr;
+    SPH_CUDA_TRY(cudaMalloc(&amax, sizeof(unsigned long long) * (size_t)nlmT));
+    cudaError_t e = cudaMemset(amax, 0, sizeof(unsigned long long) * (size_t)nlmT);
+    const dim3 grid((nh + 127) / 128, mm + 1);
+    if (e == cudaSuccess) {
+        k_i8_rowmax<<<grid, 128>>>(nh, tl, mm, h->mu, h->w, T->esy, amax);
+        k_i8_anexp<<<(unsigned)((nlmT + 255) / 256), 256>>>(nlmT, amax, T->ean);
+        k_i8_tables<<<grid, 128>>>(nh, nhP, tl, mm, h->mu, h->w, T->esy, T->ean, T->i8zoff, T->i8aoff, T->zSY,
+                                   T->rowsAN, T->zAN, T->SY, T->AN);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    cudaFree(amax);
+    if (e != cudaSuccess) {
+        set_error(std::string("int8 Legendre tables: ") + cudaGetErrorString(e));
+        return SPH_ERR_CUDA;
+    }
+    if (int rc = encode_map_i8(&T->mapSY, T->SY, (unsigned long long)nhP, (unsigned long long)T->zSY)) return rc;
+    if (int rc = encode_map_i8(&T->mapAN, T->AN, (unsigned long long)T->rowsAN, (unsigned long long)T->zAN)) return rc;
+    T->i8 = true;
+    return SPH_OK;
+}
+
 template <int NC>
 static int tc_attr() {
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tcb<SynB<NC>, NC>,
@@ -1114,6 +1206,10 @@ static int tc_attr() {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_tc<AnaDir<NC>, NC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8<SynI8<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8::BYTES));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8<AnaI8<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8::BYTES));
     return SPH_OK;
 }
 
@@ -1129,6 +1225,8 @@ int tc_kernels_init() {
     // P_l^m operand: streamed from split-TF32 tables by TMA (default) or
     // regenerated from recurrence checkpoints (SPH_TC_STREAM=0)
     if (const char* e = getenv("SPH_TC_STREAM")) g_tc_stream = atoi(e) != 0;
+    // int8 integer-split kernels (default) or only the split-TF32 ones (SPH_TC_I8=0)
+    if (const char* e = getenv("SPH_TC_I8")) g_tc_i8 = atoi(e) != 0;
     if (int rc = tc_attr<16>()) return rc;
     if (int rc = tc_attr<32>()) return rc;
     return tc_attr<64>();
@@ -1329,6 +1427,56 @@ static int tcb_launch(const Handle* h, const MixedTables* Tc, bool syn, int lmax
     return tcb_launch_nc<64>(h, T, syn, a, in, ld_in, out, s);
 }
 
+// Variants of the tensor-core Legendre stages (the autotuner's numbers):
+//   bits 0-1  column tile: 0 the built-in rule, 1: 16, 2: 32, 3: 64 real columns
+//   none of 4, 8, 16, 32   int8 integer-split kernels (legendre_i8.cuh),
+//             bit 64: m order paired with its complement instead of ascending
+//   32        split-TF32, P streamed by TMA, B staged by producer warps
+//   8         split-TF32, both operands by TMA (B prepared once per call)
+//   4         split-TF32, P regenerated from recurrence checkpoints
+//   16        the FP64 CUDA-core kernel (legendre.cu)
+static bool use_i8(const MixedTables* T, int var) { return T->i8 && !(var & (4 | 8 | 16 | 32)); }
+
+// columns per CTA of the int8 kernels: 16 (8 fields) for small batches, else 32
+static int i8_cols_v(int batch, int var) {
+    const int c = var & 3;
+    return c == 0 ? (batch <= 8 ? 16 : 32) : (8 << c);
+}
+
+static I8Args make_i8args(const Handle* h, const MixedTables* T, bool syn, int lmax, int batch, long long ld_spec,
+                          long long ldF, int var) {
+    I8Args a;
+    a.erow = syn ? T->esy : T->ean;
+    a.zoff = T->i8zoff;
+    a.aoff = T->i8aoff;
+    a.tlmax = T->lmax;
+    a.lmax = lmax;
+    a.nh = h->nh;
+    a.nlat = h->nlat;
+    a.batch = batch;
+    a.nm = std::min(lmax, h->L) + 1;
+    a.order = (var & 64) ? 1 : 0;
+    a.ld_spec = ld_spec;
+    a.ldF = ldF;
+    a.flag = T->flag;
+    a.nct = a.nrt = a.ntiles = 0;
+    return a;
+}
+
+template <template <int> class Dir>
+static int i8_launch(const CUtensorMap& map, I8Args& a, int nrt, const double2* in, double2* out, int nc,
+                     cudaStream_t s) {
+    a.nct = (2 * a.batch + nc - 1) / nc;
+    a.nrt = nrt;
+    a.ntiles = a.nct * nrt * a.nm;
+    const int grid = std::max(1, std::min(a.ntiles, g_tc_sms > 0 ? g_tc_sms : 148));
+    if (nc == 16) k_legendre_i8<Dir<16>, 16><<<grid, li8::NT, li8::BYTES, s>>>(map, a, in, out);
+    else if (nc == 32) k_legendre_i8<Dir<32>, 32><<<grid, li8::NT, li8::BYTES, s>>>(map, a, in, out);
+    else k_legendre_i8<Dir<64>, 64><<<grid, li8::NT, li8::BYTES, s>>>(map, a, in, out);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
 int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F, long long ldF,
                           int batch, cudaStream_t s) {
     const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
@@ -1336,6 +1484,10 @@ int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spe
     if (batch <= 0) return SPH_OK;
     const int nrt = (h->nh + tc::M - 1) / tc::M, nm = std::min(lmax, h->L) + 1;
     const int var = tune_get(h, TUNE_TC_SYNTHESIS, batch, 0);
+    if (use_i8(T, var)) {
+        I8Args a = make_i8args(h, T, true, lmax, batch, ld_spec, ldF, var);
+        return i8_launch<SynI8>(T->mapSY, a, (h->nh + li8::M - 1) / li8::M, spec, F, i8_cols_v(batch, var), s);
+    }
     if (T->streamed && !(var & 4) && (var & 8))
         return tcb_launch(h, T, true, lmax, batch, nrt, nm, spec, ld_spec, F, ldF, var, s);
     if (T->streamed && !(var & 4)) {
@@ -1353,6 +1505,11 @@ int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, doubl
     if (batch <= 0) return SPH_OK;
     const int nrt = lmax / (2 * tc::M) + 1, nm = std::min(lmax, h->L) + 1;
     const int var = tune_get(h, TUNE_TC_ANALYSIS, batch, 0);
+    if (use_i8(T, var)) {
+        I8Args a = make_i8args(h, T, false, lmax, batch, ld_spec, ldF, var);
+        return i8_launch<AnaI8>(T->mapAN, a, (i8_nlp(lmax, 0, 0) + li8::M - 1) / li8::M, F, spec,
+                                i8_cols_v(batch, var), s);
+    }
     if (T->streamed && !(var & 4) && (var & 8))
         return tcb_launch(h, T, false, lmax, batch, nrt, nm, F, ldF, spec, ld_spec, var, s);
     if (T->streamed && !(var & 4)) {

@@ -64,6 +64,13 @@ struct RexiPlan {
     signed char* pvel = nullptr;
     long long plane = 0;
     bool singular = false;      // a zero pivot met while factoring
+    // non-Robert form (SWERexiSPH): per-pole phi and the spectra of its
+    // grid-valued gradients, their Fourier buffer, real-layout prep buffers
+    double2* PH = nullptr;      // [npoles][ncplx] phi (complex layout n*n+n+m)
+    double2* XY = nullptr;      // [2][npoles][ncplx]: i m phi and D phi, then F(grad_lon phi), F(grad_lat phi)
+    double2* FXY = nullptr;     // [2 npoles][2L+1][nlat]
+    double2* Xs = nullptr;      // [8][nlm] real-layout spectra of the prep
+    double2* Fs = nullptr;      // [4][L+1][nlat] Fourier buffers of the prep
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double* state = nullptr;
@@ -125,6 +132,126 @@ __global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
             outp[(size_t)2 * nc + row] = v2;
         }
     }
+}
+
+// ------------------------------------------------------------ non-Robert form (SWERexiSPH)
+// Phase A: phi of every pole and m-block, written in the complex layout with
+// i m phi and the truncated (1-mu^2) d phi/dmu, whose syntheses divided by
+// cos phi are grad_lon(phi) and grad_lat(phi) (SPHOperatorsComplex.hpp:99-114,
+// 223-249).
+template <int MAXN, bool MIXED, bool STORED>
+__global__ void __launch_bounds__(64) k_rexi_s0_phi(RexiDev d, double2* __restrict__ PH, double2* __restrict__ XY) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int L = d.L;
+    if (warp >= (2 * L + 1) * d.ngroups) return;
+    const int g = warp % d.ngroups, kk = warp / d.ngroups;
+    const int m = (kk & 1) ? -((kk + 1) >> 1) : (kk >> 1);
+    const int am = m < 0 ? -m : m;
+    const int N = L + 1 - am;
+    const int base = block_off(L, m);
+    const int nc = d.ncplx;
+    const int pole = g * 32 + lane;
+    const bool valid = pole < d.npoles;
+    const double2 a = d.alpha[valid ? pole : 0];
+    double2 phi[MAXN];
+    const long long gl = (long long)g * nc * 32 + lane;
+    const bool ok = rexi_phi<MAXN, MIXED, STORED>(d, m, a, phi, gl);
+    if (!ok && valid) atomicOr(d.flag, 2);
+    if (!valid) return;
+    double2* ph = PH + (size_t)pole * nc;
+    double2* x = XY + (size_t)pole * nc;
+    double2* y = XY + ((size_t)d.npoles + pole) * nc;
+    for (int i = 0; i < N; i++) {
+        const int n = am + i, ci = n * n + n + m;
+        const double* cf = d.coef + (size_t)(base + i) * 4;
+        const double2 lo = i > 0 ? phi[i - 1] : make_double2(0, 0);
+        const double2 hi = i + 1 < N ? phi[i + 1] : make_double2(0, 0);
+        ph[ci] = phi[i];
+        x[ci] = c_im(phi[i], (double)m);
+        y[ci] = c_add(c_scale(lo, __ldg(cf + 2)), c_scale(hi, __ldg(cf + 3)));
+    }
+}
+
+// Phase B: velocity of every pole and m-block from the gradients' spectra,
+// then beta scaling and the reduction over the 32 poles of the warp (as
+// k_rexi_solve).
+template <int MAXN, bool MIXED, bool STORED>
+__global__ void __launch_bounds__(64) k_rexi_s0_vel(RexiDev d, const double2* __restrict__ PH,
+                                                   const double2* __restrict__ XY) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int L = d.L;
+    if (warp >= (2 * L + 1) * d.ngroups) return;
+    const int g = warp % d.ngroups, kk = warp / d.ngroups;
+    const int m = (kk & 1) ? -((kk + 1) >> 1) : (kk >> 1);
+    const int am = m < 0 ? -m : m;
+    const int N = L + 1 - am;
+    const int base = block_off(L, m);
+    const int nc = d.ncplx;
+    const int pole = g * 32 + lane;
+    const bool valid = pole < d.npoles;
+    const int pc = valid ? pole : 0;
+    const double2 a = d.alpha[pc];
+    const double2 bt = valid ? d.beta[pole] : make_double2(0, 0);
+    double2 ra[MAXN], rb[MAXN];
+    const long long gl = (long long)g * nc * 32 + lane;
+    const bool ok = rexi_s0_vel<MAXN, MIXED, STORED>(d, m, a, XY + (size_t)pc * nc, XY + ((size_t)d.npoles + pc) * nc,
+                                                    ra, rb, gl);
+    if (!ok && valid) atomicOr(d.flag, 2);
+    const double2* ph = PH + (size_t)pc * nc;
+    double2* outp = d.part + (size_t)g * 3 * nc;
+    for (int i = 0; i < N; i++) {
+        const int n = am + i;
+        double2 v0 = c_mul(bt, ph[n * n + n + m]), v1 = c_mul(bt, ra[i]), v2 = c_mul(bt, rb[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v0.x += __shfl_down_sync(0xffffffffu, v0.x, o);
+            v0.y += __shfl_down_sync(0xffffffffu, v0.y, o);
+            v1.x += __shfl_down_sync(0xffffffffu, v1.x, o);
+            v1.y += __shfl_down_sync(0xffffffffu, v1.y, o);
+            v2.x += __shfl_down_sync(0xffffffffu, v2.x, o);
+            v2.y += __shfl_down_sync(0xffffffffu, v2.y, o);
+        }
+        if (lane == 0) {
+            const int row = base + i;
+            outp[row] = v0;
+            outp[(size_t)nc + row] = v1;
+            outp[(size_t)2 * nc + row] = v2;
+        }
+    }
+}
+
+// Fourier-space factors of the non-Robert projections (per latitude j, times
+// 2 pi: synthesis -> analysis convention), c = sqrt(1 - mu^2):
+//   mode 0: x c     (the cos(phi) factor of div_lat, SPHOperatorsComplex.hpp:300-312)
+//   mode 1: x (1 - mu^2) / c   (grad_lat(mu) as a grid field, the Coriolis product)
+//   mode 2: x / c   (grad_lon, grad_lat of the per-pole phi)
+__global__ void k_s0_fscale(double2* __restrict__ F, long long n, int nlat, const double* __restrict__ mu, int mode) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const double z = mu[idx % nlat];
+    const double c2 = (1.0 - z) * (1.0 + z), c = sqrt(c2);
+    const double f = 2.0 * kPi * (mode == 0 ? c : (mode == 1 ? c2 / c : 1.0 / c));
+    F[idx] = make_double2(F[idx].x * f, F[idx].y * f);
+}
+
+// div and eta of the non-Robert operators from the Fourier coefficients of
+// F0 = I(i m u0), F1 = I(D w) with w = F(I(v0) cos phi), F2 = I(i m v0),
+// F3 = I(D u0) (four consecutive fields of stride ldF): in place, field 0
+// becomes div = div_lon(u0) + div_lat(v0) = F0/c + F1/(c cos(lat)) and field 1
+// eta = grad_lon(v0) - grad_lat(u0) = (F2 - F3)/c (SPHOperatorsComplex.hpp:
+// 99-114, 223-249, 283-335, 479-518), both times 2 pi
+__global__ void k_s0_fdiveta(double2* __restrict__ F, long long ldF, int nlat, const double* __restrict__ mu,
+                             const double* __restrict__ lat) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= ldF) return;
+    const int j = (int)(idx % nlat);
+    const double z = mu[j];
+    const double ic = 2.0 * kPi / sqrt((1.0 - z) * (1.0 + z)), icl = 1.0 / cos(lat[j]);
+    const double2 f0 = F[idx], f1 = F[ldF + idx], f2 = F[2 * ldF + idx], f3 = F[3 * ldF + idx];
+    F[idx] = make_double2((f0.x + f1.x * icl) * ic, (f0.y + f1.y * icl) * ic);
+    F[ldF + idx] = make_double2((f2.x - f3.x) * ic, (f2.y - f3.y) * ic);
 }
 
 // ------------------------------------------------------------ pole-independent prep
@@ -255,7 +382,106 @@ static RexiDev rexi_dev(const RexiPlan* R) {
     return d;
 }
 
+// MAXN template dispatch of the lane kernels over the truncation
+#define RX_DISPATCH(K, d, nb, s, ...)                                                             \
+    do {                                                                                          \
+        const int L1 = (d).L + 1;                                                                 \
+        if ((d).fphi) {                                                                           \
+            if (L1 <= 64) K<64, false, true><<<nb, 64, 0, s>>>(d, __VA_ARGS__);                   \
+            else if (L1 <= 128) K<128, false, true><<<nb, 64, 0, s>>>(d, __VA_ARGS__);            \
+            else K<256, false, true><<<nb, 64, 0, s>>>(d, __VA_ARGS__);                           \
+        } else if ((d).refine > 0) {                                                              \
+            if (L1 <= 64) K<64, true, false><<<nb, 64, 0, s>>>(d, __VA_ARGS__);                   \
+            else if (L1 <= 128) K<128, true, false><<<nb, 64, 0, s>>>(d, __VA_ARGS__);            \
+            else K<256, true, false><<<nb, 64, 0, s>>>(d, __VA_ARGS__);                           \
+        } else {                                                                                  \
+            if (L1 <= 64) K<64, false, false><<<nb, 64, 0, s>>>(d, __VA_ARGS__);                  \
+            else if (L1 <= 128) K<128, false, false><<<nb, 64, 0, s>>>(d, __VA_ARGS__);           \
+            else K<256, false, false><<<nb, 64, 0, s>>>(d, __VA_ARGS__);                          \
+        }                                                                                         \
+    } while (0)
+
+// One step of the non-Robert form (SWERexiSPH::solve for every pole,
+// SWERexiSPH.hpp:137-244, and the pole sum of AppSWE::run).  The pole-
+// independent vectors of rexi_phi come from the non-Robert operators: div0 =
+// ir div(u0, v0), eta0 = ir vort(u0, v0) through the grid divisions by cos phi
+// (done per wavenumber on the Legendre coefficients: the divisions do not mix
+// wavenumbers), and the Coriolis products grad_lat(mu) x for x = u0, mu2 u0,
+// mu v0 (full grid, as the Robert form).  Per pole the velocity needs
+// grad_lon(phi), grad_lat(phi) as spectra: one batched complex Legendre
+// synthesis of i m phi and D phi over all poles, the division by cos phi, one
+// batched analysis.
+static int rexi_s0_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
+    Handle* h = R->h;
+    const int L = h->L, nlm = h->nlm, nc = h->ncplx, nlat = h->nlat, mF = L + 1;
+    const long long ldF = (long long)mF * nlat, ldFc = (long long)(2 * L + 1) * nlat;
+    const double g = R->p.gravity, ir = 1.0 / R->p.radius;
+    const double2* hh = state;
+    const double2* uu = state + nlm;
+    const double2* vv = state + 2 * (size_t)nlm;
+    const dim3 gc((L + 1 + 63) / 64, 2 * L + 1), gr((L + 1 + 63) / 64, L + 1);
+    double2* V = R->V;
+    auto Vs = [&](int k) { return V + (size_t)k * nc; };
+    auto Xs = [&](int k) { return R->Xs + (size_t)k * nlm; };
+    const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
+    auto blocks = [](long long n) { return (unsigned)((n + 255) / 256); };
+    // w = F(I(v0) cos phi)
+    if (int rc = legendre_synthesis_real(h, vv, nlm, L, R->Fs, ldF, 1, s)) return rc;
+    k_s0_fscale<<<blocks(ldF), 256, 0, s>>>(R->Fs, ldF, nlat, h->mu, 0);
+    if (int rc = legendre_analysis_real(h, R->Fs, ldF, Xs(0), nlm, L, 1, s)) return rc;
+    // i m u0, D w, i m v0, D u0 -> div, eta
+    if (int rc = spec_op(h, SPH_OP_DIFF_LON, uu, nlm, Xs(1), nlm, one, zero, 1, 0, s)) return rc;
+    if (int rc = spec_op(h, SPH_OP_D1MU2, Xs(0), nlm, Xs(2), nlm, one, zero, 1, 0, s)) return rc;
+    if (int rc = spec_op(h, SPH_OP_DIFF_LON, vv, nlm, Xs(3), nlm, one, zero, 1, 0, s)) return rc;
+    if (int rc = spec_op(h, SPH_OP_D1MU2, uu, nlm, Xs(4), nlm, one, zero, 1, 0, s)) return rc;
+    if (int rc = legendre_synthesis_real(h, Xs(1), nlm, L, R->Fs, ldF, 4, s)) return rc;
+    k_s0_fdiveta<<<blocks(ldF), 256, 0, s>>>(R->Fs, ldF, nlat, h->mu, h->lat);
+    if (int rc = legendre_analysis_real(h, R->Fs, ldF, Xs(5), nlm, L, 2, s)) return rc;
+    // Coriolis products: G(x) = F(grad_lat(mu) I(x)) for x = u0, mu2 u0, mu v0
+    if (int rc = spec_op(h, SPH_OP_SCALE, uu, nlm, Xs(1), nlm, one, zero, 1, 0, s)) return rc;
+    if (int rc = spec_op(h, SPH_OP_MU2, uu, nlm, Xs(2), nlm, one, zero, 1, 0, s)) return rc;
+    if (int rc = spec_op(h, SPH_OP_MU, vv, nlm, Xs(3), nlm, one, zero, 1, 0, s)) return rc;
+    if (int rc = legendre_synthesis_real(h, Xs(1), nlm, L, R->Fs, ldF, 3, s)) return rc;
+    k_s0_fscale<<<blocks(3 * ldF), 256, 0, s>>>(R->Fs, 3 * ldF, nlat, h->mu, 1);
+    if (int rc = legendre_analysis_real(h, R->Fs, ldF, Xs(1), nlm, L, 3, s)) return rc;
+    // complex promotions: 0 div0 = ir div, 14 eta0 = ir vort, 2 phi0 = g h, 10 u0, 11 v0, 7-9 the products
+    k_rx_complexify<<<gc, 64, 0, s>>>(Xs(5), ir, Vs(0), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(Xs(6), ir, Vs(14), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(hh, g, Vs(2), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(uu, 1.0, Vs(10), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(vv, 1.0, Vs(11), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(Xs(1), 1.0, Vs(7), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(Xs(2), 1.0, Vs(8), L);
+    k_rx_complexify<<<gc, 64, 0, s>>>(Xs(3), 1.0, Vs(9), L);
+    // 1 mu(eta0), 3 mu2(phi0), 4 mu2(div0), 5 mu2(mu eta0), 6 mu2 mu2 phi0
+    k_rx_block_op<<<gc, 64, 0, s>>>(0, Vs(14), nullptr, Vs(1), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(2), nullptr, Vs(3), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(0), nullptr, Vs(4), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(1), nullptr, Vs(5), L, ir);
+    k_rx_block_op<<<gc, 64, 0, s>>>(1, Vs(3), nullptr, Vs(6), L, ir);
+    SPH_CUDA_TRY(cudaGetLastError());
+    // phase A: phi of all poles
+    const RexiDev d = rexi_dev(R);
+    const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
+    const unsigned nb = (unsigned)((nthreads + 63) / 64);
+    RX_DISPATCH(k_rexi_s0_phi, d, nb, s, R->PH, R->XY);
+    SPH_CUDA_TRY(cudaGetLastError());
+    // grad_lon(phi), grad_lat(phi) of every pole as spectra
+    const int nf = 2 * R->npoles;
+    if (int rc = legendre_synthesis_cplx(h, R->XY, nc, R->FXY, ldFc, nf, s)) return rc;
+    k_s0_fscale<<<blocks((long long)nf * ldFc), 256, 0, s>>>(R->FXY, (long long)nf * ldFc, nlat, h->mu, 2);
+    if (int rc = legendre_analysis_cplx(h, R->FXY, ldFc, R->XY, nc, nf, s)) return rc;
+    // phase B: velocities, beta scaling, pole reduction
+    RX_DISPATCH(k_rexi_s0_vel, d, nb, s, R->PH, R->XY);
+    SPH_CUDA_TRY(cudaGetLastError());
+    const double visc_fac = R->p.viscosity * R->p.tau / (R->p.radius * R->p.radius);
+    k_rx_finish<<<gr, 64, 0, s>>>(R->part, R->ngroups, nc, state, L, nlm, 1.0 / g, visc_fac, R->flag);
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
 static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
+    if (!R->p.robert) return rexi_s0_step_launch(R, state, s);
     Handle* h = R->h;
     const int L = h->L, nlm = h->nlm, nc = h->ncplx, nlat = h->nlat, mF = L + 1;
     const double g = R->p.gravity, ir = 1.0 / R->p.radius;
@@ -321,8 +547,8 @@ static void rexi_free(RexiPlan* R) {
     if (!R) return;
     if (R->exec) cudaGraphExecDestroy(R->exec);
     if (R->graph) cudaGraphDestroy(R->graph);
-    void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V,    R->part, R->X,
-                    R->Xr,    R->F,    R->flag, R->fphi, R->fvel, R->pphi, R->pvel};
+    void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V,  R->part, R->X,  R->Xr, R->F,
+                    R->flag,  R->fphi, R->fvel, R->pphi, R->pvel, R->PH, R->XY,   R->FXY, R->Xs, R->Fs};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete R;
@@ -342,10 +568,6 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
     Handle* h = reinterpret_cast<Handle*>(hh);
     if (!h || !alpha || !beta || npoles <= 0 || !p || !out || p->tau == 0.0 || p->radius <= 0.0) {
         set_error("sph_rexi_create: bad arguments");
-        return SPH_ERR_ARG;
-    }
-    if (!p->robert) {
-        set_error("sph_rexi_create: only the Robert formulation (SWERexiSPHRobert) runs on the GPU path");
         return SPH_ERR_ARG;
     }
     if (p->precision != SPH_PREC_FP64 && p->precision != SPH_PREC_MIXED) {
@@ -376,9 +598,15 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
     if (cor) {
         comp_z2(C2, cd(2.0 * T * T));
         comp_z3(C0, cd(T * T * T * T));
-        comp_z4robert(C1, cd(-P * T), r);
-        comp_z5robert(Cm1, cd(P * T * T * T), r, p->fix_z5robert != 0);
-        comp_z6robert(C0, cd(P * 2.0 * T * T), r);
+        if (p->robert) {  // SWERexiSPHRobert::setup (SWERexiSPHRobert.hpp:109-131)
+            comp_z4robert(C1, cd(-P * T), r);
+            comp_z5robert(Cm1, cd(P * T * T * T), r, p->fix_z5robert != 0);
+            comp_z6robert(C0, cd(P * 2.0 * T * T), r);
+        } else {          // SWERexiSPH::setup (SWERexiSPH.hpp:107-129)
+            comp_z4(C1, cd(-P * T), r);
+            comp_z5(Cm1, cd(P * T * T * T), r);
+            comp_z6(C0, cd(P * 2.0 * T * T), r);
+        }
         comp_z8(C0, cd(-P * T * T), r);
         comp_z2(Cv, cd(T * T));
     }
@@ -424,6 +652,16 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
     RX_TRY(cudaMalloc(&R->Xr, sizeof(double2) * h->nlm));
     RX_TRY(cudaMalloc(&R->F, sizeof(double2) * (size_t)(L + 1) * h->nlat));
     RX_TRY(cudaMalloc(&R->flag, sizeof(int)));
+    if (!p->robert) {
+        const size_t ldFc = (size_t)(2 * L + 1) * h->nlat;
+        RX_TRY(cudaMalloc(&R->PH, sizeof(double2) * (size_t)npoles * nc));
+        RX_TRY(cudaMalloc(&R->XY, sizeof(double2) * 2 * (size_t)npoles * nc));
+        RX_TRY(cudaMalloc(&R->FXY, sizeof(double2) * 2 * (size_t)npoles * ldFc));
+        RX_TRY(cudaMalloc(&R->Xs, sizeof(double2) * 8 * (size_t)h->nlm));
+        RX_TRY(cudaMalloc(&R->Fs, sizeof(double2) * 4 * (size_t)(L + 1) * h->nlat));
+        RX_TRY(cudaMemset(R->PH, 0, sizeof(double2) * (size_t)npoles * nc));
+        RX_TRY(cudaMemset(R->XY, 0, sizeof(double2) * 2 * (size_t)npoles * nc));
+    }
     RX_TRY(cudaMemcpy(R->alpha, al.data(), sizeof(double2) * npoles, cudaMemcpyHostToDevice));
     RX_TRY(cudaMemcpy(R->beta, be.data(), sizeof(double2) * npoles, cudaMemcpyHostToDevice));
     RX_TRY(cudaMemcpy(R->Cphi, cphi.data(), sizeof(double2) * cphi.size(), cudaMemcpyHostToDevice));

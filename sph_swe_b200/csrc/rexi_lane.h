@@ -504,14 +504,13 @@ __host__ __device__ inline bool rexi_factor_lane(const RexiDev& d, int m, double
     return ok;
 }
 
-// One pole, one m-block: Phi solve (both l-parities), velocity right-hand
-// sides and the two velocity solves.  Writes the unscaled phi, u, v of the
-// block's N = L+1-|m| rows to phi / ra / rb; returns false on a zero pivot.
-// STORED: substitutions only, with the factors rexi_factor_lane stored
-// (gl as there).
+// Phi of one pole and one m-block (both l-parities): the banded Phi systems
+// with Coriolis, the spectral Helmholtz solve without; writes the unscaled phi
+// of the block's N = L+1-|m| rows; returns false on a zero pivot.  Shared by
+// the Robert form and the non-Robert form (whose tables and pole-independent
+// vectors differ, not the arithmetic).
 template <int MAXN, bool MIXED = false, bool STORED = false>
-__host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* phi, double2* ra, double2* rb,
-                                   long long gl = 0) {
+__host__ __device__ bool rexi_phi(const RexiDev& d, int m, double2 a, double2* phi, long long gl = 0) {
     const int L = d.L;
     const int am = m < 0 ? -m : m;
     const int N = L + 1 - am;
@@ -521,11 +520,12 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
     const double2* V = d.V;
     const double2 a2 = c_mul(a, a), a3 = c_mul(a2, a), a4 = c_mul(a2, a2);
     const double2 ainv = c_div(make_double2(1, 0), a);
-    const double dm = m;
-
     bool ok = true;
     if (d.coriolis) {
-        // right-hand side weights of the 10 pole-independent vectors
+        // right-hand side weights of the 10 pole-independent vectors (the
+        // non-Robert form has the same weights; its vectors 0, 1, 4, 5 come from
+        // the non-Robert div0 and eta0 and 7, 8, 9 are the grid products
+        // grad_lat(mu) u0, grad_lat(mu) mu2 u0, grad_lat(mu) mu v0)
         double2 s[10];
         s[0] = c_scale(a2, P);                       // div0
         s[1] = c_scale(a, -P * T);                    // mu(eta0)
@@ -556,6 +556,40 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
             else
                 ok = band_solve<2, (MAXN + 1) / 2, 1>(Np, entry, rhs, out) && ok;
         }
+    } else {
+        // phi = (P div0 + a phi0) / (a^2 + (P/r^2) n(n+1)) (spec_solve_helmholtz)
+        for (int i = 0; i < N; i++) {
+            const int row = base + i;
+            const double n = am + i;
+            const double2 rhs = c_add(c_scale(ld(&V[row]), P), c_mul(a, ld(&V[(size_t)2 * nc + row])));
+            const double2 den = c_add(a2, make_double2(P / (d.r * d.r) * n * (n + 1.0), 0));
+            phi[i] = c_div(rhs, den);
+        }
+    }
+    return ok;
+}
+
+// One pole, one m-block: Phi solve (both l-parities), velocity right-hand
+// sides and the two velocity solves.  Writes the unscaled phi, u, v of the
+// block's N = L+1-|m| rows to phi / ra / rb; returns false on a zero pivot.
+// STORED: substitutions only, with the factors rexi_factor_lane stored
+// (gl as there).
+template <int MAXN, bool MIXED = false, bool STORED = false>
+__host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* phi, double2* ra, double2* rb,
+                                   long long gl = 0) {
+    const int L = d.L;
+    const int am = m < 0 ? -m : m;
+    const int N = L + 1 - am;
+    const int base = block_off(L, m);
+    const double T = d.T, ir = d.ir;
+    const int nc = d.ncplx;
+    const double2* V = d.V;
+    const double2 a2 = c_mul(a, a);
+    const double2 ainv = c_div(make_double2(1, 0), a);
+    const double dm = m;
+
+    bool ok = rexi_phi<MAXN, MIXED, STORED>(d, m, a, phi, gl);
+    if (d.coriolis) {
         // rhsa = a u0 + a ir i m phi - T mu(v0) - T ir mu(D phi)
         // rhsb = T mu(u0) + T ir mu(i m phi) + a v0 + a ir D phi
         // D phi of every row, parked in ra until the right-hand sides are formed
@@ -608,14 +642,7 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
                 ok = band_solve<1, (MAXN + 1) / 2, 2>(Np, entry, rhs2, out2) && ok;
         }
     } else {
-        // phi = (P div0 + a phi0) / (a^2 + (P/r^2) n(n+1)); u = (u0 + ir i m phi)/a; v = (v0 + ir D phi)/a
-        for (int i = 0; i < N; i++) {
-            const int row = base + i;
-            const double n = am + i;
-            const double2 rhs = c_add(c_scale(ld(&V[row]), P), c_mul(a, ld(&V[(size_t)2 * nc + row])));
-            const double2 den = c_add(a2, make_double2(P / (d.r * d.r) * n * (n + 1.0), 0));
-            phi[i] = c_div(rhs, den);
-        }
+        // u = (u0 + ir i m phi)/a; v = (v0 + ir D phi)/a
         for (int i = 0; i < N; i++) {
             const int row = base + i;
             const double* cf = d.coef + (size_t)row * 4;
@@ -624,6 +651,73 @@ __host__ __device__ bool rexi_lane(const RexiDev& d, int m, double2 a, double2* 
             const double2 dp = c_add(c_scale(lo, RX_LDG(cf + 2)), c_scale(hi, RX_LDG(cf + 3)));
             ra[i] = c_mul(ainv, c_add(ld(&V[(size_t)10 * nc + row]), c_scale(c_im(phi[i], dm), ir)));
             rb[i] = c_mul(ainv, c_add(ld(&V[(size_t)11 * nc + row]), c_scale(dp, ir)));
+        }
+    }
+    return ok;
+}
+
+// Non-Robert form (SWERexiSPH.hpp:137-244), velocity phase of one pole and one
+// m-block, once the pole's grid-valued gradients of phi have come back as
+// spectra (complex layout n*n+n+m): cx = F(grad_lon phi) = F(I(i m phi)/cos phi),
+// cy = F(grad_lat phi) = F(I((1-mu^2) d phi/dmu)/cos phi).  With
+// a_ = u0 + ir cx and b_ = v0 + ir cy:
+//   Coriolis:  rhsa = a a_ - T mu(b_), rhsb = T mu(a_) + a b_, then the two
+//              velocity solves (same matrix as the Robert form);
+//   otherwise: u = a_ / a, v = b_ / a.
+// Writes the unscaled u, v of the block's rows to ra / rb.
+template <int MAXN, bool MIXED = false, bool STORED = false>
+__host__ __device__ bool rexi_s0_vel(const RexiDev& d, int m, double2 a, const double2* cx, const double2* cy,
+                                     double2* ra, double2* rb, long long gl = 0) {
+    const int L = d.L;
+    const int am = m < 0 ? -m : m;
+    const int N = L + 1 - am;
+    const int base = block_off(L, m);
+    const double T = d.T, ir = d.ir;
+    const int nc = d.ncplx;
+    const double2* V = d.V;
+    const double2 a2 = c_mul(a, a);
+    const double2 ainv = c_div(make_double2(1, 0), a);
+    for (int i = 0; i < N; i++) {
+        const int row = base + i, n = am + i, ci = n * n + n + m;
+        ra[i] = c_add(ld(&V[(size_t)10 * nc + row]), c_scale(ld(&cx[ci]), ir));
+        rb[i] = c_add(ld(&V[(size_t)11 * nc + row]), c_scale(ld(&cy[ci]), ir));
+    }
+    bool ok = true;
+    if (d.coriolis) {
+        double2 aprev = make_double2(0, 0), bprev = make_double2(0, 0);  // a_, b_ of row i-1
+        for (int i = 0; i < N; i++) {
+            const double* cf = d.coef + (size_t)(base + i) * 4;
+            const double Rl = RX_LDG(cf), Sh = RX_LDG(cf + 1);
+            const double2 acur = ra[i], bcur = rb[i];
+            const double2 anext = i + 1 < N ? ra[i + 1] : make_double2(0, 0);
+            const double2 bnext = i + 1 < N ? rb[i + 1] : make_double2(0, 0);
+            const double2 mua = c_add(c_scale(aprev, Rl), c_scale(anext, Sh));  // mu(a_)_i
+            const double2 mub = c_add(c_scale(bprev, Rl), c_scale(bnext, Sh));  // mu(b_)_i
+            ra[i] = c_sub(c_mul(a, acur), c_scale(mub, T));
+            rb[i] = c_add(c_scale(mua, T), c_mul(a, bcur));
+            aprev = acur;
+            bprev = bcur;
+        }
+        for (int par = 0; par < 2; par++) {
+            const int Np = (N - par + 1) >> 1;
+            if (Np <= 0) continue;
+            auto entry = [&](int k, int dd) -> double2 { return vel_entry(d, base, par, a2, k, dd); };
+            auto rhs2 = [&](int k, int r) -> double2 { return r == 0 ? ra[par + 2 * k] : rb[par + 2 * k]; };
+            auto out2 = [&](int k, int r, double2 x) {
+                if (r == 0) ra[par + 2 * k] = x;
+                else rb[par + 2 * k] = x;
+            };
+            if constexpr (STORED)
+                band_solve_stored<1, (MAXN + 1) / 2, 2>(Np, band_ref(d.fvel, d.pvel, d, gl, base, N, par), rhs2, out2);
+            else if constexpr (MIXED)
+                ok = band_solve_mixed<1, (MAXN + 1) / 2, 2>(Np, d.refine, entry, rhs2, out2) && ok;
+            else
+                ok = band_solve<1, (MAXN + 1) / 2, 2>(Np, entry, rhs2, out2) && ok;
+        }
+    } else {
+        for (int i = 0; i < N; i++) {
+            ra[i] = c_mul(ainv, ra[i]);
+            rb[i] = c_mul(ainv, rb[i]);
         }
     }
     return ok;

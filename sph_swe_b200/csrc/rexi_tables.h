@@ -108,6 +108,34 @@ static void comp_z6robert(BandTable& t, cd s_, double r) {
         }
     }
 }
+// The non-Robert components of SWERexiSPH (SPHSolverComplex.hpp:221-234,
+// 263-280, 319-335): z4 = grad_j(mu) grad_i(phi) is diagonal (i m / r^2),
+// z5 = grad_j(mu) mu^2 grad_i(phi) is i m / r^2 times the mu^2 band, z6 =
+// grad_j(mu) mu grad_j(phi) uses the D, E, R, S identities; all offsets even.
+static void comp_z4(BandTable& t, cd s, double r) {
+    const int L = t.L;
+    for (int m = -L; m <= L; m++)
+        for (int n = std::abs(m); n <= L; n++) t.add(n, m, 0, 1.0 / (r * r) * s * cd(0, m));
+}
+static void comp_z5(BandTable& t, cd s, double r) {
+    const int L = t.L;
+    for (int m = -L; m <= L; m++)
+        for (int n = std::abs(m); n <= L; n++) {
+            const cd fac = 1.0 / (r * r) * s * cd(0, m);
+            t.add(n, m, -2, fac * idA(n - 2, m));
+            t.add(n, m, 0, fac * idB(n + 0, m));
+            t.add(n, m, +2, fac * idC(n + 2, m));
+        }
+}
+static void comp_z6(BandTable& t, cd s, double r) {
+    const int L = t.L;
+    for (int m = -L; m <= L; m++)
+        for (int n = std::abs(m); n <= L; n++) {
+            t.add(n, m, -2, -1.0 / (r * r) * s * (idD(n - 1, m) * idR(n - 2, m) + (idE(n, m) - 3.0) * idA(n - 2, m)));
+            t.add(n, m, 0, -1.0 / (r * r) * s * (1.0 + idD(n - 1, m) * idS(n, m) + (idE(n, m) - 3.0) * idB(n, m)));
+            t.add(n, m, +2, -1.0 / (r * r) * s * (idE(n, m) - 3.0) * idC(n + 2, m));
+        }
+}
 static void comp_z7(BandTable& t, cd s, double r) {
     const int L = t.L;
     for (int m = -L; m <= L; m++)

@@ -3,17 +3,23 @@
 // For a batch size it times every candidate of
 //   - the tensor-core Legendre synthesis and analysis (mixed handles): column
 //     tile of 16, 32 or 64 real columns per CTA (8, 16, 32 fields) x kernel:
-//     P loaded by the TMA unit and B staged by producer warps, both operands
-//     loaded by the TMA unit (B prepared once per call), or P regenerated from
-//     recurrence checkpoints; and the FP64 CUDA-core kernel of the plain form
-//     (variant 16: more accurate than the mixed form needs, taken when faster);
+//     the int8 integer-split kernel with the orders m ascending or paired with
+//     their complements (the m-to-CTA schedule), the split-TF32 kernels with P
+//     loaded by the TMA unit and B staged by producer warps, with both
+//     operands loaded by the TMA unit (B prepared once per call), or with P
+//     regenerated from recurrence checkpoints; and the FP64 CUDA-core kernel
+//     of the plain form (variant 16);
 //   - the fixed-length ring FFTs (automatic grids): 2P rings per CTA with the
 //     default P or half of it (more CTAs per SM, shorter tiles);
 // with CUDA events on the caller's stream (one warm-up launch, then the mean
 // of three), keeps the fastest in the handle (later calls with that batch
 // use it) and writes the table as JSON.  sph_tune_load re-applies a table.
-// Variants are exact alternatives: the column tile does not change any
-// arithmetic, the two P sources differ in the last bits of P_l^m only.
+// Within a kernel family the variants are exact alternatives: neither the
+// column tile nor the m order changes any arithmetic, the two P sources of the
+// split-TF32 form differ in the last bits of P_l^m only.  Across families the
+// results differ by the families' rounding (int8 ~1e-8, split TF32 ~3e-7
+// relative); the tuner takes the fastest of all of them, each of which meets
+// the mixed form's relL2 <= 1e-6 per transform.
 #include "common.cuh"
 
 #include <cstdio>
@@ -87,8 +93,10 @@ static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
         std::vector<int> cand;
         if (kind <= TUNE_TC_ANALYSIS) {
             if (!h->mixed) continue;
-            // B staged by producer warps (0), both operands loaded by the TMA unit (8), P regenerated (4)
-            for (int src : {0, 8, 4})
+            // int8 kernels in ascending (0) and paired (64) m order; split TF32 with
+            // B staged by producer warps (32), both operands loaded by the TMA unit
+            // (8), P regenerated (4)
+            for (int src : {0, 64, 32, 8, 4})
                 for (int c = 1; c <= 3; c++) cand.push_back(src | c);
             cand.push_back(16);  // FP64 CUDA-core kernel
         } else {

@@ -1,9 +1,10 @@
-// Exercises the per-pole REXI class SWERexiSPHRobert of
-// include/sph_swe/sph_swe.hpp the way AppSWE::run uses it (AppSWE.hpp:381-523):
+// Exercises the per-pole REXI classes SWERexiSPHRobert and SWERexiSPH of
+// include/sph_swe/sph_swe.hpp the way AppSWE::run uses them (AppSWE.hpp:381-523):
 // one object per pole, solve for (g h, u, v), sum over the poles, h = sum / g;
-// and, for comparison, one step of SWERexiRobert over all poles at once.
-// argv: L, output file.  Writes h, u, v of the pole loop, then h, u, v of
-// SWERexiRobert (complex128, packed layout); prints nlm and the pole count.
+// and, for comparison, one step of SWERexi over all poles at once.
+// argv: L, output file, form (1 Robert, the default; 0 non-Robert).  Writes
+// h, u, v of the pole loop, then h, u, v of SWERexi (complex128, packed
+// layout); prints nlm and the pole count.
 #include <sph_swe/sph_swe.hpp>
 
 #include <cmath>
@@ -23,6 +24,7 @@ static void put_spec(std::ofstream& f, const SPHData& x) {
 int main(int argc, char** argv) {
     if (argc < 3) return 1;
     const int L = std::atoi(argv[1]);
+    const bool robert = argc < 4 || std::atoi(argv[3]) != 0;
     try {
         SPHConfig cfg;
         cfg.setupAutoPhysicalSpace(L, L, nullptr, nullptr);
@@ -30,7 +32,7 @@ int main(int argc, char** argv) {
         p.earth_radius = 6.371e6;
         p.viscosity2 = 0.0;
         p.use_nonlinear_equations = false;
-        p.use_robert_functions = true;
+        p.use_robert_functions = robert;
         const double tau = 3600.0;
         // the 500 m bump at (30N, 60E), sigma = 0.1 a, on h0 = 1e4; rest state
         SPHData h(&cfg), u(&cfg), v(&cfg);
@@ -47,18 +49,22 @@ int main(int argc, char** argv) {
         rexi.setup(0.2, 16, 0, false);
         std::printf("%d %zu\n", cfg.spec_num_elems, rexi.alpha.size());
 
-        std::vector<SWERexiSPHRobert> poles(rexi.alpha.size());
+        std::vector<SWERexiSPHRobert> rpoles(robert ? rexi.alpha.size() : 0);
+        std::vector<SWERexiSPH> npoles(robert ? 0 : rexi.alpha.size());
+        std::vector<SWERexiSPHPole*> poles;
+        for (auto& q : rpoles) poles.push_back(&q);
+        for (auto& q : npoles) poles.push_back(&q);
         for (size_t k = 0; k < poles.size(); k++)
-            poles[k].setup(&cfg, rexi.alpha[k], rexi.beta_re[k], p.earth_radius, p.coriolis_omega,
-                           p.h0 * p.gravitation, tau);
+            poles[k]->setup(&cfg, rexi.alpha[k], rexi.beta_re[k], p.earth_radius, p.coriolis_omega,
+                            p.h0 * p.gravitation, tau);
         SPHOperatorsComplex op;
         const SPHData phi0 = h * p.gravitation;
         SPHData acc_phi(&cfg), acc_u(&cfg), acc_v(&cfg), t_phi, t_u, t_v;
         acc_phi.spec_set_zero();
         acc_u.spec_set_zero();
         acc_v.spec_set_zero();
-        for (auto& pole : poles) {
-            pole.solve(phi0, u, v, t_phi, t_u, t_v, op);
+        for (auto* pole : poles) {
+            pole->solve(phi0, u, v, t_phi, t_u, t_v, op);
             acc_phi += t_phi;
             acc_u += t_u;
             acc_v += t_v;
@@ -67,7 +73,7 @@ int main(int argc, char** argv) {
         put_spec(out, acc_phi * (1.0 / p.gravitation));
         put_spec(out, acc_u);
         put_spec(out, acc_v);
-        SWERexiRobert all(&cfg, p, rexi, tau);
+        SWERexi all(&cfg, p, rexi, tau, robert);
         all.run(h, u, v, 1);
         put_spec(out, h);
         put_spec(out, u);

@@ -147,3 +147,71 @@ def test_checkpoint_generator_path_vs_oracle(gpu):
     assert r.returncode == 0, r.stderr[-2000:]
     syn, ana = (float(x) for x in r.stdout.split()[-2:])
     assert syn < TOL and ana < TOL
+
+
+def _plm_at(mu_north, T):
+    import scipy.special as sp
+
+    th = np.arccos(np.asarray(mu_north))
+    cache = {}
+
+    def P(m):
+        if m not in cache:
+            cache[m] = np.nan_to_num(np.array([sp.sph_harm_y(l, m, th, 0.0).real for l in range(m, T + 1)]))
+        return cache[m]
+
+    return P
+
+
+@pytest.mark.parametrize("L,nb", [(31, 3), (63, 5), (127, 17)])
+def test_int8_legendre_matches_integer_split_model(gpu, oracle_mod, L, nb):
+    """The Legendre stages of the mixed form (int8 kernels, the default) carry
+    out the arithmetic of the integer-split model (oracle/intsplit.py) given P
+    at the handle's own Gauss nodes: the same row and column exponents, digits
+    and exact integer group sums, so the results agree far below the form's
+    own error (the model's P comes from scipy, the kernel's from its FP64
+    recurrence, so a digit may differ in the last place), and both are within
+    2e-8 of the FP64 oracle."""
+    from oracle import intsplit
+
+    s = _mixed(L)
+    g = oracle_mod.Grid(L)
+    nh = s.nlat // 2
+    P = _plm_at(s.mu[:nh], L + 1)  # the handle's tables reach degree L + 1
+    spec = random_spec(L, nb, seed=40 + L)
+    four = torch.empty(nb, L + 1, s.nlat, dtype=torch.complex128, device="cuda")
+    s.legendre_synthesis(torch.from_numpy(spec).cuda(), four)
+    _sync_ok(s)
+    Fm, gmax = intsplit.synthesis(P, nh, s.nlat, L, spec, 4)
+    assert gmax < 2 ** 31
+    got = four.cpu().numpy()
+    assert rel_l2(got, Fm) < 1e-11
+    grid = g.SH_to_spat(spec)
+    F = (2 * np.pi / s.nphi) * np.fft.fft(grid, axis=1)[:, : L + 1, :]
+    out = torch.empty(nb, s.nlm, dtype=torch.complex128, device="cuda")
+    s.legendre_analysis(torch.from_numpy(np.ascontiguousarray(F)).cuda(), out)
+    _sync_ok(s)
+    sm, gmax = intsplit.analysis(P, nh, s.nlat, L, F, np.asarray(s.w), 4)
+    assert gmax < 2 ** 31
+    assert rel_l2(out.cpu().numpy(), sm) < 1e-11
+    assert rel_l2(out.cpu().numpy(), g.spat_to_SH(grid)) < 2e-8
+
+
+@pytest.mark.parametrize("L,nb", [(63, 8), (255, 20)])
+def test_split_tf32_variant_vs_oracle(gpu, oracle_mod, L, nb):
+    """The split-TF32 kernels stay selectable (autotuner variants 33-35: P by
+    TMA, B staged by producer warps) and within relL2 1e-6 of the oracle for
+    scalar transforms."""
+    s = _mixed(L)
+    g = oracle_mod.Grid(L)
+    s.tune_load({"lmax": L, "nphi": s.nphi, "kernels": [{"kind": k, "batch": nb, "variant": 33} for k in (0, 1)]})
+    spec = random_spec(L, nb, seed=300 + L)
+    ref = g.SH_to_spat(spec)
+    out = s.SH_to_spat(torch.from_numpy(spec).cuda()).cpu().numpy()
+    back = s.spat_to_SH(torch.from_numpy(ref).cuda()).cpu().numpy()
+    _sync_ok(s)
+    ana = g.spat_to_SH(ref)
+    for b in range(nb):
+        assert rel_l2(out[b], ref[b]) < TOL
+        assert rel_l2(back[b], ana[b]) < TOL
+

@@ -1,6 +1,7 @@
-"""Parity of the GPU REXI integrator (Robert formulation) with the oracle,
-which follows SWERexiSPHRobert::setup/solve and SPHSolverComplex with LAPACK
-zgbsv semantics (full-grid Coriolis product, see the oracle header)."""
+"""Parity of the GPU REXI integrator with the oracle, which follows
+SWERexiSPHRobert::setup/solve (Robert form, S1), SWERexiSPH::setup/solve
+(non-Robert form, S0) and SPHSolverComplex with LAPACK zgbsv semantics
+(full-grid Coriolis product, see the oracle header)."""
 import numpy as np
 import pytest
 import torch
@@ -12,7 +13,7 @@ pytestmark = pytest.mark.gpu
 P6 = (6.371e6, 9.80616, 7.292e-5, 1e4, 0.0, 3600.0)
 
 
-def _run(gpu_sph, g, oracle_mod, L, M, half, steps, coriolis=1, fix=0, visc=0.0, seed=None, precision=0):
+def _run(gpu_sph, g, oracle_mod, L, M, half, steps, coriolis=1, fix=0, visc=0.0, seed=None, precision=0, robert=1):
     a, br, bi = oracle_mod.rexi_coeffs(0.2, M, half=half)
     h = g.spat_to_SH(bump_state(g))
     if seed is None:
@@ -23,11 +24,11 @@ def _run(gpu_sph, g, oracle_mod, L, M, half, steps, coriolis=1, fix=0, visc=0.0,
     p = list(P6)
     p[4] = visc
     rx = gpu_sph.rexi(a, br, radius=p[0], gravity=p[1], omega=p[2], h0=p[3], viscosity=visc, tau=p[5],
-                      coriolis=coriolis, fix_z5robert=fix, precision=precision)
+                      coriolis=coriolis, fix_z5robert=fix, precision=precision, robert=robert)
     st = torch.from_numpy(np.stack([h, u, v])).cuda()
     rx.step(st, steps)
     out = st.cpu().numpy()
-    rh, ru, rv, npol = g.rexi_run(tuple(p), h, u, v, steps, rexi_h=0.2, rexi_M=M, half=half, robert=1,
+    rh, ru, rv, npol = g.rexi_run(tuple(p), h, u, v, steps, rexi_h=0.2, rexi_M=M, half=half, robert=robert,
                                   coriolis=coriolis, fix_z5robert=fix)
     assert npol == len(a)
     return out, (rh, ru, rv)
@@ -45,6 +46,40 @@ def test_rexi_matches_oracle(gpu, oracle_mod, L, M, half, coriolis, fix, visc, s
 
     s, g = Sph(L), oracle_mod.Grid(L)
     out, ref = _run(s, g, oracle_mod, L, M, half, 2, coriolis, fix, visc, seed)
+    for q in range(3):
+        assert rel_l2(out[q], ref[q]) < 1e-10, q
+
+
+@pytest.mark.parametrize("L,M,half,coriolis,visc,seed,precision", [
+    (31, 64, False, 1, 0.0, None, 0),
+    (31, 64, True, 1, 1e5, 7, 0),
+    (31, 32, False, 0, 0.0, 8, 0),
+    (63, 64, False, 1, 0.0, 9, 0),
+    (63, 32, False, 0, 1e5, 10, 0),
+    (31, 64, False, 1, 0.0, 11, 1),
+])
+def test_non_robert_rexi_matches_oracle(gpu, oracle_mod, L, M, half, coriolis, visc, seed, precision):
+    """The non-Robert form (SWERexiSPH, S0): Phi systems from the non-Robert z4,
+    z5, z6 components (SPHSolverComplex.hpp:221-367), div0 / eta0 and the
+    velocity recovery through the grid divisions by cos(phi) of
+    SPHOperatorsComplex.  FP64 within 1e-10 of the oracle; the mixed form
+    (complex FP32 solves, FP64 refinement) within 1e-9."""
+    from sph_swe_b200.sph import Sph
+
+    s, g = Sph(L), oracle_mod.Grid(L)
+    out, ref = _run(s, g, oracle_mod, L, M, half, 2, coriolis, 0, visc, seed, precision=precision, robert=0)
+    for q in range(3):
+        assert rel_l2(out[q], ref[q]) < (1e-10 if precision == 0 else 1e-9), q
+
+
+def test_non_robert_rexi_config2_size(gpu, oracle_mod):
+    """Configuration 2 in the non-Robert form: T127, M = 256 (535 poles),
+    tau = 3600 s, two steps from the bump, FP64 within 1e-10 of the oracle."""
+    from sph_swe_b200.sph import Sph
+
+    L = 127
+    s, g = Sph(L), oracle_mod.Grid(L)
+    out, ref = _run(s, g, oracle_mod, L, 256, False, 2, robert=0)
     for q in range(3):
         assert rel_l2(out[q], ref[q]) < 1e-10, q
 

@@ -109,13 +109,15 @@ def test_complex_class_operators_match_oracle(classes_cplx_bin, oracle_mod, tmp_
     assert rel_l2(blocks[16].real, g.SH_to_spat(g.spat_to_SH(gx.real))) < 1e-12
 
 
-def test_per_pole_rexi_class_matches_oracle(gpu, oracle_mod, tmp_path):
-    """SWERexiSPHRobert used as AppSWE::run uses it (one object per pole,
-    solve, sum over the poles, divide by g) equals one SWERexiRobert step over
-    all poles and the oracle's REXI step (T31, M = 16, full pole set)."""
+@pytest.mark.parametrize("robert", [1, 0])
+def test_per_pole_rexi_class_matches_oracle(gpu, oracle_mod, tmp_path, robert):
+    """SWERexiSPHRobert (robert = 1) and SWERexiSPH (robert = 0) used as
+    AppSWE::run uses them (one object per pole, solve, sum over the poles,
+    divide by g) equal one SWERexi step over all poles and the oracle's REXI
+    step of the same form (T31, M = 16, full pole set)."""
     exe = _compile("rexi_pole_check.cpp", str(tmp_path / "rexi_pole_check"))
     outp = tmp_path / "out.bin"
-    r = subprocess.run([exe, "31", str(outp)], capture_output=True, text=True)
+    r = subprocess.run([exe, "31", str(outp), str(robert)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     nlm, npoles = map(int, r.stdout.split()[:2])
     assert npoles == 55
@@ -124,7 +126,7 @@ def test_per_pole_rexi_class_matches_oracle(gpu, oracle_mod, tmp_path):
     h = g.spat_to_SH(bump_state(g))
     z = np.zeros(g.nlm, complex)
     ref = g.rexi_run((6.371e6, 9.80616, 7.292e-5, 1e4, 0.0, 3600.0), h, z, z, 1, rexi_h=0.2, rexi_M=16, half=False,
-                     robert=1)[:3]
+                     robert=robert)[:3]
     for q in range(3):
         assert rel_l2(loop[q], full[q]) < 1e-12, q
         assert rel_l2(loop[q], ref[q]) < 1e-10, q
