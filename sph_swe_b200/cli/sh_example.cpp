@@ -194,7 +194,10 @@ void initial_state(const Vars& v, SPHConfig& cfg, SPHData& h, SPHData& u, SPHDat
                 const size_t k = (size_t)i * cfg.spat_num_lat + j;
                 hg[k] = hr[j] + hhat * std::cos(phi) * std::exp(-std::pow((lam - M_PI) / alpha, 2.0)) *
                                     std::exp(-std::pow((phi2 - phi) / beta, 2.0));
-                ug[k] = ujet(phi) * ((v.robert || v.nonlinear == 2) ? std::cos(phi) : 1.0);
+                // the reference stores the jet itself in prog_u also in the Robert
+                // form (AppSWE.hpp:199-206); only the vorticity-divergence form
+                // (N2) takes the Robert velocity u cos(phi) for its vector analysis
+                ug[k] = ujet(phi) * (v.nonlinear == 2 ? std::cos(phi) : 1.0);
             }
         }
         h.spat_from_host(hg);

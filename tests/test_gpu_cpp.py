@@ -169,6 +169,24 @@ def test_sh_example_galewsky(gpu, tmp_path):
         assert 9000 < vals.min() < vals.max() < 11000
 
 
+@pytest.mark.parametrize("robert", [0, 1])
+def test_sh_example_galewsky_initial_state_matches_oracle(gpu, oracle_mod, tmp_path, robert):
+    """Scenario Q1 (BenchmarkGalewsky.hpp:18-243) as sh_example sets it up: the
+    balanced height, the bump and the jet (in prog_u in both forms, as
+    AppSWE.hpp:199-206) against the oracle's restatement of BenchmarkGalewsky
+    with adaptive quadrature (oracle/galewsky.py), compared as spectra.  R60
+    E20 rounds to zero steps, so the checkpoint holds the initial state."""
+    from oracle import galewsky as G
+
+    st, out = _run_cli(["T63", "P0", "N1", f"S{robert}", "R60", "E20", "O1e9", "V0", "Q1"], tmp_path)
+    g = oracle_mod.Grid(63)
+    ho, uo, vo = G.initial_state(g.lat, g.nphi, 6.37122e6, 9.80616, 7.292e-5)
+    n = g.nlm
+    assert rel_l2(st[:n], g.spat_to_SH(ho)) < 1e-12
+    assert rel_l2(st[n:2 * n], g.spat_to_SH(uo)) < 1e-12
+    assert np.abs(st[2 * n:]).max() == 0.0
+
+
 def test_sh_example_checkpoint_resume(gpu, tmp_path):
     """C<file> resumes from a D<file> dump: 5 + 5 steps equal 10 steps bitwise."""
     base = ["T31", "P0", "N1", "R120", "O1e9", "Q10"]

@@ -95,3 +95,18 @@ def test_galewsky_state_shapes(oracle_mod):
     assert h.shape == u.shape == v.shape == (g.nphi, g.nlat)
     assert np.all(np.isfinite(h)) and np.max(u) <= 80.0 + 1e-9 and np.all(v == 0)
     assert 9000 < h.min() < h.max() < 11000
+
+
+@pytest.mark.parametrize("L", [63, 127])
+def test_galewsky_state_matches_oracle_restatement(oracle_mod, L):
+    """scenarios.galewsky (fixed 24-point Gauss rule per ring interval) against
+    the oracle's restatement of BenchmarkGalewsky::setup_initial_h with the
+    bump (oracle/galewsky.py, adaptive quadrature to the reference's 1e-13)."""
+    from oracle import galewsky as G
+
+    g = oracle_mod.Grid(L)
+    h, u, v = S.galewsky(g)
+    ho, uo, vo = G.initial_state(g.lat, g.nphi, 6.37122e6, 9.80616, 7.292e-5)
+    assert np.abs(h - ho).max() < 1e-9  # metres on a 1e4 m mean
+    assert np.abs(u - uo).max() < 1e-12
+    assert np.array_equal(v, vo)
