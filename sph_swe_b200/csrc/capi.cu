@@ -132,6 +132,7 @@ int sph_destroy(sph_handle* h) {
     tc_tables_free(h);
     if (h->mu) cudaFree(h->mu);
     if (h->w) cudaFree(h->w);
+    if (h->wc) cudaFree(h->wc);
     if (h->cosphi) cudaFree(h->cosphi);
     if (h->lat) cudaFree(h->lat);
     if (h->plm) cudaFree(h->plm);

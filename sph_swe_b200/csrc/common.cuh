@@ -46,6 +46,7 @@ struct Handle {
     int device = 0;
     double* mu = nullptr;       // nlat
     double* w = nullptr;        // nlat
+    double* wc = nullptr;       // nlat: w / cos(phi)
     double* cosphi = nullptr;   // nlat
     double* lat = nullptr;      // nlat
     // P_l^m(mu_j), j < nh, m = 0..L+1, l = m..L+1 at plm[poff[m] + (l-m)*nh + j]
@@ -111,8 +112,12 @@ int ring_synthesis_cplx(const Handle* h, const double2* F, long long ldF, double
 int legendre_kernels_init();  // loads the FP64 Legendre kernels (lazy module loading)
 int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
                             long long ldF, int batch, cudaStream_t s);
+// wmode 0: Gauss weights; 1: Gauss weights / cos(phi) -- the input then holds
+// cos(phi) times the integrand (e.g. u / cos(phi) analysed from u), which keeps
+// it bounded at the polar rings, where the mixed form's per-column scales would
+// otherwise be set by a 1/cos(phi) growth
 int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
-                           int lmax, int batch, cudaStream_t s);
+                           int lmax, int batch, cudaStream_t s, int wmode = 0);
 int legendre_synthesis_cplx(const Handle* h, const double2* spec, long long ld_spec, double2* F, long long ldF,
                             int batch, cudaStream_t s);
 int legendre_analysis_cplx(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
@@ -131,7 +136,7 @@ bool tc_synthesis_needs_alloc(const Handle* h, int lmax, int batch);
 int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F, long long ldF,
                           int batch, cudaStream_t s);
 int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec, int lmax,
-                         int batch, cudaStream_t s);
+                         int batch, cudaStream_t s, int wmode = 0);
 
 // spectral operators (packed real or complex layout)
 int spec_copy_modes(const Handle* hs, const double2* src, long long lds, const Handle* hd, double2* dst,

@@ -426,7 +426,8 @@ static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double
 }
 
 static int launch_anal(const Handle* h, const double2* F, long long ldF, double2* spec, SpecMap sm, int batch,
-                       cudaStream_t s) {
+                       cudaStream_t s, const double* wts = nullptr) {
+    if (!wts) wts = h->w;
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
     if (batch > 16) {
@@ -439,11 +440,11 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
             attr_done.fetch_or(bit);
         }
         dim3 grid((sm.lmax + 1 + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
-        k_legendre_analysis_w<<<grid, WNT, WSMEM_ANA, s>>>(h->plm, h->poff, h->nh, h->nlat, h->w, F, ldF, spec, sm,
+        k_legendre_analysis_w<<<grid, WNT, WSMEM_ANA, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm,
                                                         batch);
     } else {
         dim3 grid((sm.lmax + 1 + TLT - 1) / TLT, (batch + TC / 2 - 1) / (TC / 2), nm);
-        k_legendre_analysis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, h->w, F, ldF, spec, sm, batch);
+        k_legendre_analysis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch);
     }
     SPH_CUDA_TRY(cudaGetLastError());
     if (!sm.cplx && sm.lmax > h->L) {
@@ -480,9 +481,9 @@ int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_s
 }
 
 int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
-                           int lmax, int batch, cudaStream_t s) {
+                           int lmax, int batch, cudaStream_t s, int wmode) {
     if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_ANALYSIS, batch, 0) & 16)) {
-        if (int rc = legendre_analysis_tc(h, F, ldF, spec, ld_spec, lmax, batch, s)) return rc;
+        if (int rc = legendre_analysis_tc(h, F, ldF, spec, ld_spec, lmax, batch, s, wmode)) return rc;
         if (lmax > h->L) {
             k_zero_top<<<(batch + 127) / 128, 128, 0, s>>>(spec, ld_spec, lmax, batch);
             SPH_CUDA_TRY(cudaGetLastError());
@@ -490,7 +491,7 @@ int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, dou
         return SPH_OK;
     }
     SpecMap sm{0, lmax, h->L, ld_spec};
-    return launch_anal(h, F, ldF, spec, sm, batch, s);
+    return launch_anal(h, F, ldF, spec, sm, batch, s, wmode ? h->wc : h->w);
 }
 
 int legendre_synthesis_cplx(const Handle* h, const double2* spec, long long ld_spec, double2* F, long long ldF,

@@ -83,11 +83,13 @@ __device__ __forceinline__ void mma_s8(uint32_t tmem_d, uint64_t a, uint64_t b, 
         "l"(a), "l"(b), "r"(idesc), "r"(accum));
 }
 
-// balanced base-256 digit word of v = rint(x * s1 * s2) (s1 s2 = 2^(31 - e), split
-// in two powers of two so that neither overflows)
-__device__ __forceinline__ uint32_t i8_word(double x, double s1, double s2) {
-    const int v = __double2int_rn((x * s1) * s2);
-    return (uint32_t)(v + 0x808080) ^ 0x808080u;
+// balanced base-256 digit word of v = rint(t s1 s2), s1 s2 = 2^(31 - e) split in
+// two powers of two so that neither overflows (|v| < 2^31): t s1 is exact, and
+// adding 1.5 2^52 in the same FMA rounds t s1 s2 to the nearest integer (half
+// to even), which then sits in the low 32 bits of the result
+__device__ __forceinline__ uint32_t i8_word(double t, double s1, double s2) {
+    const uint32_t v = (uint32_t)__double2loint(fma(t * s1, s2, 0x1.8p52));
+    return (v + 0x808080u) ^ 0x808080u;
 }
 // the powers of two 2^(31 - e) as two factors
 __device__ __forceinline__ double2 i8_scale(int e) {
@@ -107,22 +109,48 @@ __device__ __forceinline__ double i8_pow2(int k) {
     return ldexp(1.0, k);
 }
 
-// digit planes of 16 words w[0..15] (values of 16 consecutive K indices):
-// plane d (0 = most significant digit) as 16 bytes, value i at byte i
-__device__ __forceinline__ void i8_planes(const uint32_t* w, uint4* pl) {
-    uint32_t o[4][4];  // [plane][word]
+// unsigned 64-bit pattern of a non-negative double (ordered like the values)
+__device__ __forceinline__ unsigned long long i8_bits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// the digit planes of 4 words (values of 4 consecutive K indices): o[d] holds
+// digit d (0 = most significant) of the 4 values, value k at byte k
+__device__ __forceinline__ void i8_planes4(uint32_t a, uint32_t b, uint32_t c, uint32_t e, uint32_t* o) {
+    const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
+    const uint32_t t2 = __byte_perm(c, e, 0x5140), t3 = __byte_perm(c, e, 0x7362);
+    o[3] = __byte_perm(t0, t2, 0x5410);  // byte 0 of each word: d3
+    o[2] = __byte_perm(t0, t2, 0x7632);  // byte 1: d2
+    o[1] = __byte_perm(t1, t3, 0x5410);  // byte 2: d1
+    o[0] = __byte_perm(t1, t3, 0x7632);  // byte 3: d0
+}
+
+// Producer micro-tasks: one task = one field and 4 consecutive K indices of
+// both parities; task t -> (q = t & 3, fl = (t >> 2) % NF, zl = (t >> 2) / NF)
+// with K indices 16 zl + 4 q + (0..3), so that 4 neighbouring lanes fill one
+// 16-byte row of a digit plane.  Every producer runs the same number of loop
+// trips (tasks beyond the count contribute nothing), so the column-maximum
+// reduction can use warp shuffles.
+__device__ __forceinline__ int i8_trips(int ntasks) { return (ntasks + li8::NPROD - 1) / li8::NPROD; }
+
+// column maxima (bit patterns of non-negative doubles) of a task's two columns,
+// reduced over the 4 lanes of one field before one shared-memory atomic each
+__device__ __forceinline__ void i8_colmax(double mr, double mi, bool lead, int fl, unsigned long long* colmax) {
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const uint32_t a = w[4 * q], b = w[4 * q + 1], c = w[4 * q + 2], e = w[4 * q + 3];
-        const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
-        const uint32_t t2 = __byte_perm(c, e, 0x5140), t3 = __byte_perm(c, e, 0x7362);
-        o[3][q] = __byte_perm(t0, t2, 0x5410);  // byte 0 of each: d3
-        o[2][q] = __byte_perm(t0, t2, 0x7632);  // byte 1: d2
-        o[1][q] = __byte_perm(t1, t3, 0x5410);  // byte 2: d1
-        o[0][q] = __byte_perm(t1, t3, 0x7632);  // byte 3: d0
+    for (int o = 1; o < 4; o <<= 1) {
+        mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+        mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
     }
+    if (lead) {
+        atomicMax(&colmax[2 * fl], i8_bits(mr));
+        atomicMax(&colmax[2 * fl + 1], i8_bits(mi));
+    }
+}
+
+// store the 4 plane words of one (parity, column) stream of a task
+template <int NC, int ZSEG>
+__device__ __forceinline__ void i8_put(unsigned char* Bs, int par, int zl, int c, int q, const uint32_t* o) {
 #pragma unroll
-    for (int d = 0; d < 4; d++) pl[d] = make_uint4(o[d][0], o[d][1], o[d][2], o[d][3]);
+    for (int d = 0; d < li8::ND; d++)
+        *reinterpret_cast<uint32_t*>(Bs + ((size_t)((par * li8::ND + d) * ZSEG + zl) * NC + c) * 16 + 4 * q) = o[d];
 }
 
 struct I8Args {
@@ -163,8 +191,6 @@ __device__ __forceinline__ I8Tile i8_tile(const I8Args& a, int t) {
     return p;
 }
 
-// unsigned 64-bit pattern of a non-negative double (ordered like the values)
-__device__ __forceinline__ unsigned long long i8_bits(double x) { return (unsigned long long)__double_as_longlong(x); }
 
 // ------------------------------------------------------------------ synthesis
 template <int NC>
@@ -177,52 +203,49 @@ struct SynI8 {
         const long long z = a.zoff[p.m] + (long long)par * 2 * i8_nch(a.tlmax, p.m) + 2 * kc;
         return make_int3(0, 2 * p.rt, (int)z);
     }
-    // pass 1: task (field, z group, parity) -> column maxima of |re|, |im|
-    __device__ static int scan_tasks(const I8Tile& p) { return NF * 2 * (2 * p.nch); }
-    __device__ static void scan(const I8Args& a, const I8Tile& p, int task, const double2* __restrict__ spec,
+    // tasks of a K range of nz z groups (16 K indices each, per parity)
+    __device__ static int tasks(int nz) { return NF * 4 * nz; }
+    // the 8 coefficients l = m + 2 k0 .. m + 2 k0 + 7 (K indices k0..k0+3 of both parities)
+    __device__ static void load(const I8Args& a, const I8Tile& p, int f, int k0, const double2* __restrict__ spec,
+                                double2* q) {
+        const double2* src = spec + (long long)(f < a.batch ? f : 0) * a.ld_spec;
+        const int l0 = p.m + 2 * k0;
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            q[i] = (f < a.batch && l0 + i <= a.lmax) ? src[pidx(a.lmax, l0 + i, p.m)] : make_double2(0.0, 0.0);
+    }
+    // pass 1: column maxima of |re|, |im| over all degrees of the tile
+    __device__ static void scan(const I8Args& a, const I8Tile& p, int task, bool live, const double2* __restrict__ spec,
                                 unsigned long long* colmax) {
-        const int fl = task % NF, rest = task / NF, par = rest & 1, z = rest >> 1;
-        const int f = p.ct * NF + fl;
-        if (f >= a.batch) return;
-        const double2* src = spec + (long long)f * a.ld_spec;
+        const int q = task & 3, fl = (task >> 2) % NF, zl = (task >> 2) / NF;
         double mr = 0.0, mi = 0.0;
-#pragma unroll 4
-        for (int i = 0; i < 16; i++) {
-            const int l = p.m + par + 2 * (16 * z + i);
-            if (l <= a.lmax) {
-                const double2 q = src[pidx(a.lmax, l, p.m)];
-                mr = fmax(mr, fabs(q.x));
-                mi = fmax(mi, fabs(q.y));
+        if (live) {
+            double2 v[8];
+            load(a, p, p.ct * NF + fl, 16 * zl + 4 * q, spec, v);
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                mr = fmax(mr, fabs(v[i].x));
+                mi = fmax(mi, fabs(v[i].y));
             }
         }
-        atomicMax(&colmax[2 * fl], i8_bits(mr));
-        atomicMax(&colmax[2 * fl + 1], i8_bits(mi));
+        i8_colmax(mr, mi, live && q == 0, fl, colmax);
     }
-    // pass 2: task (field, z group of the segment, parity) -> 2 x 4 digit rows
-    __device__ static int digit_tasks(int nz) { return NF * 2 * nz; }
+    // pass 2: the digit planes of 4 K indices of both parities, both columns
     __device__ static void digits(const I8Args& a, const I8Tile& p, int task, int z0, const double2* __restrict__ spec,
                                   const double2* scl, unsigned char* Bs) {
-        const int fl = task % NF, rest = task / NF, par = rest & 1, zl = rest >> 1;
-        const int f = p.ct * NF + fl, z = z0 + zl;
-        uint32_t wr[16], wi[16];
+        const int q = task & 3, fl = (task >> 2) % NF, zl = (task >> 2) / NF;
+        double2 v[8];
+        load(a, p, p.ct * NF + fl, 16 * (z0 + zl) + 4 * q, spec, v);
         const double2 sr = scl[2 * fl], si = scl[2 * fl + 1];
-        const double2* src = spec + (long long)(f < a.batch ? f : 0) * a.ld_spec;
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int l = p.m + par + 2 * (16 * z + i);
-            double2 q = make_double2(0.0, 0.0);
-            if (f < a.batch && l <= a.lmax) q = src[pidx(a.lmax, l, p.m)];
-            wr[i] = i8_word(q.x, sr.x, sr.y);
-            wi[i] = i8_word(q.y, si.x, si.y);
-        }
-        uint4 pr[4], pi[4];
-        i8_planes(wr, pr);
-        i8_planes(wi, pi);
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-            uint4* row = reinterpret_cast<uint4*>(Bs + ((size_t)((par * li8::ND + d) * ZSEG + zl) * NC + 2 * fl) * 16);
-            row[0] = pr[d];
-            row[1] = pi[d];
+        for (int par = 0; par < 2; par++) {
+            uint32_t o[4];
+            i8_planes4(i8_word(v[par].x, sr.x, sr.y), i8_word(v[2 + par].x, sr.x, sr.y),
+                       i8_word(v[4 + par].x, sr.x, sr.y), i8_word(v[6 + par].x, sr.x, sr.y), o);
+            i8_put<NC, ZSEG>(Bs, par, zl, 2 * fl, q, o);
+            i8_planes4(i8_word(v[par].y, si.x, si.y), i8_word(v[2 + par].y, si.x, si.y),
+                       i8_word(v[4 + par].y, si.x, si.y), i8_word(v[6 + par].y, si.x, si.y), o);
+            i8_put<NC, ZSEG>(Bs, par, zl, 2 * fl + 1, q, o);
         }
     }
     // consumer: TMEM lane r = latitude 128 rt + r; e, o: 8 columns of parity 0 / 1
@@ -258,56 +281,64 @@ struct AnaI8 {
         const long long y = a.aoff[p.m] + (long long)par * tcs_pad64(i8_nlp(a.tlmax, p.m, 0)) + li8::M * p.rt;
         return make_int3(0, (int)(y >> 6), 2 * kc);
     }
-    // pass 1: task (field, z group) -> column maxima of |north| + |south|
-    __device__ static int scan_tasks(const I8Tile& p) { return NF * 2 * p.nch; }
-    __device__ static void scan(const I8Args& a, const I8Tile& p, int task, const double2* __restrict__ F,
+    __device__ static int tasks(int nz) { return NF * 4 * nz; }
+    // north and south Fourier values of the latitudes j0..j0+3
+    __device__ static void load(const I8Args& a, const I8Tile& p, int f, int j0, const double2* __restrict__ F,
+                                double2* n, double2* s) {
+        const double2* src = F + (long long)(f < a.batch ? f : 0) * a.ldF + (long long)p.m * a.nlat;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const bool v = f < a.batch && j0 + i < a.nh;
+            n[i] = v ? src[j0 + i] : make_double2(0.0, 0.0);
+            s[i] = v ? src[a.nlat - 1 - j0 - i] : make_double2(0.0, 0.0);
+        }
+    }
+    // pass 1: column maxima of |north| + |south| (re, im) over all latitudes
+    __device__ static void scan(const I8Args& a, const I8Tile& p, int task, bool live, const double2* __restrict__ F,
                                 unsigned long long* colmax) {
-        const int fl = task % NF, z = task / NF;
-        const int f = p.ct * NF + fl;
-        if (f >= a.batch) return;
-        const double2* src = F + (long long)f * a.ldF + (long long)p.m * a.nlat;
+        const int q = task & 3, fl = (task >> 2) % NF, zl = (task >> 2) / NF;
         double mr = 0.0, mi = 0.0;
-#pragma unroll 4
-        for (int i = 0; i < 16; i++) {
-            const int j = 16 * z + i;
-            if (j < a.nh) {
-                const double2 n = src[j], s = src[a.nlat - 1 - j];
-                mr = fmax(mr, fabs(n.x) + fabs(s.x));
-                mi = fmax(mi, fabs(n.y) + fabs(s.y));
+        if (live) {
+            double2 n[4], s[4];
+            load(a, p, p.ct * NF + fl, 16 * zl + 4 * q, F, n, s);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                mr = fmax(mr, fabs(n[i].x) + fabs(s[i].x));
+                mi = fmax(mi, fabs(n[i].y) + fabs(s[i].y));
             }
         }
-        atomicMax(&colmax[2 * fl], i8_bits(mr));
-        atomicMax(&colmax[2 * fl + 1], i8_bits(mi));
+        i8_colmax(mr, mi, live && q == 0, fl, colmax);
     }
-    __device__ static int digit_tasks(int nz) { return NF * 2 * nz; }
+    // pass 2: digits of north + south (parity 0) and north - south (parity 1)
+    // of 4 latitudes, both columns; the scale is applied to north and south
+    // first (exact), so the sum is rounded once, as (north +/- south) would be
     __device__ static void digits(const I8Args& a, const I8Tile& p, int task, int z0, const double2* __restrict__ F,
                                   const double2* scl, unsigned char* Bs) {
-        const int fl = task % NF, rest = task / NF, par = rest & 1, zl = rest >> 1;
-        const int f = p.ct * NF + fl, z = z0 + zl;
-        uint32_t wr[16], wi[16];
+        const int q = task & 3, fl = (task >> 2) % NF, zl = (task >> 2) / NF;
+        double2 n[4], s[4];
+        load(a, p, p.ct * NF + fl, 16 * (z0 + zl) + 4 * q, F, n, s);
         const double2 sr = scl[2 * fl], si = scl[2 * fl + 1];
-        const double2* src = F + (long long)(f < a.batch ? f : 0) * a.ldF + (long long)p.m * a.nlat;
-        const double sg = par ? -1.0 : 1.0;
+        double nr[4], sre[4], ni[4], sim[4];
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int j = 16 * z + i;
-            double2 n = make_double2(0.0, 0.0), s = make_double2(0.0, 0.0);
-            if (f < a.batch && j < a.nh) {
-                n = src[j];
-                s = src[a.nlat - 1 - j];
-            }
-            wr[i] = i8_word(n.x + sg * s.x, sr.x, sr.y);
-            wi[i] = i8_word(n.y + sg * s.y, si.x, si.y);
+        for (int i = 0; i < 4; i++) {
+            nr[i] = n[i].x * sr.x;
+            sre[i] = s[i].x * sr.x;
+            ni[i] = n[i].y * si.x;
+            sim[i] = s[i].y * si.x;
         }
-        uint4 pr[4], pi[4];
-        i8_planes(wr, pr);
-        i8_planes(wi, pi);
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-            uint4* row = reinterpret_cast<uint4*>(Bs + ((size_t)((par * li8::ND + d) * ZSEG + zl) * NC + 2 * fl) * 16);
-            row[0] = pr[d];
-            row[1] = pi[d];
-        }
+        auto w = [](double t, double s2) {
+            const uint32_t v = (uint32_t)__double2loint(fma(t, s2, 0x1.8p52));
+            return (v + 0x808080u) ^ 0x808080u;
+        };
+        uint32_t o[4];
+        i8_planes4(w(nr[0] + sre[0], sr.y), w(nr[1] + sre[1], sr.y), w(nr[2] + sre[2], sr.y), w(nr[3] + sre[3], sr.y), o);
+        i8_put<NC, ZSEG>(Bs, 0, zl, 2 * fl, q, o);
+        i8_planes4(w(ni[0] + sim[0], si.y), w(ni[1] + sim[1], si.y), w(ni[2] + sim[2], si.y), w(ni[3] + sim[3], si.y), o);
+        i8_put<NC, ZSEG>(Bs, 0, zl, 2 * fl + 1, q, o);
+        i8_planes4(w(nr[0] - sre[0], sr.y), w(nr[1] - sre[1], sr.y), w(nr[2] - sre[2], sr.y), w(nr[3] - sre[3], sr.y), o);
+        i8_put<NC, ZSEG>(Bs, 1, zl, 2 * fl, q, o);
+        i8_planes4(w(ni[0] - sim[0], si.y), w(ni[1] - sim[1], si.y), w(ni[2] - sim[2], si.y), w(ni[3] - sim[3], si.y), o);
+        i8_put<NC, ZSEG>(Bs, 1, zl, 2 * fl + 1, q, o);
     }
     // consumer: TMEM lane r = degree index l' = 128 rt + r of both parities
     __device__ static void epilogue(const I8Args& a, const I8Tile& p, int r, int c0, const int* ecol, const double* e,
@@ -435,8 +466,11 @@ __global__ void __launch_bounds__(li8::NT, 1) k_legendre_i8(const __grid_constan
         for (I8Tile p = first; p.t < a.ntiles && ok; p = i8_tile<Dir>(a, p.t + gridDim.x), j++) {
             if (tid < 64) colmax[tid] = 0ull;
             producers_sync_s();
-            const int ns = Dir::scan_tasks(p);
-            for (int task = tid; task < ns; task += li8::NPROD) Dir::scan(a, p, task, in, colmax);
+            const int ns = Dir::tasks(2 * p.nch), trips = i8_trips(ns);
+            for (int it = 0; it < trips; it++) {
+                const int task = tid + it * li8::NPROD;
+                Dir::scan(a, p, task, task < ns, in, colmax);
+            }
             // the exponent slot of this tile is free once the consumers have read tile j - 2's
             bool v = true;
             if (tid == 0 && j >= 2)
@@ -464,7 +498,7 @@ __global__ void __launch_bounds__(li8::NT, 1) k_legendre_i8(const __grid_constan
                 }
                 const int z0 = sg * ZSEG, nz = min(ZSEG, 2 * p.nch - z0);
                 unsigned char* Bs = smem + li8::OFF_B + slot * li8::B_SLOT;
-                const int nt = Dir::digit_tasks(nz);
+                const int nt = Dir::tasks(nz);
                 for (int task = tid; task < nt; task += li8::NPROD) Dir::digits(a, p, task, z0, in, scl, Bs);
                 fence_async_smem();
                 producers_sync_s();
@@ -636,8 +670,8 @@ __device__ __forceinline__ void i8_recurrence(double z, int m, int T, Put&& put)
     }
 }
 
-// row maxima: synthesis row (m, j) over all degrees -> esy; analysis row
-// (m, l) over the latitudes of |P w| -> amax (bit patterns, atomic max)
+// row maxima: synthesis row (m, j) over all degrees -> esy (null: skipped);
+// analysis row (m, l) over the latitudes of |P w| -> amax (bit patterns, atomic max)
 __global__ void k_i8_rowmax(int nh, int T, int mm, const double* __restrict__ x, const double* __restrict__ w,
                             int* __restrict__ esy, unsigned long long* __restrict__ amax) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x, m = blockIdx.y;
@@ -648,7 +682,7 @@ __global__ void k_i8_rowmax(int nh, int T, int mm, const double* __restrict__ x,
         smax = fmax(smax, fabs(v));
         atomicMax(&amax[pidx(T, l, m)], i8_bits(fabs(v * wj)));
     });
-    esy[(long long)m * nh + j] = i8_exp(smax);
+    if (esy) esy[(long long)m * nh + j] = i8_exp(smax);
 }
 
 __global__ void k_i8_anexp(long long n, const unsigned long long* __restrict__ amax, int* __restrict__ ean) {
@@ -656,7 +690,8 @@ __global__ void k_i8_anexp(long long n, const unsigned long long* __restrict__ a
     if (i < n) ean[i] = i8_exp(__longlong_as_double((long long)amax[i]));
 }
 
-// digit words of P (synthesis rows) and P w (analysis rows) into the two tables
+// digit words of P (synthesis rows, skipped when SY is null) and P w (analysis
+// rows) into the two tables
 __global__ void k_i8_tables(int nh, int nhP, int T, int mm, const double* __restrict__ x, const double* __restrict__ w,
                             const int* __restrict__ esy, const int* __restrict__ ean,
                             const long long* __restrict__ zoff, const long long* __restrict__ aoff, long long zS,
@@ -677,7 +712,7 @@ __global__ void k_i8_tables(int nh, int nhP, int T, int mm, const double* __rest
         const long long ia = ((long long)(j >> 4) * rowsA + (par ? a1 : a0) + lp) * 16 + (j & 15);
 #pragma unroll
         for (int dp = 0; dp < 4; dp++) {
-            SY[dp * plS + is] = (unsigned char)(ws >> (24 - 8 * dp));
+            if (SY) SY[dp * plS + is] = (unsigned char)(ws >> (24 - 8 * dp));
             AN[dp * plA + ia] = (unsigned char)(wa >> (24 - 8 * dp));
         }
     });

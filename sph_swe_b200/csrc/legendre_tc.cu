@@ -95,15 +95,17 @@ struct MixedTables {
     size_t Bcap = 0;
     // int8 digit tables of the integer-split kernels (legendre_i8.cuh)
     unsigned char* SY = nullptr;  // synthesis digit planes
-    unsigned char* AN = nullptr;  // analysis digit planes
+    unsigned char* AN = nullptr;  // analysis digit planes (P w)
+    unsigned char* ANc = nullptr; // analysis digit planes (P w / cos(phi))
     int* esy = nullptr;           // synthesis row exponents [m][j]
     int* ean = nullptr;           // analysis row exponents [pidx(lmax, l, m)]
+    int* eanc = nullptr;          // the same for ANc
     long long* i8zoff = nullptr;  // [m] first z of order m in SY
     long long* i8aoff = nullptr;  // [m] first row of order m in AN
     long long zSY = 0, rowsAN = 0;
     int zAN = 0;
     bool i8 = false;
-    CUtensorMap mapSY, mapAN;
+    CUtensorMap mapSY, mapAN, mapANc;
 };
 
 // Offsets of degree m's blocks in the coefficient and checkpoint tables of
@@ -412,7 +414,7 @@ void tc_tables_free(Handle* h) {
     MixedTables* T = static_cast<MixedTables*>(h->mixed);
     if (!T) return;
     void* bufs[] = {T->ab, T->ck,   T->ckx, T->flag,   T->S,      T->A,     T->soff,
-                    T->aoff, T->Bbuf, T->SY, T->AN, T->esy, T->ean, T->i8zoff, T->i8aoff};
+                    T->aoff, T->Bbuf, T->SY, T->AN, T->ANc, T->esy, T->ean, T->eanc, T->i8zoff, T->i8aoff};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete T;
@@ -1159,11 +1161,15 @@ static int i8_tables_build(Handle* h, MixedTables* T) {
     const size_t bs = (size_t)4 * T->zSY * nhP * 16, ba = (size_t)4 * T->zAN * T->rowsAN * 16;
     SPH_CUDA_TRY(cudaMalloc(&T->SY, bs));
     SPH_CUDA_TRY(cudaMalloc(&T->AN, ba));
+    SPH_CUDA_TRY(cudaMalloc(&T->ANc, ba));
     SPH_CUDA_TRY(cudaMemset(T->SY, 0, bs));
     SPH_CUDA_TRY(cudaMemset(T->AN, 0, ba));
+    SPH_CUDA_TRY(cudaMemset(T->ANc, 0, ba));
     SPH_CUDA_TRY(cudaMalloc(&T->esy, sizeof(int) * (size_t)(mm + 1) * nh));
     SPH_CUDA_TRY(cudaMalloc(&T->ean, sizeof(int) * (size_t)nlmT));
     SPH_CUDA_TRY(cudaMemset(T->ean, 0, sizeof(int) * (size_t)nlmT));
+    SPH_CUDA_TRY(cudaMalloc(&T->eanc, sizeof(int) * (size_t)nlmT));
+    SPH_CUDA_TRY(cudaMemset(T->eanc, 0, sizeof(int) * (size_t)nlmT));
     SPH_CUDA_TRY(cudaMalloc(&T->i8zoff, sizeof(long long) * (mm + 2)));
     SPH_CUDA_TRY(cudaMalloc(&T->i8aoff, sizeof(long long) * (mm + 2)));
     SPH_CUDA_TRY(cudaMemcpy(T->i8zoff, zo.data(), sizeof(long long) * (mm + 2), cudaMemcpyHostToDevice));
@@ -1173,10 +1179,20 @@ static int i8_tables_build(Handle* h, MixedTables* T) {
     cudaError_t e = cudaMemset(amax, 0, sizeof(unsigned long long) * (size_t)nlmT);
     const dim3 grid((nh + 127) / 128, mm + 1);
     if (e == cudaSuccess) {
+        // weights w: synthesis rows and the analysis table AN
         k_i8_rowmax<<<grid, 128>>>(nh, tl, mm, h->mu, h->w, T->esy, amax);
         k_i8_anexp<<<(unsigned)((nlmT + 255) / 256), 256>>>(nlmT, amax, T->ean);
         k_i8_tables<<<grid, 128>>>(nh, nhP, tl, mm, h->mu, h->w, T->esy, T->ean, T->i8zoff, T->i8aoff, T->zSY,
                                    T->rowsAN, T->zAN, T->SY, T->AN);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * (size_t)nlmT);
+    if (e == cudaSuccess) {
+        // weights w / cos(phi): the analysis table ANc only
+        k_i8_rowmax<<<grid, 128>>>(nh, tl, mm, h->mu, h->wc, nullptr, amax);
+        k_i8_anexp<<<(unsigned)((nlmT + 255) / 256), 256>>>(nlmT, amax, T->eanc);
+        k_i8_tables<<<grid, 128>>>(nh, nhP, tl, mm, h->mu, h->wc, T->esy, T->eanc, T->i8zoff, T->i8aoff, T->zSY,
+                                   T->rowsAN, T->zAN, nullptr, T->ANc);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }
@@ -1187,6 +1203,8 @@ static int i8_tables_build(Handle* h, MixedTables* T) {
     }
     if (int rc = encode_map_i8(&T->mapSY, T->SY, (unsigned long long)nhP, (unsigned long long)T->zSY)) return rc;
     if (int rc = encode_map_i8(&T->mapAN, T->AN, (unsigned long long)T->rowsAN, (unsigned long long)T->zAN)) return rc;
+    if (int rc = encode_map_i8(&T->mapANc, T->ANc, (unsigned long long)T->rowsAN, (unsigned long long)T->zAN))
+        return rc;
     T->i8 = true;
     return SPH_OK;
 }
@@ -1376,7 +1394,7 @@ int tc_reserve(const Handle* h, int batch) {
 
 template <int NC>
 static int tcb_launch_nc(const Handle* h, MixedTables* T, bool syn, TbArgs& a, const double2* in, long long ld_in,
-                         double2* out, cudaStream_t s) {
+                         double2* out, const double* wts, cudaStream_t s) {
     constexpr int PART = NC * tc::KC;
     const dim3 pb((PART + 255) / 256);
     if (syn) {
@@ -1385,7 +1403,7 @@ static int tcb_launch_nc(const Handle* h, MixedTables* T, bool syn, TbArgs& a, c
                                                                               T->Bbuf);
     } else {
         if ((long long)a.nm * a.nkA > 65535) { set_error("tensor-core Legendre stage: too many chunks"); return SPH_ERR_ARG; }
-        k_tcb_prep_ana<NC><<<dim3(pb.x, a.nm * a.nkA, a.nct), 256, 0, s>>>(in, ld_in, a.nlat, a.nh, a.nm, a.nkA, h->w,
+        k_tcb_prep_ana<NC><<<dim3(pb.x, a.nm * a.nkA, a.nct), 256, 0, s>>>(in, ld_in, a.nlat, a.nh, a.nm, a.nkA, wts,
                                                                           a.batch, T->Bbuf);
     }
     SPH_CUDA_TRY(cudaGetLastError());
@@ -1399,7 +1417,9 @@ static int tcb_launch_nc(const Handle* h, MixedTables* T, bool syn, TbArgs& a, c
 // loader-only kernel: prepare B, then run the contraction (in: spectra for
 // synthesis, Fourier data for analysis)
 static int tcb_launch(const Handle* h, const MixedTables* Tc, bool syn, int lmax, int batch, int nrt, int nm,
-                      const double2* in, long long ld_in, double2* out, long long ld_out, int var, cudaStream_t s) {
+                      const double2* in, long long ld_in, double2* out, long long ld_out, int var, cudaStream_t s,
+                      const double* wts = nullptr) {
+    if (!wts) wts = h->w;
     MixedTables* T = const_cast<MixedTables*>(Tc);
     const int nc = tc_cols_v(batch, var);
     TbArgs a;
@@ -1422,9 +1442,9 @@ static int tcb_launch(const Handle* h, const MixedTables* Tc, bool syn, int lmax
     a.flag = T->flag;
     if (int rc = tcb_ensure(T, tcb_bytes(h, syn, lmax, a.nct * nc), s)) return rc;
     a.B = T->Bbuf;
-    if (nc == 16) return tcb_launch_nc<16>(h, T, syn, a, in, ld_in, out, s);
-    if (nc == 32) return tcb_launch_nc<32>(h, T, syn, a, in, ld_in, out, s);
-    return tcb_launch_nc<64>(h, T, syn, a, in, ld_in, out, s);
+    if (nc == 16) return tcb_launch_nc<16>(h, T, syn, a, in, ld_in, out, wts, s);
+    if (nc == 32) return tcb_launch_nc<32>(h, T, syn, a, in, ld_in, out, wts, s);
+    return tcb_launch_nc<64>(h, T, syn, a, in, ld_in, out, wts, s);
 }
 
 // Variants of the tensor-core Legendre stages (the autotuner's numbers):
@@ -1499,24 +1519,28 @@ int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spe
 }
 
 int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec, int lmax,
-                         int batch, cudaStream_t s) {
+                         int batch, cudaStream_t s, int wmode) {
     const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
     if (int rc = check_tables(T, lmax)) return rc;
     if (batch <= 0) return SPH_OK;
     const int nrt = lmax / (2 * tc::M) + 1, nm = std::min(lmax, h->L) + 1;
     const int var = tune_get(h, TUNE_TC_ANALYSIS, batch, 0);
+    const double* wts = wmode ? h->wc : h->w;
     if (use_i8(T, var)) {
         I8Args a = make_i8args(h, T, false, lmax, batch, ld_spec, ldF, var);
-        return i8_launch<AnaI8>(T->mapAN, a, (i8_nlp(lmax, 0, 0) + li8::M - 1) / li8::M, F, spec,
+        if (wmode) a.erow = T->eanc;
+        return i8_launch<AnaI8>(wmode ? T->mapANc : T->mapAN, a, (i8_nlp(lmax, 0, 0) + li8::M - 1) / li8::M, F, spec,
                                 i8_cols_v(batch, var), s);
     }
     if (T->streamed && !(var & 4) && (var & 8))
-        return tcb_launch(h, T, false, lmax, batch, nrt, nm, F, ldF, spec, ld_spec, var, s);
+        return tcb_launch(h, T, false, lmax, batch, nrt, nm, F, ldF, spec, ld_spec, var, s, wts);
     if (T->streamed && !(var & 4)) {
         TsArgs a = make_sargs(h, T, lmax, batch, ld_spec, ldF);
+        a.w = wts;
         return tcs_launch<AnaS>(T->mapA, a, nrt, nm, F, spec, var, s);
     }
     TcArgs a = make_args(h, T, lmax, batch, ld_spec, ldF);
+    a.w = wts;
     return tc_launch<AnaDir>(a, nrt, nm, F, spec, var, s);
 }
 

@@ -71,6 +71,7 @@ struct RexiPlan {
     double2* FXY = nullptr;     // [2 npoles][2L+1][nlat]
     double2* Xs = nullptr;      // [8][nlm] real-layout spectra of the prep
     double2* Fs = nullptr;      // [4][L+1][nlat] Fourier buffers of the prep
+    double* glp = nullptr;      // [nlat] grad_lat(mu) projected to degree L, on the rings
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double* state = nullptr;
@@ -224,16 +225,52 @@ __global__ void __launch_bounds__(64) k_rexi_s0_vel(RexiDev d, const double2* __
 
 // Fourier-space factors of the non-Robert projections (per latitude j, times
 // 2 pi: synthesis -> analysis convention), c = sqrt(1 - mu^2):
-//   mode 0: x c     (the cos(phi) factor of div_lat, SPHOperatorsComplex.hpp:300-312)
-//   mode 1: x (1 - mu^2) / c   (grad_lat(mu) as a grid field, the Coriolis product)
-//   mode 2: x / c   (grad_lon, grad_lat of the per-pole phi)
-__global__ void k_s0_fscale(double2* __restrict__ F, long long n, int nlat, const double* __restrict__ mu, int mode) {
+//   mode 0: x c      (the cos(phi) factor of div_lat, SPHOperatorsComplex.hpp:300-312)
+//   mode 1: x glp_j  (the Coriolis product with grad_lat(mu); see glp below)
+//   mode 2: x / c    (grad_lon, grad_lat of the per-pole phi)
+__global__ void k_s0_fscale(double2* __restrict__ F, long long n, int nlat, const double* __restrict__ mu,
+                            const double* __restrict__ glp, int mode) {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n) return;
-    const double z = mu[idx % nlat];
-    const double c2 = (1.0 - z) * (1.0 + z), c = sqrt(c2);
-    const double f = 2.0 * kPi * (mode == 0 ? c : (mode == 1 ? c2 / c : 1.0 / c));
+    const int j = (int)(idx % nlat);
+    const double z = mu[j];
+    const double c = sqrt((1.0 - z) * (1.0 + z));
+    const double f = 2.0 * kPi * (mode == 0 ? c : (mode == 1 ? glp[j] : 1.0 / c));
     F[idx] = make_double2(F[idx].x * f, F[idx].y * f);
+}
+
+// grad_lat(mu) as the Coriolis product of SWERexiSPH::solve uses it
+// (SWERexiSPH.hpp:183-186): the grid field (1 - mu^2) / sqrt(1 - mu^2) is
+// multiplied by the scalar two_omega * ir first, which takes it to spectral
+// space (degree L) and back before the grid product, so the product sees its
+// degree-L projection, not cos(phi) itself.  The field is zonal: the
+// projection is the m = 0 Legendre analysis (Gauss weights, the 2 pi of the
+// longitude quadrature) and synthesis with the orthonormal P_l^0, on the host.
+static std::vector<double> s0_grad_lat_mu(const Handle* h) {
+    const int L = h->L, nlat = h->nlat;
+    std::vector<double> g0(nlat), out(nlat, 0.0), q(L + 1, 0.0);
+    std::vector<double> P((size_t)(L + 1) * nlat);
+    for (int j = 0; j < nlat; j++) {
+        const double z = h->mu_h[j];
+        g0[j] = (1.0 - z * z) / std::sqrt((1.0 - z) * (1.0 + z));
+        double p0 = std::sqrt(1.0 / (4.0 * kPi)), p1 = z * std::sqrt(3.0) * p0;
+        P[j] = p0;
+        if (L >= 1) P[(size_t)nlat + j] = p1;
+        for (int l = 2; l <= L; l++) {
+            const double dl = l;
+            const double al = std::sqrt((4.0 * dl * dl - 1.0) / (dl * dl));
+            const double bl = std::sqrt(((dl - 1.0) * (dl - 1.0)) / (4.0 * (dl - 1.0) * (dl - 1.0) - 1.0));
+            const double p2 = al * (z * p1 - bl * p0);
+            p0 = p1;
+            p1 = p2;
+            P[(size_t)l * nlat + j] = p2;
+        }
+    }
+    for (int l = 0; l <= L; l++)
+        for (int j = 0; j < nlat; j++) q[l] += h->w_h[j] * 2.0 * kPi * g0[j] * P[(size_t)l * nlat + j];
+    for (int l = 0; l <= L; l++)
+        for (int j = 0; j < nlat; j++) out[j] += q[l] * P[(size_t)l * nlat + j];
+    return out;
 }
 
 // div and eta of the non-Robert operators from the Fourier coefficients of
@@ -427,7 +464,7 @@ static int rexi_s0_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     auto blocks = [](long long n) { return (unsigned)((n + 255) / 256); };
     // w = F(I(v0) cos phi)
     if (int rc = legendre_synthesis_real(h, vv, nlm, L, R->Fs, ldF, 1, s)) return rc;
-    k_s0_fscale<<<blocks(ldF), 256, 0, s>>>(R->Fs, ldF, nlat, h->mu, 0);
+    k_s0_fscale<<<blocks(ldF), 256, 0, s>>>(R->Fs, ldF, nlat, h->mu, R->glp, 0);
     if (int rc = legendre_analysis_real(h, R->Fs, ldF, Xs(0), nlm, L, 1, s)) return rc;
     // i m u0, D w, i m v0, D u0 -> div, eta
     if (int rc = spec_op(h, SPH_OP_DIFF_LON, uu, nlm, Xs(1), nlm, one, zero, 1, 0, s)) return rc;
@@ -437,12 +474,12 @@ static int rexi_s0_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     if (int rc = legendre_synthesis_real(h, Xs(1), nlm, L, R->Fs, ldF, 4, s)) return rc;
     k_s0_fdiveta<<<blocks(ldF), 256, 0, s>>>(R->Fs, ldF, nlat, h->mu, h->lat);
     if (int rc = legendre_analysis_real(h, R->Fs, ldF, Xs(5), nlm, L, 2, s)) return rc;
-    // Coriolis products: G(x) = F(grad_lat(mu) I(x)) for x = u0, mu2 u0, mu v0
+    // Coriolis products: G(x) = F(glp I(x)) for x = u0, mu2 u0, mu v0
     if (int rc = spec_op(h, SPH_OP_SCALE, uu, nlm, Xs(1), nlm, one, zero, 1, 0, s)) return rc;
     if (int rc = spec_op(h, SPH_OP_MU2, uu, nlm, Xs(2), nlm, one, zero, 1, 0, s)) return rc;
     if (int rc = spec_op(h, SPH_OP_MU, vv, nlm, Xs(3), nlm, one, zero, 1, 0, s)) return rc;
     if (int rc = legendre_synthesis_real(h, Xs(1), nlm, L, R->Fs, ldF, 3, s)) return rc;
-    k_s0_fscale<<<blocks(3 * ldF), 256, 0, s>>>(R->Fs, 3 * ldF, nlat, h->mu, 1);
+    k_s0_fscale<<<blocks(3 * ldF), 256, 0, s>>>(R->Fs, 3 * ldF, nlat, h->mu, R->glp, 1);
     if (int rc = legendre_analysis_real(h, R->Fs, ldF, Xs(1), nlm, L, 3, s)) return rc;
     // complex promotions: 0 div0 = ir div, 14 eta0 = ir vort, 2 phi0 = g h, 10 u0, 11 v0, 7-9 the products
     k_rx_complexify<<<gc, 64, 0, s>>>(Xs(5), ir, Vs(0), L);
@@ -469,7 +506,7 @@ static int rexi_s0_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     // grad_lon(phi), grad_lat(phi) of every pole as spectra
     const int nf = 2 * R->npoles;
     if (int rc = legendre_synthesis_cplx(h, R->XY, nc, R->FXY, ldFc, nf, s)) return rc;
-    k_s0_fscale<<<blocks((long long)nf * ldFc), 256, 0, s>>>(R->FXY, (long long)nf * ldFc, nlat, h->mu, 2);
+    k_s0_fscale<<<blocks((long long)nf * ldFc), 256, 0, s>>>(R->FXY, (long long)nf * ldFc, nlat, h->mu, R->glp, 2);
     if (int rc = legendre_analysis_cplx(h, R->FXY, ldFc, R->XY, nc, nf, s)) return rc;
     // phase B: velocities, beta scaling, pole reduction
     RX_DISPATCH(k_rexi_s0_vel, d, nb, s, R->PH, R->XY);
@@ -548,7 +585,7 @@ static void rexi_free(RexiPlan* R) {
     if (R->exec) cudaGraphExecDestroy(R->exec);
     if (R->graph) cudaGraphDestroy(R->graph);
     void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V,  R->part, R->X,  R->Xr, R->F,
-                    R->flag,  R->fphi, R->fvel, R->pphi, R->pvel, R->PH, R->XY,   R->FXY, R->Xs, R->Fs};
+                    R->flag,  R->fphi, R->fvel, R->pphi, R->pvel, R->PH, R->XY,   R->FXY, R->Xs, R->Fs, R->glp};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete R;
@@ -661,6 +698,9 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
         RX_TRY(cudaMalloc(&R->Fs, sizeof(double2) * 4 * (size_t)(L + 1) * h->nlat));
         RX_TRY(cudaMemset(R->PH, 0, sizeof(double2) * (size_t)npoles * nc));
         RX_TRY(cudaMemset(R->XY, 0, sizeof(double2) * 2 * (size_t)npoles * nc));
+        const std::vector<double> glp = s0_grad_lat_mu(h);
+        RX_TRY(cudaMalloc(&R->glp, sizeof(double) * h->nlat));
+        RX_TRY(cudaMemcpy(R->glp, glp.data(), sizeof(double) * h->nlat, cudaMemcpyHostToDevice));
     }
     RX_TRY(cudaMemcpy(R->alpha, al.data(), sizeof(double2) * npoles, cudaMemcpyHostToDevice));
     RX_TRY(cudaMemcpy(R->beta, be.data(), sizeof(double2) * npoles, cudaMemcpyHostToDevice));

@@ -3,6 +3,8 @@
 // called from SPHConfig::setup / setupAutoPhysicalSpace, SPHConfig.hpp:324-399).
 #include "common.cuh"
 
+#include <vector>
+
 #include <cmath>
 #include <cstring>
 
@@ -130,6 +132,12 @@ int setup_tables(Handle* h) {
     SPH_CUDA_TRY(cudaMemcpy(h->w_h.data(), h->w, sizeof(double) * n, cudaMemcpyDeviceToHost));
     SPH_CUDA_TRY(cudaMemcpy(h->cosphi_h.data(), h->cosphi, sizeof(double) * n, cudaMemcpyDeviceToHost));
     SPH_CUDA_TRY(cudaMemcpy(h->lat_h.data(), h->lat, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    // Gauss weights over cos(phi): the weights of analyses whose input carries
+    // a factor cos(phi) that the integrand does not have (see legendre_analysis_real)
+    std::vector<double> wc(n);
+    for (int j = 0; j < n; j++) wc[j] = h->w_h[j] / h->cosphi_h[j];
+    SPH_CUDA_TRY(cudaMalloc(&h->wc, sizeof(double) * n));
+    SPH_CUDA_TRY(cudaMemcpy(h->wc, wc.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
     return SPH_OK;
 }
 

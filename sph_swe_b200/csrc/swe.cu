@@ -363,7 +363,8 @@ __global__ void k_vd_prep(const double2* __restrict__ S, const double2* __restri
     o[3 * (size_t)nlmp + k] = x_at(0, n);
 }
 
-// G4 per member [U, V, zeta, h] -> G5 [eta U / c^2, eta V / c^2, h U / c^2, h V / c^2, g h + (U^2 + V^2) / (2 c^2)]
+// G4 per member [U, V, zeta, h] -> G5 = c [eta U / c^2, eta V / c^2, h U / c^2, h V / c^2, g h + (U^2 + V^2) / (2 c^2)],
+// the five integrands times c for the analysis with the weights w / c (bounded at the polar rings)
 __global__ void k_vd_pointwise(const double* __restrict__ G4, double* __restrict__ G5, const double* __restrict__ mu,
                                const double* __restrict__ cosphi, int nlat, int nspat, double grav, double omega) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -374,13 +375,13 @@ __global__ void k_vd_pointwise(const double* __restrict__ G4, double* __restrict
     double* o = G5 + (size_t)mem * 5 * nspat + idx;
     const double U = g[0], V = g[(size_t)nspat], Z = g[2 * (size_t)nspat], H = g[3 * (size_t)nspat];
     const double c = cosphi[j];
-    const double ic2 = 1.0 / (c * c);
+    const double ic = 1.0 / c;
     const double eta = Z + 2.0 * omega * mu[j];
-    o[0] = eta * U * ic2;
-    o[(size_t)nspat] = eta * V * ic2;
-    o[2 * (size_t)nspat] = H * U * ic2;
-    o[3 * (size_t)nspat] = H * V * ic2;
-    o[4 * (size_t)nspat] = grav * H + 0.5 * (U * U + V * V) * ic2;
+    o[0] = eta * U * ic;
+    o[(size_t)nspat] = eta * V * ic;
+    o[2 * (size_t)nspat] = H * U * ic;
+    o[3 * (size_t)nspat] = H * V * ic;
+    o[4 * (size_t)nspat] = grav * H * c + 0.5 * (U * U + V * V) * ic;
 }
 
 // K_s = [h_t, zeta_t, delta_t] from the degree-(L+1) analyses A5 = [a(A), a(B), a(C), a(D), a(E)]
@@ -490,7 +491,7 @@ static int swe_stage_vd(Handle* h, RKState* r, const sph_swe_params* p, const do
                                                                       p->gravity, p->omega);
     SPH_CUDA_TRY(cudaGetLastError());
     if (int rc = ring_analysis_real(h, r->G9, h->nspat, r->F6, fou, mF, 5 * nmem, s)) return rc;
-    if (int rc = legendre_analysis_real(h, r->F6, fou, r->X6, nlmp, Lp, 5 * nmem, s)) return rc;
+    if (int rc = legendre_analysis_real(h, r->F6, fou, r->X6, nlmp, Lp, 5 * nmem, s, 1)) return rc;
     k_vd_stage_out<<<dim3((L + 1 + 63) / 64, L + 1, nmem), 64, 0, s>>>(S, Kp, coef, r->dts, r->X6, Ks, L, nlm, nlmp,
                                                                        p->radius, p->viscosity);
     SPH_CUDA_TRY(cudaGetLastError());

@@ -162,7 +162,7 @@ static int tune_load(Handle* h, const char* json) {
         if (!b || !v) break;
         batch = std::atoi(b + 8);
         var = std::atoi(v + 10);
-        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 31) {
+        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 127) {
             set_error("sph_tune_load: malformed entry");
             return SPH_ERR_ARG;
         }

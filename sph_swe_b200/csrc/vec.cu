@@ -5,7 +5,8 @@
 //   synthesis  psi = lap^-1 vort, chi = lap^-1 div
 //              U = u c = d chi/d lambda - (1-mu^2) d psi/d mu
 //              V = v c = d psi/d lambda + (1-mu^2) d chi/d mu
-//   analysis   with U' = U/c^2, V' = V/c^2 and a_l(.) the degree-(L+1) analysis,
+//   analysis   with U' = U/c^2, V' = V/c^2 and a_l(.) the degree-(L+1) analysis
+//              (taken as c U' under the weights w / c),
 //              vort_l = i m a_l(V') + (l+1) e_l a_{l-1}(U') - l e_{l+1} a_{l+1}(U')
 //              div_l  = i m a_l(U') - (l+1) e_l a_{l-1}(V') + l e_{l+1} a_{l+1}(V')
 //              (integration by parts of d/dmu; exact by Gauss quadrature)
@@ -151,10 +152,15 @@ int sph_vec_spat_to_SH(sph_handle* hh, const double* u, const double* v, double*
     // Fourier of u into fields 2b, of v into 2b+1
     if (int rc = ring_analysis_real(h, u, h->nspat, F, 2 * ldF, mF, batch, s)) return rc;
     if (int rc = ring_analysis_real(h, v, h->nspat, F + ldF, 2 * ldF, mF, batch, s)) return rc;
-    k_fourier_scale<<<dim3((unsigned)((ldF + 255) / 256), 2 * batch), 256, 0, s>>>(F, ldF, mF, h->nlat, h->cosphi,
-                                                                                    robert ? 2 : 1);
-    SPH_CUDA_TRY(cudaGetLastError());
-    if (int rc = legendre_analysis_real(h, F, ldF, A, nlmp, Lp, 2 * batch, s)) return rc;
+    // the integrands U' = U / c^2 are analysed with the weights w / c from
+    // c U' = U / c: u itself for velocities, U / c for the Robert form.  Both
+    // stay bounded at the polar rings, which keeps the per-column scales of the
+    // mixed form at the field's magnitude rather than at 1 / c there
+    if (robert) {
+        k_fourier_scale<<<dim3((unsigned)((ldF + 255) / 256), 2 * batch), 256, 0, s>>>(F, ldF, mF, h->nlat, h->cosphi, 1);
+        SPH_CUDA_TRY(cudaGetLastError());
+    }
+    if (int rc = legendre_analysis_real(h, F, ldF, A, nlmp, Lp, 2 * batch, s, 1)) return rc;
     k_vec_post<<<dim3((L + 1 + 63) / 64, L + 1, batch), 64, 0, s>>>(A, nlmp, reinterpret_cast<double2*>(vort),
                                                                    reinterpret_cast<double2*>(div), h->nlm, L);
     SPH_CUDA_TRY(cudaGetLastError());

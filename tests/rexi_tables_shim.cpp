@@ -110,6 +110,9 @@ extern "C" void shim_component(int L, int comp, double s_re, double s_im, double
         case 6: comp_z6robert(t, s, r); break;
         case 7: comp_z7(t, s, r); break;
         case 8: comp_z8(t, s, r); break;
+        case 14: comp_z4(t, s, r); break;
+        case 15: comp_z5(t, s, r); break;
+        case 16: comp_z6(t, s, r); break;
         default: break;
     }
     std::memcpy(out, (const void*)t.a.data(), sizeof(cd) * t.a.size());

@@ -161,4 +161,6 @@ def test_rexi_rejects_unsupported(gpu):
 
     s = Sph(15)
     with pytest.raises(capi.SphError):
-        s.rexi([1 + 1j], [1 + 0j], robert=0)
+        s.rexi([1 + 1j], [1 + 0j], tau=0.0)
+    with pytest.raises(capi.SphError):
+        s.rexi([1 + 1j], [1 + 0j], precision=7)

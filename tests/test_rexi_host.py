@@ -25,7 +25,8 @@ def shim():
     return lib
 
 
-COMPS = {2: "z2", 3: "z3", 4: "z4robert", 5: "z5robert", 6: "z6robert", 7: "z7", 8: "z8"}
+COMPS = {2: "z2", 3: "z3", 4: "z4robert", 5: "z5robert", 6: "z6robert", 7: "z7", 8: "z8",
+         14: "z4", 15: "z5", 16: "z6"}
 
 
 @pytest.mark.parametrize("fix", [0, 1])
