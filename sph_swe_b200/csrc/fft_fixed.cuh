@@ -2,21 +2,29 @@
 // grids use: 96, 192, 384, 768, 1536, 3072), used by fft.cu in place of the
 // generic kernels for those lengths.
 //
-// A CTA of 256 threads transforms P complex sequences (by default P = 8 up to
-// N = 768, i.e. 16 rings: every longitude row of the tile is one 128-byte run
-// of the theta-contiguous grid; P is a template parameter so that the
-// autotuner can trade tile width for CTAs per SM), i.e. 2P consecutive
-// latitude rings of one field packed in pairs (ring 2q real part, ring 2q+1
-// imaginary part).  Shared memory holds the tile element-major with the
-// sequences innermost, buf[i * P + q]: element i of all P sequences is the
-// 16 P bytes that longitude i of the 2P rings occupies in the grid, so the
-// grid tile is copied in (analysis) and out (synthesis) as 16-byte chunks
-// without rearrangement, by asynchronous copies (cp.async) on the way in.
-// The Stockham passes (radix 3 first, then 8, 4, 2; all radices and strides
-// compile-time) run in place in that one buffer, the sequence index fastest
-// across threads so that every quarter-warp touches one contiguous row: each
-// pass reads its butterfly inputs into registers, synchronises, and writes
-// the outputs, so only P * N * 16 bytes of shared memory are needed.
+// A CTA of 384 threads transforms P complex sequences (P = 8 up to N = 768,
+// i.e. 16 rings: every longitude row of the tile is one 128-byte run of the
+// theta-contiguous grid; P is a template parameter so that the autotuner can
+// trade tile width for CTAs per SM), i.e. 2P consecutive latitude rings of one
+// field packed in pairs (ring 2q real part, ring 2q+1 imaginary part).  Shared
+// memory holds the tile element-major with the sequences innermost,
+// buf[i * P + q]: element i of all P sequences is the 16 P bytes that
+// longitude i of the 2P rings occupies in the grid.
+//
+// Stockham passes, all radices and strides compile-time, the sequence index
+// fastest across threads so that every quarter-warp touches one contiguous
+// 128-byte row of shared memory.  Shared-memory traffic is what bounds these
+// kernels, so the schedule keeps the passes through shared memory few:
+//   analysis   radix 3 first, fused with the tile load (global -> registers ->
+//              butterfly -> shared memory; the first pass has no twiddles), then
+//              radix 16 passes (and one 2, 4 or 8); the last pass writes only
+//              the outputs the spectrum keeps (m <= L and N - m);
+//   synthesis  radix 16 passes (and one 2, 4 or 8) first, the first one
+//              reading only the nonzero Fourier rows (the rest are never
+//              written), then radix 3 last, fused with the tile store.
+// N = 768 takes 2 shared-memory passes (3 | 16 16) instead of 4 (3 8 8 4).
+// Twiddles of a radix-16 pass come from 4 table loads (w, w^2, w^4, w^8) and
+// products of them.
 #pragma once
 
 // needs FFTPlan / RingMap of fft.cu (included from there)
@@ -24,20 +32,10 @@
 namespace sphgpu {
 namespace fftx {
 
-constexpr int NT = 256;     // threads per CTA
-// default complex sequences per CTA (2 P real rings) and the padded row stride
+constexpr int NT = 384;     // threads per CTA
+// default complex sequences per CTA (2 P real rings)
 template <int N>
 constexpr int seqs() { return N <= 768 ? 8 : (N == 1536 ? 4 : 2); }
-
-// 16-byte asynchronous global -> shared copy; bytes = 0 writes zeros
-__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, int bytes) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -48,6 +46,11 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_doub
 template <int SIGN>
 __device__ __forceinline__ double2 mul_i(double2 a) {
     return SIGN < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+}
+// a * (c + SIGN i s)
+template <int SIGN>
+__device__ __forceinline__ double2 rot(double2 a, double c, double s) {
+    return make_double2(a.x * c - SIGN * s * a.y, a.y * c + SIGN * s * a.x);
 }
 
 template <int SIGN>
@@ -81,7 +84,6 @@ __device__ __forceinline__ void dft3(double2& a, double2& b, double2& c) {
 template <int SIGN>
 __device__ __forceinline__ void dft8(double2* v) {
     constexpr double h = 0.70710678118654752440084436210485;
-    // radix-2 over the halves: e_k = v_k + v_{k+4}, o_k = (v_k - v_{k+4}) w8^k
     double2 e[4], o[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -89,9 +91,9 @@ __device__ __forceinline__ void dft8(double2* v) {
         o[k] = csub(v[k], v[k + 4]);
     }
     // w8^1 = (h, SIGN h), w8^2 = SIGN i, w8^3 = (-h, SIGN h)
-    o[1] = make_double2(h * (o[1].x - SIGN * o[1].y), h * (o[1].y + SIGN * o[1].x));
+    o[1] = rot<SIGN>(o[1], h, h);
     o[2] = mul_i<SIGN>(o[2]);
-    o[3] = make_double2(-h * (o[3].x + SIGN * o[3].y), h * (SIGN * o[3].x - o[3].y));
+    o[3] = rot<SIGN>(o[3], -h, h);
     dft4<SIGN>(e[0], e[1], e[2], e[3]);
     dft4<SIGN>(o[0], o[1], o[2], o[3]);
 #pragma unroll
@@ -101,48 +103,129 @@ __device__ __forceinline__ void dft8(double2* v) {
     }
 }
 
+// v[0..15] in natural order -> DFT-16 in natural order: n = n2 + 4 n1,
+// k = k1 + 4 k2; DFT-4 over n1, twiddles w16^(n2 k1), DFT-4 over n2
+template <int SIGN>
+__device__ __forceinline__ void dft16(double2* v) {
+    constexpr double c1 = 0.92387953251128675612818318939679;  // cos(pi / 8)
+    constexpr double s1 = 0.38268343236508977172845998403040;  // sin(pi / 8)
+    constexpr double h = 0.70710678118654752440084436210485;
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) dft4<SIGN>(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
+    // v[n2 + 4 k1] *= w16^(n2 k1), w16 = exp(SIGN 2 pi i / 16)
+    v[5] = rot<SIGN>(v[5], c1, s1);     // w^1
+    v[9] = rot<SIGN>(v[9], h, h);       // w^2
+    v[13] = rot<SIGN>(v[13], s1, c1);   // w^3
+    v[6] = rot<SIGN>(v[6], h, h);       // w^2
+    v[10] = mul_i<SIGN>(v[10]);         // w^4
+    v[14] = rot<SIGN>(v[14], -h, h);    // w^6
+    v[7] = rot<SIGN>(v[7], s1, c1);     // w^3
+    v[11] = rot<SIGN>(v[11], -h, h);    // w^6
+    v[15] = rot<SIGN>(v[15], -c1, -s1); // w^9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) dft4<SIGN>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    // X[k1 + 4 k2] sits at v[4 k1 + k2]: transpose
+    double2 t[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) t[i] = v[i];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[4 * k1 + k2];
+}
+
 template <int R, int SIGN>
 __device__ __forceinline__ void dft(double2* v) {
     if constexpr (R == 2) dft2<SIGN>(v[0], v[1]);
     else if constexpr (R == 3) dft3<SIGN>(v[0], v[1], v[2]);
     else if constexpr (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
-    else dft8<SIGN>(v);
+    else if constexpr (R == 8) dft8<SIGN>(v);
+    else dft16<SIGN>(v);
 }
 
-// pass schedule of N = 3 * 2^k: radix 3, then 8s, then a 4 or a 2
-constexpr int pow2_part(int n) { return n % 3 == 0 ? n / 3 : n; }
-constexpr int radix_at(int N, int q) {
-    if (q == 0) return 3;
-    int m = pow2_part(N);
-    for (int i = 1; i < q; i++) m /= (m % 8 == 0 && m != 16 && m != 4 && m != 2) ? 8 : (m % 4 == 0 ? 4 : 2);
-    return (m % 8 == 0 && m != 16) ? 8 : (m % 4 == 0 ? 4 : 2);
+// twiddles w^(r b), r = 1..R-1, applied to v[r]; w = exp(SIGN 2 pi i / N) from
+// the table tw[t] = exp(-2 pi i t / N).  Radix 16 and 8 load w^b, w^2b, w^4b
+// (and w^8b) and form the other powers as products of at most four of them.
+template <int N, int R, int SIGN>
+__device__ __forceinline__ void twiddle(double2* v, int b, const double2* __restrict__ tw) {
+    auto ld = [&](int e) {
+        double2 w = __ldg(&tw[e % N]);
+        if (SIGN > 0) w.y = -w.y;
+        return w;
+    };
+    if constexpr (R == 2) {
+        v[1] = cmul(v[1], ld(b));
+    } else if constexpr (R == 3 || R == 4) {
+#pragma unroll
+        for (int r = 1; r < R; r++) v[r] = cmul(v[r], ld(r * b));
+    } else {
+        double2 p[R];
+        p[1] = ld(b);
+        p[2] = ld(2 * b);
+        p[4] = ld(4 * b);
+        p[3] = cmul(p[1], p[2]);
+        p[5] = cmul(p[1], p[4]);
+        p[6] = cmul(p[2], p[4]);
+        p[7] = cmul(p[3], p[4]);
+        if constexpr (R == 16) {
+            p[8] = ld(8 * b);
+#pragma unroll
+            for (int r = 9; r < 16; r++) p[r] = cmul(p[r - 8], p[8]);
+        }
+#pragma unroll
+        for (int r = 1; r < R; r++) v[r] = cmul(v[r], p[r]);
+    }
 }
-constexpr int npasses(int N) {
-    int m = pow2_part(N), q = 1;
-    while (m > 1) {
-        m /= (m % 8 == 0 && m != 16) ? 8 : (m % 4 == 0 ? 4 : 2);
+
+// pass schedules.  Power-of-two part M = N / 3 as radix 16s, then one 2, 4 or 8.
+constexpr int p2_count(int M) {
+    int q = 0;
+    while (M >= 16) {
+        M /= 16;
         q++;
     }
-    return q;
+    return q + (M > 1 ? 1 : 0);
 }
+constexpr int p2_radix(int M, int i) {
+    int q = 0;
+    while (M >= 16) {
+        if (q == i) return 16;
+        M /= 16;
+        q++;
+    }
+    return M;
+}
+constexpr int npasses(int N) { return 1 + p2_count(N / 3); }
+// DIR -1 (analysis): 3 first; +1 (synthesis): 3 last
+template <int DIR>
+constexpr int radix_at(int N, int q) {
+    if (DIR < 0) return q == 0 ? 3 : p2_radix(N / 3, q - 1);
+    return q == npasses(N) - 1 ? 3 : p2_radix(N / 3, q);
+}
+template <int DIR>
 constexpr int ls_at(int N, int q) {
     int ls = 1;
-    for (int i = 0; i < q; i++) ls *= radix_at(N, i);
+    for (int i = 0; i < q; i++) ls *= radix_at<DIR>(N, i);
     return ls;
 }
 
-// One Stockham pass on P sequences in place: butterflies t = (f, j), j < N/R,
-// inputs s[j + r N/R] times w^(r k N/(Ls R)), k = j mod Ls, outputs to
-// d[(j - k) R + k + r Ls]; w = exp(SIGN 2 pi i / N) from the table tw[t] = exp(-2 pi i t / N).
-// Element e of sequence f is buf[e * P + f]; f = t mod P.
-template <int N, int P, int Q, int SIGN>
-__device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ tw) {
-    constexpr int R = radix_at(N, Q);
-    constexpr int Ls = ls_at(N, Q);
+// One Stockham pass through shared memory on P sequences, in place: butterflies
+// t = (f, j), j < N/R, inputs s[j + r N/R] times w^(r k N/(Ls R)), k = j mod Ls,
+// outputs to d[(j - k) R + k + r Ls].  Element e of sequence f is buf[e * P + f].
+// Every thread holds at most 16 complex values across the barrier.
+//   ZMASK (first synthesis pass): elements mm < e < N - mm were never written
+//         and read as zeros;
+//   WMASK (last analysis pass, k = j): only outputs e <= mm or e >= N - mm
+//         are written.
+template <int N, int P, int Q, int SIGN, int DIR, bool ZMASK, bool WMASK>
+__device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ tw, int mm) {
+    constexpr int R = radix_at<DIR>(N, Q);
+    constexpr int Ls = ls_at<DIR>(N, Q);
     constexpr int NR = N / R;
     constexpr int TOT = P * NR;
     constexpr int IT = (TOT + NT - 1) / NT;
     constexpr int TS = N / (Ls * R);
+    static_assert(IT * R <= 16, "at most 16 complex values per thread");
     double2 v[IT][R];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
@@ -150,13 +233,12 @@ __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ t
         if (TOT % NT == 0 || t < TOT) {
             const int f = t % P, j = t / P, k = j % Ls;
             const double2* s = buf + f;
-            v[it][0] = s[j * P];
 #pragma unroll
-            for (int r = 1; r < R; r++) {
-                double2 w = __ldg(&tw[(r * k * TS) % N]);
-                if (SIGN > 0) w.y = -w.y;
-                v[it][r] = cmul(s[(j + r * NR) * P], w);
+            for (int r = 0; r < R; r++) {
+                const int e = j + r * NR;
+                v[it][r] = (!ZMASK || e <= mm || e >= N - mm) ? s[e * P] : make_double2(0, 0);
             }
+            if constexpr (Ls > 1) twiddle<N, R, SIGN>(v[it], k * TS, tw);
             dft<R, SIGN>(v[it]);
         }
     }
@@ -168,17 +250,23 @@ __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ t
             const int f = t % P, j = t / P, k = j % Ls;
             double2* d = buf + ((j - k) * R + k) * P + f;
 #pragma unroll
-            for (int r = 0; r < R; r++) d[r * Ls * P] = v[it][r];
+            for (int r = 0; r < R; r++) {
+                const int e = (j - k) * R + k + r * Ls;
+                if (!WMASK || e <= mm || e >= N - mm) d[r * Ls * P] = v[it][r];
+            }
         }
     }
     __syncthreads();
 }
 
-template <int N, int P, int Q, int SIGN>
-__device__ __forceinline__ void passes(double2* buf, const double2* __restrict__ tw) {
-    if constexpr (Q < npasses(N)) {
-        pass<N, P, Q, SIGN>(buf, tw);
-        passes<N, P, Q + 1, SIGN>(buf, tw);
+// the shared-memory passes Q .. QE-1
+template <int N, int P, int Q, int QE, int SIGN, int DIR>
+__device__ __forceinline__ void passes(double2* buf, const double2* __restrict__ tw, int mm) {
+    if constexpr (Q < QE) {
+        constexpr bool zm = DIR > 0 && Q == 0;
+        constexpr bool wm = DIR < 0 && Q == npasses(N) - 1;
+        pass<N, P, Q, SIGN, DIR, zm, wm>(buf, tw, mm);
+        passes<N, P, Q + 1, QE, SIGN, DIR>(buf, tw, mm);
     }
 }
 
@@ -189,46 +277,49 @@ namespace sphgpu {
 
 // grid tile (2P rings, pairs packed) -> F[b][m][j], m = 0..mF-1 (m > L zero),
 // scaled by 2 pi / N (quadrature weight in longitude).  vec != 0: nlat even and
-// the field rows 16-byte aligned, so each (longitude, ring pair) is one
-// aligned 16-byte chunk copied by cp.async.
+// the field rows 16-byte aligned, so each (longitude, ring pair) is one aligned
+// 16-byte load.
 template <int N, int P>
-__global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const double* __restrict__ spat, long long ld_spat,
+__global__ void __launch_bounds__(fftx::NT, 1) k_ring_analysis_real_n(const double* __restrict__ spat, long long ld_spat,
                                                                     double2* __restrict__ F, long long ldF, int mF, int L,
                                                                     int nlat, const double2* __restrict__ tw, int vec) {
-    constexpr int JT = 2 * P;
+    constexpr int JT = 2 * P, N3 = N / 3, TOT = P * N3;
+    constexpr int U = 3;  // radix-3 butterflies whose loads are in flight together
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
     const double* src = spat + (long long)blockIdx.y * ld_spat;
-    if (vec) {
-        for (int idx = threadIdx.x; idx < N * P; idx += fftx::NT) {
-            const int i = idx / P, j = j0 + 2 * (idx % P);
-            const bool in = j < nlat;
-            fftx::cp_async16(&fbuf[idx], src + (long long)i * nlat + (in ? j : 0), in ? 16 : 0);
-        }
-        fftx::cp_async_wait_all();
-    } else {
-        // tile load in batches of U independent loads per thread
-        constexpr int PER = N * JT / fftx::NT;
-        constexpr int U = PER <= 12 ? PER : 8;
-        static_assert((N * JT) % fftx::NT == 0 && PER % U == 0, "tile divides into batches");
-        for (int base = 0; base < N * JT; base += U * fftx::NT) {
-            double v[U];
+    const int mk = min(mF - 1, L);  // the last pass writes elements m <= mk and N - m
+    // first pass (radix 3, Ls = 1: no twiddles) straight from the grid:
+    // butterfly (f, j) reads longitudes j, j + N/3, j + 2N/3 of ring pair f and
+    // writes elements 3j, 3j + 1, 3j + 2
+    for (int base = threadIdx.x; base < TOT; base += U * fftx::NT) {
+        double2 x[U][3];
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int idx = base + threadIdx.x + u * fftx::NT;
-                const int i = idx / JT, j = j0 + idx % JT;
-                v[u] = (j < nlat) ? __ldg(&src[(long long)i * nlat + j]) : 0.0;
+        for (int u = 0; u < U; u++) {
+            const int t = base + u * fftx::NT;
+            const int f = t % P, j = t / P, jr = j0 + 2 * f;
+            const bool in = t < TOT && jr < nlat;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const double* p = src + (long long)(j + r * N3) * nlat + jr;
+                if (!in) x[u][r] = make_double2(0, 0);
+                else if (vec) x[u][r] = __ldg(reinterpret_cast<const double2*>(p));
+                else x[u][r] = make_double2(__ldg(p), jr + 1 < nlat ? __ldg(p + 1) : 0.0);
             }
+        }
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int idx = base + threadIdx.x + u * fftx::NT;
-                const int i = idx / JT, jj = idx % JT;
-                reinterpret_cast<double*>(&fbuf[i * P + (jj >> 1)])[jj & 1] = v[u];
+        for (int u = 0; u < U; u++) {
+            const int t = base + u * fftx::NT;
+            if (TOT % (U * fftx::NT) == 0 || t < TOT) {
+                const int f = t % P, j = t / P;
+                fftx::dft3<-1>(x[u][0], x[u][1], x[u][2]);
+#pragma unroll
+                for (int r = 0; r < 3; r++) fbuf[(3 * j + r) * P + f] = x[u][r];
             }
         }
     }
     __syncthreads();
-    fftx::passes<N, P, 0, -1>(fbuf, tw);
+    fftx::passes<N, P, 1, fftx::npasses(N), -1, -1>(fbuf, tw, mk);
     const double scale = 2.0 * kPi / N;
     double2* out = F + (long long)blockIdx.y * ldF;
     for (int idx = threadIdx.x; idx < mF * P; idx += fftx::NT) {
@@ -250,11 +341,12 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_analysis_real_n(const doub
 // F[fs][m][j] (optionally times i*m) -> grid k; m = 0 contributes its real part.
 // vec != 0: nlat even and the field rows 16-byte aligned (16-byte stores).
 template <int N, int P>
-__global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const double2* __restrict__ F, long long ldF, int mF,
+__global__ void __launch_bounds__(fftx::NT, 1) k_ring_synthesis_real_n(const double2* __restrict__ F, long long ldF, int mF,
                                                                      int L, double* __restrict__ spat, long long ld_spat,
                                                                      int nlat, const double2* __restrict__ tw,
                                                                      RingMap map, int vec) {
-    constexpr int JT = 2 * P;
+    constexpr int JT = 2 * P, N3 = N / 3, TOT = P * N3;
+    constexpr int U = 3;
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
     const int k = blockIdx.y;
@@ -266,14 +358,14 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const dou
     }
     const double2* in = F + (long long)fs * ldF;
     const int mm = min(min(mF - 1, L), (N - 1) / 2);
-    // rows mm+1 .. N-mm-1 are zero; rows 0..mm and N-mm..N-1 are written below
-    for (int idx = (mm + 1) * P + threadIdx.x; idx < (N - mm) * P; idx += fftx::NT) fbuf[idx] = make_double2(0, 0);
-    constexpr int U = 8;
+    // rows 0..mm and N-mm..N-1; the rows between are never written (the first
+    // pass reads them as zeros)
+    constexpr int UL = 8;
     const int tot = (mm + 1) * P;
-    for (int base = threadIdx.x; base < tot; base += U * fftx::NT) {
-        double2 X[U], Y[U];
+    for (int base = threadIdx.x; base < tot; base += UL * fftx::NT) {
+        double2 X[UL], Y[UL];
 #pragma unroll
-        for (int u = 0; u < U; u++) {
+        for (int u = 0; u < UL; u++) {
             const int idx = base + u * fftx::NT;
             const int m = idx / P, j = j0 + 2 * (idx % P);
             X[u] = Y[u] = make_double2(0, 0);
@@ -281,7 +373,7 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const dou
             if (idx < tot && j + 1 < nlat) Y[u] = __ldg(&in[(long long)m * nlat + j + 1]);
         }
 #pragma unroll
-        for (int u = 0; u < U; u++) {
+        for (int u = 0; u < UL; u++) {
             const int idx = base + u * fftx::NT;
             if (idx >= tot) break;
             const int m = idx / P, q = idx % P;
@@ -299,21 +391,41 @@ __global__ void __launch_bounds__(fftx::NT, 2) k_ring_synthesis_real_n(const dou
         }
     }
     __syncthreads();
-    fftx::passes<N, P, 0, +1>(fbuf, tw);
+    constexpr int NP = fftx::npasses(N);
+    fftx::passes<N, P, 0, NP - 1, +1, +1>(fbuf, tw, mm);
+    // last pass (radix 3, Ls = N/3, k = j) straight to the grid: butterfly
+    // (f, j) reads elements j, j + N/3, j + 2N/3 and writes longitudes
+    // j, j + N/3, j + 2N/3 of ring pair f
     double* out = spat + (long long)k * ld_spat;
-    if (vec) {
-#pragma unroll 8
-        for (int idx = threadIdx.x; idx < N * P; idx += fftx::NT) {
-            const int i = idx / P, j = j0 + 2 * (idx % P);
-            if (j < nlat) *reinterpret_cast<double2*>(&out[(long long)i * nlat + j]) = fbuf[idx];
+    for (int base = threadIdx.x; base < TOT; base += U * fftx::NT) {
+        double2 x[U][3];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int t = base + u * fftx::NT;
+            if (TOT % (U * fftx::NT) == 0 || t < TOT) {
+                const int f = t % P, j = t / P;
+#pragma unroll
+                for (int r = 0; r < 3; r++) x[u][r] = fbuf[(j + r * N3) * P + f];
+                fftx::twiddle<N, 3, +1>(x[u], j, tw);
+                fftx::dft3<+1>(x[u][0], x[u][1], x[u][2]);
+            }
         }
-    } else {
-#pragma unroll 8
-        for (int idx = threadIdx.x; idx < N * JT; idx += fftx::NT) {
-            const int i = idx / JT, jj = idx % JT;
-            const int j = j0 + jj;
-            const double2 z = fbuf[i * P + (jj >> 1)];
-            if (j < nlat) out[(long long)i * nlat + j] = (jj & 1) ? z.y : z.x;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int t = base + u * fftx::NT;
+            const int f = t % P, j = t / P, jr = j0 + 2 * f;
+            if ((TOT % (U * fftx::NT) == 0 || t < TOT) && jr < nlat) {
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    double* p = out + (long long)(j + r * N3) * nlat + jr;
+                    if (vec) {
+                        *reinterpret_cast<double2*>(p) = x[u][r];
+                    } else {
+                        p[0] = x[u][r].x;
+                        if (jr + 1 < nlat) p[1] = x[u][r].y;
+                    }
+                }
+            }
         }
     }
 }

@@ -409,10 +409,11 @@ __global__ void k_zero_top(double2* spec, long long ld, int lmax, int batch) {
     if (f < batch) spec[(long long)f * ld + pidx(lmax, lmax, lmax)] = make_double2(0, 0);
 }
 
+// nm_only > 0: the first nm_only orders m only
 static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double2* F, long long ldF, int batch,
-                        cudaStream_t s) {
+                        cudaStream_t s, int nm_only = 0) {
     if (batch <= 0) return SPH_OK;
-    const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
+    const int nm = nm_only > 0 ? nm_only : (sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1);
     if (batch > 16) {
         dim3 grid((h->nh + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
         k_legendre_synthesis_w<<<grid, WNT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
@@ -472,11 +473,13 @@ int legendre_kernels_init() {
 }
 
 int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
-                            long long ldF, int batch, cudaStream_t s) {
-    // mixed handles: the tensor-core kernels unless the autotuner found the FP64 kernel faster (variant bit 16)
-    if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_SYNTHESIS, batch, 0) & 16))
-        return legendre_synthesis_tc(h, spec, ld_spec, lmax, F, ldF, batch, s);
+                            long long ldF, int batch, cudaStream_t s, int exact_m0, int nobuf) {
     SpecMap sm{0, lmax, h->L, ld_spec};
+    // mixed handles: the tensor-core kernels unless the autotuner found the FP64 kernel faster (variant bit 16)
+    if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_SYNTHESIS, batch, 0) & 16)) {
+        if (int rc = legendre_synthesis_tc(h, spec, ld_spec, lmax, F, ldF, batch, s, nobuf)) return rc;
+        return exact_m0 ? launch_synth(h, spec, sm, F, ldF, batch, s, 1) : SPH_OK;
+    }
     return launch_synth(h, spec, sm, F, ldF, batch, s);
 }
 

@@ -70,6 +70,18 @@ static_assert(OFF_B % 1024 == 0 && B_SLOT % 1024 == 0 && OFF_MAX % 16 == 0, "ali
 // degrees of one parity of order m up to degree T, 32-degree chunks of parity 0
 __host__ __device__ inline int i8_nlp(int T, int m, int par) { return T - m - par >= 0 ? (T - m - par) / 2 + 1 : 0; }
 __host__ __device__ inline int i8_nch(int T, int m) { return (i8_nlp(T, m, 0) + li8::KC - 1) / li8::KC; }
+// prepared-B chunks (kernels with both operands by TMA, legendre_i8b.cuh):
+// synthesis chunks of the orders below m (degree lmax), sum_{m' < m} ((lmax - m') / 64 + 1)
+__host__ __device__ inline long long i8b_syn_coff(int lmax, int m) {
+    auto fs = [](int n) -> long long {  // sum_{x = 0..n} floor(x / 64)
+        if (n < 0) return 0;
+        const long long q = n / 64, r = n % 64;
+        return 32 * q * (q - 1) + q * (r + 1);
+    };
+    return (long long)m + fs(lmax) - fs(lmax - m);
+}
+// analysis chunks of one order: the latitudes of one hemisphere in steps of 32
+__host__ __device__ inline int i8b_ana_nch(int nh) { return (nh + li8::KC - 1) / li8::KC; }
 
 // instruction descriptor: D = S32, A = B = S8, both K-major, M x N
 __host__ __device__ constexpr uint32_t idesc_s8(int m, int n) {
@@ -155,6 +167,9 @@ __device__ __forceinline__ void i8_put(unsigned char* Bs, int par, int zl, int c
 
 struct I8Args {
     const int* erow;        // row exponents: synthesis esy[m * nh + j]; analysis ean[pidx(tlmax, l, m)]
+    unsigned char* B;       // prepared B chunks (kernels with both operands by TMA)
+    int* ecol;              // their column exponents [ct][m][NC]
+    long long cpt;          // B chunks per column tile
     const long long* zoff;  // synthesis table: first z of order m
     const long long* aoff;  // analysis table: first row of order m
     int tlmax, lmax, nh, nlat, batch;
@@ -199,6 +214,9 @@ struct SynI8 {
     static constexpr int KSEG = li8::B_SLOT / (2 * li8::ND * NC);  // K per B segment
     static constexpr int ZSEG = KSEG / 16;
     __device__ static int nch(const I8Args& a, int m, int) { return (i8_nlp(a.lmax, m, 0) + li8::KC - 1) / li8::KC; }
+    // prepared B: chunks of order m and their first chunk within the column tile
+    __device__ static int prep_nch(const I8Args& a, int m) { return nch(a, m, 0); }
+    __device__ static long long prep_coff(const I8Args& a, int m) { return i8b_syn_coff(a.lmax, m); }
     __device__ static int3 box(const I8Args& a, const I8Tile& p, int kc, int par) {
         const long long z = a.zoff[p.m] + (long long)par * 2 * i8_nch(a.tlmax, p.m) + 2 * kc;
         return make_int3(0, 2 * p.rt, (int)z);
@@ -230,9 +248,11 @@ struct SynI8 {
         }
         i8_colmax(mr, mi, live && q == 0, fl, colmax);
     }
-    // pass 2: the digit planes of 4 K indices of both parities, both columns
+    // pass 2: the digit planes of 4 K indices of both parities, both columns,
+    // handed to put(parity, z group, column, lane q, plane words)
+    template <class Put>
     __device__ static void digits(const I8Args& a, const I8Tile& p, int task, int z0, const double2* __restrict__ spec,
-                                  const double2* scl, unsigned char* Bs) {
+                                  const double2* scl, Put&& put) {
         const int q = task & 3, fl = (task >> 2) % NF, zl = (task >> 2) / NF;
         double2 v[8];
         load(a, p, p.ct * NF + fl, 16 * (z0 + zl) + 4 * q, spec, v);
@@ -242,10 +262,10 @@ struct SynI8 {
             uint32_t o[4];
             i8_planes4(i8_word(v[par].x, sr.x, sr.y), i8_word(v[2 + par].x, sr.x, sr.y),
                        i8_word(v[4 + par].x, sr.x, sr.y), i8_word(v[6 + par].x, sr.x, sr.y), o);
-            i8_put<NC, ZSEG>(Bs, par, zl, 2 * fl, q, o);
+            put(par, zl, 2 * fl, q, o);
             i8_planes4(i8_word(v[par].y, si.x, si.y), i8_word(v[2 + par].y, si.x, si.y),
                        i8_word(v[4 + par].y, si.x, si.y), i8_word(v[6 + par].y, si.x, si.y), o);
-            i8_put<NC, ZSEG>(Bs, par, zl, 2 * fl + 1, q, o);
+            put(par, zl, 2 * fl + 1, q, o);
         }
     }
     // consumer: TMEM lane r = latitude 128 rt + r; e, o: 8 columns of parity 0 / 1
@@ -277,6 +297,8 @@ struct AnaI8 {
     __device__ static int nch(const I8Args& a, int m, int rt) {
         return li8::M * rt < i8_nlp(a.lmax, m, 0) ? (a.nh + li8::KC - 1) / li8::KC : 0;
     }
+    __device__ static int prep_nch(const I8Args& a, int) { return i8b_ana_nch(a.nh); }
+    __device__ static long long prep_coff(const I8Args& a, int m) { return (long long)m * i8b_ana_nch(a.nh); }
     __device__ static int3 box(const I8Args& a, const I8Tile& p, int kc, int par) {
         const long long y = a.aoff[p.m] + (long long)par * tcs_pad64(i8_nlp(a.tlmax, p.m, 0)) + li8::M * p.rt;
         return make_int3(0, (int)(y >> 6), 2 * kc);
@@ -312,8 +334,9 @@ struct AnaI8 {
     // pass 2: digits of north + south (parity 0) and north - south (parity 1)
     // of 4 latitudes, both columns; the scale is applied to north and south
     // first (exact), so the sum is rounded once, as (north +/- south) would be
+    template <class Put>
     __device__ static void digits(const I8Args& a, const I8Tile& p, int task, int z0, const double2* __restrict__ F,
-                                  const double2* scl, unsigned char* Bs) {
+                                  const double2* scl, Put&& put) {
         const int q = task & 3, fl = (task >> 2) % NF, zl = (task >> 2) / NF;
         double2 n[4], s[4];
         load(a, p, p.ct * NF + fl, 16 * (z0 + zl) + 4 * q, F, n, s);
@@ -332,13 +355,13 @@ struct AnaI8 {
         };
         uint32_t o[4];
         i8_planes4(w(nr[0] + sre[0], sr.y), w(nr[1] + sre[1], sr.y), w(nr[2] + sre[2], sr.y), w(nr[3] + sre[3], sr.y), o);
-        i8_put<NC, ZSEG>(Bs, 0, zl, 2 * fl, q, o);
+        put(0, zl, 2 * fl, q, o);
         i8_planes4(w(ni[0] + sim[0], si.y), w(ni[1] + sim[1], si.y), w(ni[2] + sim[2], si.y), w(ni[3] + sim[3], si.y), o);
-        i8_put<NC, ZSEG>(Bs, 0, zl, 2 * fl + 1, q, o);
+        put(0, zl, 2 * fl + 1, q, o);
         i8_planes4(w(nr[0] - sre[0], sr.y), w(nr[1] - sre[1], sr.y), w(nr[2] - sre[2], sr.y), w(nr[3] - sre[3], sr.y), o);
-        i8_put<NC, ZSEG>(Bs, 1, zl, 2 * fl, q, o);
+        put(1, zl, 2 * fl, q, o);
         i8_planes4(w(ni[0] - sim[0], si.y), w(ni[1] - sim[1], si.y), w(ni[2] - sim[2], si.y), w(ni[3] - sim[3], si.y), o);
-        i8_put<NC, ZSEG>(Bs, 1, zl, 2 * fl + 1, q, o);
+        put(1, zl, 2 * fl + 1, q, o);
     }
     // consumer: TMEM lane r = degree index l' = 128 rt + r of both parities
     __device__ static void epilogue(const I8Args& a, const I8Tile& p, int r, int c0, const int* ecol, const double* e,
@@ -499,7 +522,10 @@ __global__ void __launch_bounds__(li8::NT, 1) k_legendre_i8(const __grid_constan
                 const int z0 = sg * ZSEG, nz = min(ZSEG, 2 * p.nch - z0);
                 unsigned char* Bs = smem + li8::OFF_B + slot * li8::B_SLOT;
                 const int nt = Dir::tasks(nz);
-                for (int task = tid; task < nt; task += li8::NPROD) Dir::digits(a, p, task, z0, in, scl, Bs);
+                auto put = [Bs](int par, int zl, int c, int q, const uint32_t* o) {
+                    i8_put<NC, ZSEG>(Bs, par, zl, c, q, o);
+                };
+                for (int task = tid; task < nt; task += li8::NPROD) Dir::digits(a, p, task, z0, in, scl, put);
                 fence_async_smem();
                 producers_sync_s();
                 if (tid == 0) mbar_arrive(smem_u32(&bfull[slot]));

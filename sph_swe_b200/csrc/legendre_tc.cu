@@ -91,8 +91,13 @@ struct MixedTables {
     bool streamed = false;
     CUtensorMap mapS, mapA;
     // B operand prepared by the loader-only kernel (legendre_tcb.cuh)
+    // (also the prepared B chunks and column exponents of the int8 kernels with
+    // both operands by TMA, legendre_i8b.cuh)
     float* Bbuf = nullptr;
     size_t Bcap = 0;
+    // buffers replaced by larger ones: a captured graph may still hold their
+    // addresses, so they live until the tables are freed
+    std::vector<void*> retired;
     // int8 digit tables of the integer-split kernels (legendre_i8.cuh)
     unsigned char* SY = nullptr;  // synthesis digit planes
     unsigned char* AN = nullptr;  // analysis digit planes (P w)
@@ -417,6 +422,7 @@ void tc_tables_free(Handle* h) {
                     T->aoff, T->Bbuf, T->SY, T->AN, T->ANc, T->esy, T->ean, T->eanc, T->i8zoff, T->i8aoff};
     for (void* p : bufs)
         if (p) cudaFree(p);
+    for (void* p : T->retired) cudaFree(p);
     delete T;
     h->mixed = nullptr;
 }
@@ -1060,6 +1066,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_legendre_tc(TcArgs a, const doubl
 #include "legendre_tcs.cuh"
 #include "legendre_tcb.cuh"
 #include "legendre_i8.cuh"
+#include "legendre_i8b.cuh"
 
 // rows: padded row count (a multiple of 64), slices: z extent
 static int encode_map(CUtensorMap* map, float* base, unsigned long long rows, unsigned long long slices) {
@@ -1228,6 +1235,13 @@ static int tc_attr() {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, li8::BYTES));
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8<AnaI8<NC>, NC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, li8::BYTES));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8b<SynI8<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8b::BYTES));
+    SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8b<AnaI8<NC>, NC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8b::BYTES));
+    cudaFuncAttributes fa;  // load the preparation kernels now (lazy module loading)
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep<SynI8<NC>, NC>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep<AnaI8<NC>, NC>));
     return SPH_OK;
 }
 
@@ -1344,6 +1358,13 @@ static size_t tcb_bytes(const Handle* h, bool syn, int lmax, int cols) {
     return (size_t)chunks * (size_t)cols * tc::KC * 4 * sizeof(float);
 }
 
+// bytes of the prepared B chunks and column exponents of an int8 call
+static size_t i8b_bytes(const Handle* h, bool syn, int lmax, int nct, int nc) {
+    const int nm = std::min(lmax, h->L) + 1;
+    const long long cpt = syn ? i8b_syn_coff(lmax, nm) : (long long)nm * i8b_ana_nch(h->nh);
+    return (size_t)nct * (size_t)cpt * i8b_chunk(nc) + (size_t)nct * nm * nc * sizeof(int);
+}
+
 // grow the B buffer; inside a stream capture it must already be large enough
 static int tcb_ensure(MixedTables* T, size_t bytes, cudaStream_t s) {
     if (bytes <= T->Bcap) return SPH_OK;
@@ -1353,13 +1374,12 @@ static int tcb_ensure(MixedTables* T, size_t bytes, cudaStream_t s) {
         set_error("tensor-core Legendre stage: operand workspace not reserved before stream capture");
         return SPH_ERR_ARG;
     }
-    if (T->Bbuf) {
-        SPH_CUDA_TRY(cudaDeviceSynchronize());
-        cudaFree(T->Bbuf);
-        T->Bbuf = nullptr;
-        T->Bcap = 0;
-    }
-    SPH_CUDA_TRY(cudaMalloc(&T->Bbuf, bytes));
+    // the old buffer is retired, not freed: work in flight and graphs captured
+    // earlier may still use it
+    float* nb = nullptr;
+    SPH_CUDA_TRY(cudaMalloc(&nb, bytes));
+    if (T->Bbuf) T->retired.push_back(T->Bbuf);
+    T->Bbuf = nb;
     T->Bcap = bytes;
     return SPH_OK;
 }
@@ -1379,17 +1399,25 @@ bool tc_synthesis_needs_alloc(const Handle* h, int lmax, int batch) {
 
 int tc_reserve(const Handle* h, int batch) {
     MixedTables* T = static_cast<MixedTables*>(h->mixed);
-    if (!T || !T->streamed || batch <= 0) return SPH_OK;
-    // only the loader-only variant (autotuned in) needs the prepared-B buffer
+    if (!T || batch <= 0) return SPH_OK;
+    const int cols = (2 * batch + 63) / 64 * 64;  // covers every column tile width
+    size_t need = 0;
+    // the int8 kernels with both operands by TMA (the default) prepare B in the buffer
+    if (T->i8) {
+        for (int nc : {16, 32, 64}) {
+            const int nct = (2 * batch + nc - 1) / nc;
+            need = std::max(need, std::max(i8b_bytes(h, true, T->lmax, nct, nc), i8b_bytes(h, false, T->lmax, nct, nc)));
+        }
+    }
+    // so does the split-TF32 loader-only variant (autotuned in)
     bool used = false;
     for (const auto& kv : h->tune) {
         const int kind = (int)(kv.first >> 32), var = kv.second;
         if (kind <= TUNE_TC_ANALYSIS && (var & 8) && !(var & 4)) used = true;
     }
-    if (!used) return SPH_OK;
-    const int cols = (2 * batch + 63) / 64 * 64;  // covers every column tile width
-    const size_t need = std::max(tcb_bytes(h, true, T->lmax, cols), tcb_bytes(h, false, T->lmax, cols));
-    return tcb_ensure(T, need, nullptr);
+    if (used && T->streamed)
+        need = std::max(need, std::max(tcb_bytes(h, true, T->lmax, cols), tcb_bytes(h, false, T->lmax, cols)));
+    return need ? tcb_ensure(T, need, nullptr) : SPH_OK;
 }
 
 template <int NC>
@@ -1449,13 +1477,16 @@ static int tcb_launch(const Handle* h, const MixedTables* Tc, bool syn, int lmax
 
 // Variants of the tensor-core Legendre stages (the autotuner's numbers):
 //   bits 0-1  column tile: 0 the built-in rule, 1: 16, 2: 32, 3: 64 real columns
-//   none of 4, 8, 16, 32   int8 integer-split kernels (legendre_i8.cuh),
+//   none of 4, 8, 16, 32   int8 integer-split kernels: both operands by TMA
+//             after a B preparation kernel (legendre_i8b.cuh), or with bit 128
+//             B staged by producer warps inside the kernel (legendre_i8.cuh);
 //             bit 64: m order paired with its complement instead of ascending
 //   32        split-TF32, P streamed by TMA, B staged by producer warps
 //   8         split-TF32, both operands by TMA (B prepared once per call)
 //   4         split-TF32, P regenerated from recurrence checkpoints
 //   16        the FP64 CUDA-core kernel (legendre.cu)
 static bool use_i8(const MixedTables* T, int var) { return T->i8 && !(var & (4 | 8 | 16 | 32)); }
+
 
 // columns per CTA of the int8 kernels: 16 (8 fields) for small batches, else 32
 static int i8_cols_v(int batch, int var) {
@@ -1483,6 +1514,36 @@ static I8Args make_i8args(const Handle* h, const MixedTables* T, bool syn, int l
     return a;
 }
 
+// the int8 kernels with both operands by TMA: B preparation, then the contraction
+template <template <int> class Dir>
+static int i8b_launch(const Handle* h, const MixedTables* Tc, bool syn, const CUtensorMap& map, I8Args& a, int nrt,
+                      const double2* in, double2* out, int nc, cudaStream_t s) {
+    MixedTables* T = const_cast<MixedTables*>(Tc);
+    a.nct = (2 * a.batch + nc - 1) / nc;
+    a.nrt = nrt;
+    a.ntiles = a.nct * nrt * a.nm;
+    a.cpt = syn ? i8b_syn_coff(a.lmax, a.nm) : (long long)a.nm * i8b_ana_nch(a.nh);
+    if (a.nct > 65535) { set_error("tensor-core Legendre stage: too many column tiles"); return SPH_ERR_ARG; }
+    const size_t bbytes = (size_t)a.nct * (size_t)a.cpt * i8b_chunk(nc);
+    if (int rc = tcb_ensure(T, i8b_bytes(h, syn, a.lmax, a.nct, nc), s)) return rc;
+    a.B = reinterpret_cast<unsigned char*>(T->Bbuf);
+    a.ecol = reinterpret_cast<int*>(a.B + bbytes);
+    const dim3 pg((unsigned)a.nm, (unsigned)a.nct);
+    const int grid = std::max(1, std::min(a.ntiles, g_tc_sms > 0 ? g_tc_sms : 148));
+    if (nc == 16) {
+        k_i8b_prep<Dir<16>, 16><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
+        k_legendre_i8b<Dir<16>, 16><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
+    } else if (nc == 32) {
+        k_i8b_prep<Dir<32>, 32><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
+        k_legendre_i8b<Dir<32>, 32><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
+    } else {
+        k_i8b_prep<Dir<64>, 64><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
+        k_legendre_i8b<Dir<64>, 64><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
+    }
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
 template <template <int> class Dir>
 static int i8_launch(const CUtensorMap& map, I8Args& a, int nrt, const double2* in, double2* out, int nc,
                      cudaStream_t s) {
@@ -1498,7 +1559,7 @@ static int i8_launch(const CUtensorMap& map, I8Args& a, int nrt, const double2* 
 }
 
 int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F, long long ldF,
-                          int batch, cudaStream_t s) {
+                          int batch, cudaStream_t s, int nobuf) {
     const MixedTables* T = static_cast<const MixedTables*>(h->mixed);
     if (int rc = check_tables(T, lmax)) return rc;
     if (batch <= 0) return SPH_OK;
@@ -1506,7 +1567,10 @@ int legendre_synthesis_tc(const Handle* h, const double2* spec, long long ld_spe
     const int var = tune_get(h, TUNE_TC_SYNTHESIS, batch, 0);
     if (use_i8(T, var)) {
         I8Args a = make_i8args(h, T, true, lmax, batch, ld_spec, ldF, var);
-        return i8_launch<SynI8>(T->mapSY, a, (h->nh + li8::M - 1) / li8::M, spec, F, i8_cols_v(batch, var), s);
+        const int nrt8 = (h->nh + li8::M - 1) / li8::M;
+        if (!(var & 128) && !nobuf)
+            return i8b_launch<SynI8>(h, T, true, T->mapSY, a, nrt8, spec, F, i8_cols_v(batch, var), s);
+        return i8_launch<SynI8>(T->mapSY, a, nrt8, spec, F, i8_cols_v(batch, var), s);
     }
     if (T->streamed && !(var & 4) && (var & 8))
         return tcb_launch(h, T, true, lmax, batch, nrt, nm, spec, ld_spec, F, ldF, var, s);
@@ -1529,8 +1593,10 @@ int legendre_analysis_tc(const Handle* h, const double2* F, long long ldF, doubl
     if (use_i8(T, var)) {
         I8Args a = make_i8args(h, T, false, lmax, batch, ld_spec, ldF, var);
         if (wmode) a.erow = T->eanc;
-        return i8_launch<AnaI8>(wmode ? T->mapANc : T->mapAN, a, (i8_nlp(lmax, 0, 0) + li8::M - 1) / li8::M, F, spec,
-                                i8_cols_v(batch, var), s);
+        const CUtensorMap& map = wmode ? T->mapANc : T->mapAN;
+        const int nrt8 = (i8_nlp(lmax, 0, 0) + li8::M - 1) / li8::M;
+        if (!(var & 128)) return i8b_launch<AnaI8>(h, T, false, map, a, nrt8, F, spec, i8_cols_v(batch, var), s);
+        return i8_launch<AnaI8>(map, a, nrt8, F, spec, i8_cols_v(batch, var), s);
     }
     if (T->streamed && !(var & 4) && (var & 8))
         return tcb_launch(h, T, false, lmax, batch, nrt, nm, F, ldF, spec, ld_spec, var, s, wts);

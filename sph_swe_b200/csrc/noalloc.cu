@@ -102,7 +102,8 @@ extern "C" int sph_SH_to_spat_noalloc(sph_handle* hh, const double* spec, double
     // the Legendre stage writes every (m <= L, j) entry of each field's slice
     // before the longitude stage reads it, so no part of the scratch has to
     // start at zero
-    if (int rc = legendre_synthesis_real(h, reinterpret_cast<const double2*>(spec), h->nlm, h->L, F, ldF, batch, s))
+    if (int rc = legendre_synthesis_real(h, reinterpret_cast<const double2*>(spec), h->nlm, h->L, F, ldF, batch, s, 0,
+                                         1))
         return rc;
     return ring_synthesis_real(h, F, ldF, mF, spat, h->nspat, batch, nullptr, nullptr, 0, 0, s);
 }

@@ -754,6 +754,9 @@ int sph_rexi_step(sph_rexi* R, double* state, int nsteps, void* stream) {
     if (!R->exec || R->state != state || R->stream != s) {
         if (R->exec) { cudaGraphExecDestroy(R->exec); R->exec = nullptr; }
         if (R->graph) { cudaGraphDestroy(R->graph); R->graph = nullptr; }
+        // operand workspace of the mixed transforms of the step (at most 4 fields
+        // per call): a capture cannot allocate
+        if (int rc = tc_reserve(R->h, 4)) return rc;
         cudaStream_t cap;
         SPH_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         SPH_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));

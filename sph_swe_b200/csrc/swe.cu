@@ -224,7 +224,9 @@ __global__ void k_rk_mid(const double2* __restrict__ T4, double2* __restrict__ X
     o[nlm + k] = make_double2(cl * lo.x + ch * hi.x, cl * lo.y + ch * hi.y);
 }
 
-// Fh[m][j] = i m A_m(j) / c^pa + B_m(j) / c^2   (pa = 1, or 2 for Robert)
+// Fh[m][j] = c (i m A_m(j) / c^pa + B_m(j) / c^2)   (pa = 1, or 2 for Robert):
+// the integrand times c, bounded at the polar rings, for the analysis with the
+// weights w / c
 __global__ void k_fourier_h(const double2* __restrict__ F2, double2* __restrict__ Fh, const double* __restrict__ cosphi,
                             int nlat, int mF, int pa) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -234,12 +236,11 @@ __global__ void k_fourier_h(const double2* __restrict__ F2, double2* __restrict_
     const int m = idx / nlat, j = idx - m * nlat;
     const double2 a = F2[(size_t)mem * 2 * fou + idx], b = F2[(size_t)mem * 2 * fou + fou + idx];
     const double c = cosphi[j];
-    const double ca = pa == 1 ? c : c * c;
-    const double c2 = c * c;
+    const double ca = pa == 1 ? 1.0 : c;
     // the synthesis Fourier coefficients lack the 2 pi longitude quadrature
     // weight that the ring analysis applies
     const double tp = 2.0 * kPi;
-    Fh[(size_t)mem * fou + idx] = make_double2(tp * (-m * a.y / ca + b.x / c2), tp * (m * a.x / ca + b.y / c2));
+    Fh[(size_t)mem * fou + idx] = make_double2(tp * (-m * a.y / ca + b.x / c), tp * (m * a.x / ca + b.y / c));
 }
 
 // K_s = [-(1/a) Th, T4[2], T4[3]] (+ Robert spectral gradient terms) + viscosity
@@ -456,7 +457,7 @@ static int swe_stage(Handle* h, RKState* r, const sph_swe_params* p, const doubl
     const dim3 gs((L + 1 + 63) / 64, L + 1, 3 * nmem);
     k_rk_prep<<<gs, 64, 0, s>>>(S, Kp, coef, r->dts, r->X6, L, nlm);
     SPH_CUDA_TRY(cudaGetLastError());
-    if (int rc = legendre_synthesis_real(h, r->X6, nlm, L, r->F6, fou, 6 * nmem, s)) return rc;
+    if (int rc = legendre_synthesis_real(h, r->X6, nlm, L, r->F6, fou, 6 * nmem, s, 1)) return rc;
     static const int src9[9] = {0, 1, 2, 0, 1, 2, 3, 4, 5};
     static const int mod9[9] = {0, 0, 0, 1, 1, 1, 0, 0, 0};
     if (int rc = ring_synthesis_real(h, r->F6, fou, mF, r->G9, h->nspat, 9 * nmem, src9, mod9, 9, 6, s)) return rc;
@@ -466,11 +467,11 @@ static int swe_stage(Handle* h, RKState* r, const sph_swe_params* p, const doubl
     if (int rc = legendre_analysis_real(h, r->F4, fou, r->T4, nlm, L, 4 * nmem, s)) return rc;
     k_rk_mid<<<dim3((L + 1 + 63) / 64, L + 1, nmem), 64, 0, s>>>(r->T4, r->X2, L, nlm);
     SPH_CUDA_TRY(cudaGetLastError());
-    if (int rc = legendre_synthesis_real(h, r->X2, nlm, L, r->F2, fou, 2 * nmem, s)) return rc;
+    if (int rc = legendre_synthesis_real(h, r->X2, nlm, L, r->F2, fou, 2 * nmem, s, 1)) return rc;
     k_fourier_h<<<dim3((unsigned)((fou + 255) / 256), nmem), 256, 0, s>>>(r->F2, r->Fh, h->cosphi, nlat, mF,
                                                                           kc.mode == 2 ? 2 : 1);
     SPH_CUDA_TRY(cudaGetLastError());
-    if (int rc = legendre_analysis_real(h, r->Fh, fou, r->Th, nlm, L, nmem, s)) return rc;
+    if (int rc = legendre_analysis_real(h, r->Fh, fou, r->Th, nlm, L, nmem, s, 1)) return rc;
     k_rk_stage_out<<<dim3((L + 1 + 63) / 64, L + 1, nmem), 64, 0, s>>>(S, Kp, coef, r->dts, r->T4, r->Th, Ks, L, nlm, kc);
     SPH_CUDA_TRY(cudaGetLastError());
     return SPH_OK;
@@ -485,7 +486,7 @@ static int swe_stage_vd(Handle* h, RKState* r, const sph_swe_params* p, const do
     k_vd_prep<<<dim3((Lp + 1 + 63) / 64, Lp + 1, nmem), 64, 0, s>>>(S, Kp, coef, r->dts, r->X6, L, nlm, nlmp,
                                                                      p->radius);
     SPH_CUDA_TRY(cudaGetLastError());
-    if (int rc = legendre_synthesis_real(h, r->X6, nlmp, Lp, r->F6, fou, 4 * nmem, s)) return rc;
+    if (int rc = legendre_synthesis_real(h, r->X6, nlmp, Lp, r->F6, fou, 4 * nmem, s, 1)) return rc;
     if (int rc = ring_synthesis_real(h, r->F6, fou, mF, r->G4, h->nspat, 4 * nmem, nullptr, nullptr, 0, 0, s)) return rc;
     k_vd_pointwise<<<dim3((h->nspat + 255) / 256, nmem), 256, 0, s>>>(r->G4, r->G9, h->mu, h->cosphi, nlat, h->nspat,
                                                                       p->gravity, p->omega);

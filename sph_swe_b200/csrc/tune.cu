@@ -3,8 +3,10 @@
 // For a batch size it times every candidate of
 //   - the tensor-core Legendre synthesis and analysis (mixed handles): column
 //     tile of 16, 32 or 64 real columns per CTA (8, 16, 32 fields) x kernel:
-//     the int8 integer-split kernel with the orders m ascending or paired with
-//     their complements (the m-to-CTA schedule), the split-TF32 kernels with P
+//     the int8 integer-split kernels (B prepared by a separate kernel and
+//     loaded by the TMA unit, or staged by producer warps inside the kernel)
+//     with the orders m ascending or paired with their complements (the
+//     m-to-CTA schedule), the split-TF32 kernels with P
 //     loaded by the TMA unit and B staged by producer warps, with both
 //     operands loaded by the TMA unit (B prepared once per call), or with P
 //     regenerated from recurrence checkpoints; and the FP64 CUDA-core kernel
@@ -93,10 +95,11 @@ static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
         std::vector<int> cand;
         if (kind <= TUNE_TC_ANALYSIS) {
             if (!h->mixed) continue;
-            // int8 kernels in ascending (0) and paired (64) m order; split TF32 with
+            // int8 kernels with both operands by TMA (0) or B staged by producer
+            // warps (128), in ascending or paired (+64) m order; split TF32 with
             // B staged by producer warps (32), both operands loaded by the TMA unit
             // (8), P regenerated (4)
-            for (int src : {0, 64, 32, 8, 4})
+            for (int src : {0, 64, 128, 192, 32, 8, 4})
                 for (int c = 1; c <= 3; c++) cand.push_back(src | c);
             cand.push_back(16);  // FP64 CUDA-core kernel
         } else {
@@ -162,7 +165,7 @@ static int tune_load(Handle* h, const char* json) {
         if (!b || !v) break;
         batch = std::atoi(b + 8);
         var = std::atoi(v + 10);
-        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 127) {
+        if (kind < 0 || kind > 3 || batch <= 0 || var < 0 || var > 255) {
             set_error("sph_tune_load: malformed entry");
             return SPH_ERR_ARG;
         }

@@ -117,7 +117,7 @@ int sph_vec_SH_to_spat(sph_handle* hh, const double* vort, const double* div, do
                                                                      reinterpret_cast<const double2*>(div), h->nlm, X, L,
                                                                      nlmp);
     SPH_CUDA_TRY(cudaGetLastError());
-    if (int rc = legendre_synthesis_real(h, X, nlmp, Lp, F, ldF, 2 * batch, s)) return rc;
+    if (int rc = legendre_synthesis_real(h, X, nlmp, Lp, F, ldF, 2 * batch, s, 1)) return rc;
     if (!robert) {
         k_fourier_scale<<<dim3((unsigned)((ldF + 255) / 256), 2 * batch), 256, 0, s>>>(F, ldF, mF, h->nlat, h->cosphi, 1);
         SPH_CUDA_TRY(cudaGetLastError());

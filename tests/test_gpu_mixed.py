@@ -1,15 +1,16 @@
-"""Mixed-precision form (SPH_PREC_MIXED): Legendre stage on tcgen05 in
-split-TF32 with FP32 chunk sums folded into FP64, everything else FP64.
+"""Mixed-precision form (SPH_PREC_MIXED): Legendre stage on tcgen05, by
+default the int8 integer-split kernels (exact int32 digit-product sums, one
+FP64 combination per tile), everything else FP64.
 
 Tolerances (relative L2 against the FP64 oracle / FP64 GPU path):
-  scalar synthesis and analysis           <= 1e-6  (measured 2e-7 .. 4e-7)
-  vector synthesis u, v                   <= 2e-6
-  vector round trip vort -> u,v -> vort   <= 5e-5  (the analysis of u, v divides
-      by l(l+1) and amplifies the split-TF32 error at high degree)
-  nonlinear RK4, T63, 200 steps: h <= 1e-6; u, v <= 1e-4 (measured 4e-5:
-      the two-term TF32 split (22 bits) and the FP32 rounding of each MMA
-      bound each transform near 2e-7, and the 200-step map amplifies that by
-      ~100 in the velocity, which starts from rest)
+  scalar synthesis and analysis           <= 1e-6  (measured ~1e-8)
+  vector synthesis u, v                   <= 1e-6  (the m = 0 column of the
+      Robert velocities is synthesised in FP64: it vanishes like cos^2 at the
+      poles while its terms do not, and u = U / cos would amplify the error)
+  vector round trip vort -> u,v -> vort   <= 1e-6
+  nonlinear RK4, T63, 200 steps: h <= 1e-6; u, v <= 1e-4 (the 200-step map
+      amplifies each transform's error in the velocity, which starts from rest)
+The split-TF32 kernels (autotuner variants) reach ~3e-7 per transform.
 """
 import numpy as np
 import pytest
@@ -74,11 +75,13 @@ def test_vector_pair_vs_fp64(gpu, L):
     for robert in (False, True):
         u, v = s.vec_SH_to_spat(vort, div, robert=robert)
         u64, v64 = s64.vec_SH_to_spat(vort, div, robert=robert)
-        assert rel_l2(u.cpu().numpy(), u64.cpu().numpy()) < 2e-6
-        assert rel_l2(v.cpu().numpy(), v64.cpu().numpy()) < 2e-6
+        eu = rel_l2(u.cpu().numpy(), u64.cpu().numpy())
+        ev = rel_l2(v.cpu().numpy(), v64.cpu().numpy())
+        assert eu < TOL and ev < TOL, (robert, eu, ev)
         z, d = s.vec_spat_to_SH(u, v, robert=robert)
-        assert rel_l2(z.cpu().numpy(), vort.cpu().numpy()) < 5e-5
-        assert rel_l2(d.cpu().numpy(), div.cpu().numpy()) < 5e-5
+        ez = rel_l2(z.cpu().numpy(), vort.cpu().numpy())
+        ed = rel_l2(d.cpu().numpy(), div.cpu().numpy())
+        assert ez < TOL and ed < TOL, (robert, ez, ed)
     _sync_ok(s)
 
 
@@ -163,18 +166,23 @@ def _plm_at(mu_north, T):
     return P
 
 
-@pytest.mark.parametrize("L,nb", [(31, 3), (63, 5), (127, 17)])
-def test_int8_legendre_matches_integer_split_model(gpu, oracle_mod, L, nb):
-    """The Legendre stages of the mixed form (int8 kernels, the default) carry
-    out the arithmetic of the integer-split model (oracle/intsplit.py) given P
-    at the handle's own Gauss nodes: the same row and column exponents, digits
-    and exact integer group sums, so the results agree far below the form's
-    own error (the model's P comes from scipy, the kernel's from its FP64
-    recurrence, so a digit may differ in the last place), and both are within
-    2e-8 of the FP64 oracle."""
+@pytest.mark.parametrize("L,nb", [(31, 3), (63, 5), (127, 17), (255, 40)])
+@pytest.mark.parametrize("variant", [0, 128])
+def test_int8_legendre_matches_integer_split_model(gpu, oracle_mod, L, nb, variant):
+    """The Legendre stages of the mixed form (int8 kernels: B prepared by a
+    separate kernel and loaded by the TMA unit, the default, or staged by
+    producer warps, variant 128) carry out the arithmetic of the integer-split
+    model (oracle/intsplit.py) given P at the handle's own Gauss nodes: the same
+    row and column exponents, digits and exact integer group sums, so the
+    results agree far below the form's own error (the model's P comes from
+    scipy, the kernel's from its FP64 recurrence, so a digit may differ in the
+    last place), and both are within 2e-8 of the FP64 oracle."""
     from oracle import intsplit
 
     s = _mixed(L)
+    if variant:
+        s.tune_load({"lmax": L, "nphi": s.nphi,
+                     "kernels": [{"kind": k, "batch": nb, "variant": variant} for k in (0, 1)]})
     g = oracle_mod.Grid(L)
     nh = s.nlat // 2
     P = _plm_at(s.mu[:nh], L + 1)  # the handle's tables reach degree L + 1

@@ -30,7 +30,7 @@ def test_autotune_table_and_results(gpu, oracle_mod, L, prec):
     if prec == capi.SPH_PREC_MIXED:
         assert {"legendre_synthesis_tc", "legendre_analysis_tc"} <= names
         tc = [k for k in table["kernels"] if k["name"].endswith("_tc")]
-        assert all(len(k["candidates"]) == 16 for k in tc)
+        assert all(len(k["candidates"]) == 22 for k in tc)
     for k in table["kernels"]:
         assert k["us"] > 0 and k["us"] == min(c["us"] for c in k["candidates"])
     grid1 = s.SH_to_spat(spec)
@@ -43,7 +43,8 @@ def test_autotune_table_and_results(gpu, oracle_mod, L, prec):
     assert rel_l2(grid1.cpu().numpy(), grid0.cpu().numpy()) < tuned_tol
     assert rel_l2(back1.cpu().numpy(), back0.cpu().numpy()) < tuned_tol
     # every variant forced through a loaded table gives the same transforms
-    variants = [0, 1] if prec == 0 else [1, 2, 3, 65, 66, 67, 33, 34, 35, 5, 6, 7, 9, 10, 11, 16]
+    variants = [0, 1] if prec == 0 else [1, 2, 3, 65, 66, 67, 129, 130, 131, 193, 194, 195, 33, 34, 35, 5, 6, 7,
+                                         9, 10, 11, 16]
     for v in variants:
         forced = {"lmax": L, "nphi": s.nphi, "kernels": [
             {"kind": kind, "batch": nb, "variant": (v if kind < 2 else v & 1)} for kind in range(4)]}
