@@ -185,8 +185,11 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
         __syncwarp();
     } else {
         // ---------------------------------------------------------------- consumers
+        // a warp reads the tensor-memory lane quadrant warp % 4 (the only one
+        // tcgen05.ld lets it access); warps 2-5 take the first half of the
+        // columns, warps 6-9 the second
         const int cw = warp - li8b::CONS_WARP0;
-        const int qd = cw & 3, half = cw >> 2;  // lane quadrant, column half
+        const int qd = warp & 3, half = cw >> 2;
         const int r = qd * 32 + lane;
         int j = 0;
         for (I8Tile p = first; p.t < a.ntiles; p = i8_tile<Dir>(a, p.t + gridDim.x), j++) {
