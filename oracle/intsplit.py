@@ -51,8 +51,9 @@ def digits(M: np.ndarray, e: np.ndarray, axis: int):
     """The four balanced digit planes d0..d3 (int64 arrays with values in
     [-128, 127]) of v = rint(M 2^-e 2^31), e broadcast along `axis` (1: one
     exponent per row, 0: one per column)."""
-    sc = np.ldexp(1.0, (VBITS - (e[:, None] if axis == 1 else e[None, :])).astype(np.int64))
-    v = np.rint(M * sc).astype(np.int64)
+    k = (VBITS - (e[:, None] if axis == 1 else e[None, :])).astype(np.int64)
+    # M 2^k in one step: 2^k alone overflows for rows of tiny magnitude
+    v = np.rint(np.ldexp(M, np.broadcast_to(k, M.shape))).astype(np.int64)
     out = []
     for _ in range(3):
         d = ((v + 128) & 255) - 128
