@@ -290,9 +290,12 @@ static int ring_tile(int n, int complex_rings) {
     return jt;
 }
 
-// sequences per CTA of the fixed-length kernels: variant 0 the default, 1 half of it
+// sequences per CTA of the fixed-length kernels: variant 0 the default, 1 twice
+// it, 2 half of it (at least 1)
 template <int N, int V>
-constexpr int fixed_p() { return V == 0 ? fftx::seqs<N>() : fftx::seqs<N>() / 2; }
+constexpr int fixed_p() {
+    return V == 0 ? fftx::seqs<N>() : (V == 1 ? 2 * fftx::seqs<N>() : (fftx::seqs<N>() > 1 ? fftx::seqs<N>() / 2 : 1));
+}
 
 template <int N, int P>
 static size_t fixed_smem() {
@@ -311,7 +314,8 @@ static int fixed_attr_p() {
 template <int N>
 static int fixed_attr() {
     if (int rc = fixed_attr_p<N, fixed_p<N, 0>()>()) return rc;
-    return fixed_attr_p<N, fixed_p<N, 1>()>();
+    if (int rc = fixed_attr_p<N, fixed_p<N, 1>()>()) return rc;
+    return fixed_attr_p<N, fixed_p<N, 2>()>();
 }
 
 // every (longitude, ring pair) of every field is an aligned 16-byte chunk
@@ -322,14 +326,14 @@ static int rows16(const Handle* h, const double* spat, long long ld_spat) {
 template <int N, int P>
 static void launch_ra(const Handle* h, const double* spat, long long ld_spat, double2* F, long long ldF, int mF, int batch,
                       cudaStream_t s) {
-    k_ring_analysis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::NT, fixed_smem<N, P>(), s>>>(
+    k_ring_analysis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::nt<N, P>(), fixed_smem<N, P>(), s>>>(
         spat, ld_spat, F, ldF, mF, h->L, h->nlat, h->fft.tw, rows16(h, spat, ld_spat));
 }
 
 template <int N, int P>
 static void launch_rs(const Handle* h, const double2* F, long long ldF, int mF, double* spat, long long ld_spat, int batch,
                       const RingMap& map, cudaStream_t s) {
-    k_ring_synthesis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::NT, fixed_smem<N, P>(), s>>>(
+    k_ring_synthesis_real_n<N, P><<<dim3((h->nlat + 2 * P - 1) / (2 * P), batch), fftx::nt<N, P>(), fixed_smem<N, P>(), s>>>(
         F, ldF, mF, h->L, spat, ld_spat, h->nlat, h->fft.tw, map, rows16(h, spat, ld_spat));
 }
 
@@ -352,7 +356,8 @@ int ring_analysis_real(const Handle* h, const double* spat, long long ld_spat, d
     switch (h->nphi) {
 #define SPH_RA(NN)                                                                                                   \
     case NN:                                                                                                         \
-        if (var) launch_ra<NN, fixed_p<NN, 1>()>(h, spat, ld_spat, F, ldF, mF, batch, s);                            \
+        if (var == 1) launch_ra<NN, fixed_p<NN, 1>()>(h, spat, ld_spat, F, ldF, mF, batch, s);                       \
+        else if (var == 2) launch_ra<NN, fixed_p<NN, 2>()>(h, spat, ld_spat, F, ldF, mF, batch, s);                  \
         else launch_ra<NN, fixed_p<NN, 0>()>(h, spat, ld_spat, F, ldF, mF, batch, s);                                \
         SPH_CUDA_TRY(cudaGetLastError());                                                                            \
         return SPH_OK;
@@ -398,7 +403,8 @@ int ring_synthesis_real(const Handle* h, const double2* F, long long ldF, int mF
     switch (h->nphi) {
 #define SPH_RS(NN)                                                                                                   \
     case NN:                                                                                                         \
-        if (var) launch_rs<NN, fixed_p<NN, 1>()>(h, F, ldF, mF, spat, ld_spat, batch, map, s);                       \
+        if (var == 1) launch_rs<NN, fixed_p<NN, 1>()>(h, F, ldF, mF, spat, ld_spat, batch, map, s);                  \
+        else if (var == 2) launch_rs<NN, fixed_p<NN, 2>()>(h, F, ldF, mF, spat, ld_spat, batch, map, s);             \
         else launch_rs<NN, fixed_p<NN, 0>()>(h, F, ldF, mF, spat, ld_spat, batch, map, s);                           \
         SPH_CUDA_TRY(cudaGetLastError());                                                                            \
         return SPH_OK;

@@ -2,11 +2,13 @@
 // grids use: 96, 192, 384, 768, 1536, 3072), used by fft.cu in place of the
 // generic kernels for those lengths.
 //
-// A CTA of 384 threads transforms P complex sequences (P = 8 up to N = 768,
-// i.e. 16 rings: every longitude row of the tile is one 128-byte run of the
-// theta-contiguous grid; P is a template parameter so that the autotuner can
-// trade tile width for CTAs per SM), i.e. 2P consecutive latitude rings of one
-// field packed in pairs (ring 2q real part, ring 2q+1 imaginary part).  Shared
+// A CTA transforms P complex sequences, i.e. 2P consecutive latitude rings of
+// one field packed in pairs (ring 2q real part, ring 2q+1 imaginary part), with
+// max(128, P N / 16) threads (one radix-16 butterfly each).  By default P = 4 up
+// to N = 768 (8 rings: every longitude row of the tile is one 64-byte run of
+// the theta-contiguous grid, 49 KB of shared memory at N = 768), so that
+// several CTAs share an SM and one CTA's loads overlap another's passes; the
+// autotuner may take twice or half that.  Shared
 // memory holds the tile element-major with the sequences innermost,
 // buf[i * P + q]: element i of all P sequences is the 16 P bytes that
 // longitude i of the 2P rings occupies in the grid.
@@ -32,10 +34,15 @@
 namespace sphgpu {
 namespace fftx {
 
-constexpr int NT = 384;     // threads per CTA
 // default complex sequences per CTA (2 P real rings)
 template <int N>
-constexpr int seqs() { return N <= 768 ? 8 : (N == 1536 ? 4 : 2); }
+constexpr int seqs() { return N <= 768 ? 4 : (N == 1536 ? 2 : 1); }
+// threads per CTA: one radix-16 butterfly each, at least 128
+template <int N, int P>
+constexpr int nt() { return P * N / 16 > 128 ? P * N / 16 : 128; }
+// CTAs per SM the register budget is set for
+template <int N, int P>
+constexpr int minb() { return nt<N, P>() >= 384 ? 1 : (nt<N, P>() >= 192 ? 3 : 4); }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -219,6 +226,7 @@ constexpr int ls_at(int N, int q) {
 //         are written.
 template <int N, int P, int Q, int SIGN, int DIR, bool ZMASK, bool WMASK>
 __device__ __forceinline__ void pass(double2* buf, const double2* __restrict__ tw, int mm) {
+    constexpr int NT = nt<N, P>();
     constexpr int R = radix_at<DIR>(N, Q);
     constexpr int Ls = ls_at<DIR>(N, Q);
     constexpr int NR = N / R;
@@ -280,10 +288,10 @@ namespace sphgpu {
 // the field rows 16-byte aligned, so each (longitude, ring pair) is one aligned
 // 16-byte load.
 template <int N, int P>
-__global__ void __launch_bounds__(fftx::NT, 1) k_ring_analysis_real_n(const double* __restrict__ spat, long long ld_spat,
+__global__ void __launch_bounds__(fftx::nt<N, P>(), fftx::minb<N, P>()) k_ring_analysis_real_n(const double* __restrict__ spat, long long ld_spat,
                                                                     double2* __restrict__ F, long long ldF, int mF, int L,
                                                                     int nlat, const double2* __restrict__ tw, int vec) {
-    constexpr int JT = 2 * P, N3 = N / 3, TOT = P * N3;
+    constexpr int JT = 2 * P, N3 = N / 3, TOT = P * N3, NT = fftx::nt<N, P>();
     constexpr int U = 3;  // radix-3 butterflies whose loads are in flight together
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
@@ -292,11 +300,11 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_analysis_real_n(const doub
     // first pass (radix 3, Ls = 1: no twiddles) straight from the grid:
     // butterfly (f, j) reads longitudes j, j + N/3, j + 2N/3 of ring pair f and
     // writes elements 3j, 3j + 1, 3j + 2
-    for (int base = threadIdx.x; base < TOT; base += U * fftx::NT) {
+    for (int base = threadIdx.x; base < TOT; base += U * NT) {
         double2 x[U][3];
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const int t = base + u * fftx::NT;
+            const int t = base + u * NT;
             const int f = t % P, j = t / P, jr = j0 + 2 * f;
             const bool in = t < TOT && jr < nlat;
 #pragma unroll
@@ -309,8 +317,8 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_analysis_real_n(const doub
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const int t = base + u * fftx::NT;
-            if (TOT % (U * fftx::NT) == 0 || t < TOT) {
+            const int t = base + u * NT;
+            if (TOT % (U * NT) == 0 || t < TOT) {
                 const int f = t % P, j = t / P;
                 fftx::dft3<-1>(x[u][0], x[u][1], x[u][2]);
 #pragma unroll
@@ -322,7 +330,7 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_analysis_real_n(const doub
     fftx::passes<N, P, 1, fftx::npasses(N), -1, -1>(fbuf, tw, mk);
     const double scale = 2.0 * kPi / N;
     double2* out = F + (long long)blockIdx.y * ldF;
-    for (int idx = threadIdx.x; idx < mF * P; idx += fftx::NT) {
+    for (int idx = threadIdx.x; idx < mF * P; idx += NT) {
         const int m = idx / P, q = idx % P;
         const int j = j0 + 2 * q;
         if (j >= nlat) continue;
@@ -341,11 +349,11 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_analysis_real_n(const doub
 // F[fs][m][j] (optionally times i*m) -> grid k; m = 0 contributes its real part.
 // vec != 0: nlat even and the field rows 16-byte aligned (16-byte stores).
 template <int N, int P>
-__global__ void __launch_bounds__(fftx::NT, 1) k_ring_synthesis_real_n(const double2* __restrict__ F, long long ldF, int mF,
+__global__ void __launch_bounds__(fftx::nt<N, P>(), fftx::minb<N, P>()) k_ring_synthesis_real_n(const double2* __restrict__ F, long long ldF, int mF,
                                                                      int L, double* __restrict__ spat, long long ld_spat,
                                                                      int nlat, const double2* __restrict__ tw,
                                                                      RingMap map, int vec) {
-    constexpr int JT = 2 * P, N3 = N / 3, TOT = P * N3;
+    constexpr int JT = 2 * P, N3 = N / 3, TOT = P * N3, NT = fftx::nt<N, P>();
     constexpr int U = 3;
     extern __shared__ double2 fbuf[];
     const int j0 = blockIdx.x * JT;
@@ -362,11 +370,11 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_synthesis_real_n(const dou
     // pass reads them as zeros)
     constexpr int UL = 8;
     const int tot = (mm + 1) * P;
-    for (int base = threadIdx.x; base < tot; base += UL * fftx::NT) {
+    for (int base = threadIdx.x; base < tot; base += UL * NT) {
         double2 X[UL], Y[UL];
 #pragma unroll
         for (int u = 0; u < UL; u++) {
-            const int idx = base + u * fftx::NT;
+            const int idx = base + u * NT;
             const int m = idx / P, j = j0 + 2 * (idx % P);
             X[u] = Y[u] = make_double2(0, 0);
             if (idx < tot && j < nlat) X[u] = __ldg(&in[(long long)m * nlat + j]);
@@ -374,7 +382,7 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_synthesis_real_n(const dou
         }
 #pragma unroll
         for (int u = 0; u < UL; u++) {
-            const int idx = base + u * fftx::NT;
+            const int idx = base + u * NT;
             if (idx >= tot) break;
             const int m = idx / P, q = idx % P;
             double2 x = X[u], y = Y[u];
@@ -397,12 +405,12 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_synthesis_real_n(const dou
     // (f, j) reads elements j, j + N/3, j + 2N/3 and writes longitudes
     // j, j + N/3, j + 2N/3 of ring pair f
     double* out = spat + (long long)k * ld_spat;
-    for (int base = threadIdx.x; base < TOT; base += U * fftx::NT) {
+    for (int base = threadIdx.x; base < TOT; base += U * NT) {
         double2 x[U][3];
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const int t = base + u * fftx::NT;
-            if (TOT % (U * fftx::NT) == 0 || t < TOT) {
+            const int t = base + u * NT;
+            if (TOT % (U * NT) == 0 || t < TOT) {
                 const int f = t % P, j = t / P;
 #pragma unroll
                 for (int r = 0; r < 3; r++) x[u][r] = fbuf[(j + r * N3) * P + f];
@@ -412,9 +420,9 @@ __global__ void __launch_bounds__(fftx::NT, 1) k_ring_synthesis_real_n(const dou
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const int t = base + u * fftx::NT;
+            const int t = base + u * NT;
             const int f = t % P, j = t / P, jr = j0 + 2 * f;
-            if ((TOT % (U * fftx::NT) == 0 || t < TOT) && jr < nlat) {
+            if ((TOT % (U * NT) == 0 || t < TOT) && jr < nlat) {
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double* p = out + (long long)(j + r * N3) * nlat + jr;

@@ -268,18 +268,26 @@ struct SynI8 {
             put(par, zl, 2 * fl + 1, q, o);
         }
     }
-    // consumer: TMEM lane r = latitude 128 rt + r; e, o: 8 columns of parity 0 / 1
-    __device__ static void epilogue(const I8Args& a, const I8Tile& p, int r, int c0, const int* ecol, const double* e,
-                                    const double* o, double2* __restrict__ F) {
+    // consumer: the row exponent of TMEM lane r (latitude 128 rt + r), less
+    // the 14 of the combination, loaded ahead of the accumulator
+    __device__ static void row_exp(const I8Args& a, const I8Tile& p, int r, int* er) {
+        const int j = p.rt * li8::M + r;
+        er[0] = j < a.nh ? a.erow[(long long)p.m * a.nh + j] - 14 : 0;
+        er[1] = 0;
+    }
+    // consumer: TMEM lane r = latitude 128 rt + r; e, o: 8 columns c0.. of
+    // parity 0 / 1, ec8 their column exponents
+    __device__ static void epilogue(const I8Args& a, const I8Tile& p, int r, int c0, const int* er, const int* ec8,
+                                    const double* e, const double* o, double2* __restrict__ F) {
         const int j = p.rt * li8::M + r;
         if (j >= a.nh) return;
-        const int ea = a.erow[(long long)p.m * a.nh + j] - 14;
+        const int ea = er[0];
         const int fb = p.ct * NF + c0 / 2;
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const int f = fb + u;
             if (f >= a.batch) continue;
-            const double sr = i8_pow2(ea + ecol[c0 + 2 * u]), si = i8_pow2(ea + ecol[c0 + 2 * u + 1]);
+            const double sr = i8_pow2(ea + ec8[2 * u]), si = i8_pow2(ea + ec8[2 * u + 1]);
             const double er = e[2 * u] * sr, ei = e[2 * u + 1] * si, orr = o[2 * u] * sr, oi = o[2 * u + 1] * si;
             double2* out = F + (long long)f * a.ldF + (long long)p.m * a.nlat;
             out[j] = make_double2(er + orr, ei + oi);
@@ -363,22 +371,28 @@ struct AnaI8 {
         i8_planes4(w(ni[0] - sim[0], si.y), w(ni[1] - sim[1], si.y), w(ni[2] - sim[2], si.y), w(ni[3] - sim[3], si.y), o);
         put(1, zl, 2 * fl + 1, q, o);
     }
+    // consumer: row exponents (less 14) of the degrees l' = 128 rt + r of both
+    // parities, loaded ahead of the accumulator
+    __device__ static void row_exp(const I8Args& a, const I8Tile& p, int r, int* er) {
+        const int le = p.m + 2 * (li8::M * p.rt + r);
+        er[0] = le <= a.lmax ? a.erow[pidx(a.tlmax, le, p.m)] - 14 : 0;
+        er[1] = le + 1 <= a.lmax ? a.erow[pidx(a.tlmax, le + 1, p.m)] - 14 : 0;
+    }
     // consumer: TMEM lane r = degree index l' = 128 rt + r of both parities
-    __device__ static void epilogue(const I8Args& a, const I8Tile& p, int r, int c0, const int* ecol, const double* e,
-                                    const double* o, double2* __restrict__ spec) {
+    __device__ static void epilogue(const I8Args& a, const I8Tile& p, int r, int c0, const int* er, const int* ec8,
+                                    const double* e, const double* o, double2* __restrict__ spec) {
         const int lp = li8::M * p.rt + r;
         const int le = p.m + 2 * lp;
         if (le > a.lmax) return;
         const bool odd = le + 1 <= a.lmax;
-        const int eae = a.erow[pidx(a.tlmax, le, p.m)] - 14;
-        const int eao = odd ? a.erow[pidx(a.tlmax, le + 1, p.m)] - 14 : 0;
+        const int eae = er[0], eao = er[1];
         const int fb = p.ct * NF + c0 / 2;
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const int f = fb + u;
             if (f >= a.batch) continue;
             double2* out = spec + (long long)f * a.ld_spec;
-            const int cr = ecol[c0 + 2 * u], ci = ecol[c0 + 2 * u + 1];
+            const int cr = ec8[2 * u], ci = ec8[2 * u + 1];
             out[pidx(a.lmax, le, p.m)] = make_double2(e[2 * u] * i8_pow2(eae + cr), e[2 * u + 1] * i8_pow2(eae + ci));
             if (odd)
                 out[pidx(a.lmax, le + 1, p.m)] =
@@ -615,12 +629,14 @@ __global__ void __launch_bounds__(li8::NT, 1) k_legendre_i8(const __grid_constan
             for (int c = 0; c < NC; c++) ecol[c] = exps[(j & 1) * 64 + c];
             mbar_arrive(smem_u32(&expempty[j & 1]));
             const uint32_t base = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * TCOLS);
+            int er[2];
+            Dir::row_exp(a, p, r, er);
 #pragma unroll
             for (int c0 = 0; c0 < NC; c0 += 8) {
                 double e[8], o[8];
                 i8_ld_combine<NC>(base + (uint32_t)c0, e);
                 i8_ld_combine<NC>(base + (uint32_t)(li8::NG * NC + c0), o);
-                Dir::epilogue(a, p, r, c0, ecol, e, o, out);
+                Dir::epilogue(a, p, r, c0, er, ecol + c0, e, o, out);
             }
             tc_fence_before();
             mbar_arrive(smem_u32(&accempty[b]));

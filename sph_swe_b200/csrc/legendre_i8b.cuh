@@ -194,18 +194,24 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
         int j = 0;
         for (I8Tile p = first; p.t < a.ntiles; p = i8_tile<Dir>(a, p.t + gridDim.x), j++) {
             const int b = j % NACC;
+            // row and column exponents of this thread's outputs: loaded before the
+            // wait, so their latency overlaps the tile's MMAs
+            int er[2], ec[HALF];
+            Dir::row_exp(a, p, r, er);
+            const int* ecol = a.ecol + ((long long)p.ct * a.nm + p.m) * NC + half * HALF;
+#pragma unroll
+            for (int c = 0; c < HALF; c++) ec[c] = __ldg(ecol + c);
             const bool v = mbar_wait_abort(smem_u32(&accfull[b]), (uint32_t)((j / NACC) & 1), abort);
             if (!__all_sync(0xffffffffu, v)) break;
             tc_fence_after();
-            const int* ecol = a.ecol + ((long long)p.ct * a.nm + p.m) * NC;
             const uint32_t base = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * TCOLS);
 #pragma unroll
-            for (int c0 = 0; c0 < NC; c0 += 8) {
-                if (c0 / HALF != half) continue;
+            for (int cb = 0; cb < HALF; cb += 8) {
+                const int c0 = half * HALF + cb;
                 double e[8], o[8];
                 i8_ld_combine<NC>(base + (uint32_t)c0, e);
                 i8_ld_combine<NC>(base + (uint32_t)(li8::NG * NC + c0), o);
-                Dir::epilogue(a, p, r, c0, ecol, e, o, out);
+                Dir::epilogue(a, p, r, c0, er, ec + cb, e, o, out);
             }
             tc_fence_before();
             mbar_arrive(smem_u32(&accempty[b]));

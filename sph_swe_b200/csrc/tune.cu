@@ -12,7 +12,7 @@
 //     regenerated from recurrence checkpoints; and the FP64 CUDA-core kernel
 //     of the plain form (variant 16);
 //   - the fixed-length ring FFTs (automatic grids): 2P rings per CTA with the
-//     default P or half of it (more CTAs per SM, shorter tiles);
+//     default P, twice or half of it (fewer or more CTAs per SM);
 // with CUDA events on the caller's stream (one warm-up launch, then the mean
 // of three), keeps the fastest in the handle (later calls with that batch
 // use it) and writes the table as JSON.  sph_tune_load re-applies a table.
@@ -104,7 +104,7 @@ static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
             cand.push_back(16);  // FP64 CUDA-core kernel
         } else {
             if (!fixed_ring(h->nphi)) continue;
-            cand = {0, 1};
+            cand = {0, 1, 2};
         }
         const long long key = ((long long)kind << 32) | (unsigned)batch;
         h->tune.erase(key);
