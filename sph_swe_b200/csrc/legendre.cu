@@ -409,11 +409,40 @@ __global__ void k_zero_top(double2* spec, long long ld, int lmax, int batch) {
     if (f < batch) spec[(long long)f * ld + pidx(lmax, lmax, lmax)] = make_double2(0, 0);
 }
 
-// nm_only > 0: the first nm_only orders m only
+// The order m = 0 alone, FP64, one thread per northern latitude j and field:
+// E = sum over even l, O = sum over odd l of P_l(mu_j) X_l; north E + O, south
+// E - O.  Coalesced table reads (consecutive j), the 257-term sums in registers:
+// a few microseconds where the general kernel, given one order, would run a
+// handful of CTAs.
+__global__ void __launch_bounds__(128) k_legendre_synthesis_m0(const double* __restrict__ plm, int nh, int nlat,
+                                                               const double2* __restrict__ spec, long long ld_spec,
+                                                               int lmax, double2* __restrict__ F, long long ldF) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nh) return;
+    const int f = blockIdx.y;
+    const double2* x = spec + (long long)f * ld_spec;  // m = 0 block: degrees 0..lmax at the start
+    double2 e = make_double2(0, 0), o = make_double2(0, 0);
+    for (int l = 0; l <= lmax; l += 2) {
+        const double p0 = plm[(long long)l * nh + j];
+        const double2 x0 = __ldg(&x[l]);
+        e.x = fma(p0, x0.x, e.x);
+        e.y = fma(p0, x0.y, e.y);
+        if (l + 1 <= lmax) {
+            const double p1 = plm[(long long)(l + 1) * nh + j];
+            const double2 x1 = __ldg(&x[l + 1]);
+            o.x = fma(p1, x1.x, o.x);
+            o.y = fma(p1, x1.y, o.y);
+        }
+    }
+    double2* out = F + (long long)f * ldF;  // m = 0 row
+    out[j] = make_double2(e.x + o.x, e.y + o.y);
+    out[nlat - 1 - j] = make_double2(e.x - o.x, e.y - o.y);
+}
+
 static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double2* F, long long ldF, int batch,
-                        cudaStream_t s, int nm_only = 0) {
+                        cudaStream_t s) {
     if (batch <= 0) return SPH_OK;
-    const int nm = nm_only > 0 ? nm_only : (sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1);
+    const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
     if (batch > 16) {
         dim3 grid((h->nh + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
         k_legendre_synthesis_w<<<grid, WNT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
@@ -469,6 +498,7 @@ int legendre_kernels_init() {
     // launch, also before launches inside a stream capture
     SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_w, cudaFuncAttributeMaxDynamicSharedMemorySize, WSMEM_ANA));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_zero_top));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_m0));
     return SPH_OK;
 }
 
@@ -478,7 +508,12 @@ int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_s
     // mixed handles: the tensor-core kernels unless the autotuner found the FP64 kernel faster (variant bit 16)
     if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_SYNTHESIS, batch, 0) & 16)) {
         if (int rc = legendre_synthesis_tc(h, spec, ld_spec, lmax, F, ldF, batch, s, nobuf)) return rc;
-        return exact_m0 ? launch_synth(h, spec, sm, F, ldF, batch, s, 1) : SPH_OK;
+        if (!exact_m0) return SPH_OK;
+        if (batch > 65535) { set_error("legendre synthesis: too many fields for one launch"); return SPH_ERR_ARG; }
+        k_legendre_synthesis_m0<<<dim3((h->nh + 127) / 128, batch), 128, 0, s>>>(h->plm + h->poff_h[0], h->nh, h->nlat,
+                                                                                  spec, ld_spec, lmax, F, ldF);
+        SPH_CUDA_TRY(cudaGetLastError());
+        return SPH_OK;
     }
     return launch_synth(h, spec, sm, F, ldF, batch, s);
 }

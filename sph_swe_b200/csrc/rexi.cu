@@ -63,6 +63,9 @@ struct RexiPlan {
     signed char* pphi = nullptr;
     signed char* pvel = nullptr;
     long long plane = 0;
+    // Robert form with stored factors: phi of every pole between the Phi and
+    // the velocity phase, [pole group][block row][32 lanes]
+    double2* PHr = nullptr;
     bool singular = false;      // a zero pivot met while factoring
     // non-Robert form (SWERexiSPH): per-pole phi and the spectra of its
     // grid-valued gradients, their Fourier buffer, real-layout prep buffers
@@ -133,6 +136,148 @@ __global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
             outp[(size_t)2 * nc + row] = v2;
         }
     }
+}
+
+// ------------------------------------------------------------ Robert form, stored factors
+// The substitutions of k_rexi_solve<.., STORED> split into two launches of one
+// warp per (pole group, m-block, l-parity), one pole per lane, so that no lane
+// keeps the block's phi, u, v in local memory (that traffic, not the factor
+// stream, bounded the single kernel): the Phi phase writes phi of its parity's
+// rows to PH[group][block row][lane] (one coalesced 512-byte row per warp
+// access) and sums beta phi over its poles; the velocity phase forms each
+// row's right-hand sides from a window phi[i-2 .. i+2] of both parities read
+// back from PH, solves, and sums beta u, beta v.  The arithmetic of every row
+// is that of rexi_phi / rexi_lane.
+__device__ __forceinline__ void rx_warp_index(const RexiDev& d, int warp, int& g, int& m, int& par) {
+    par = warp & 1;
+    const int w2 = warp >> 1;
+    g = w2 % d.ngroups;
+    const int kk = w2 / d.ngroups;
+    m = (kk & 1) ? -((kk + 1) >> 1) : (kk >> 1);  // 0, -1, 1, -2, 2, ...: largest blocks first
+}
+
+// beta x summed over the 32 poles of the warp into *dst (lane 0 writes)
+__device__ __forceinline__ void rx_warp_sum(double2 bt, double2 x, double2* dst, int lane) {
+    double2 v = c_mul(bt, x);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+    }
+    if (lane == 0) *dst = v;
+}
+
+template <int MAXN>
+__global__ void __launch_bounds__(64) k_rexi_phi_st(RexiDev d, double2* __restrict__ PH) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int L = d.L;
+    if (warp >= 2 * (2 * L + 1) * d.ngroups) return;
+    int g, m, par;
+    rx_warp_index(d, warp, g, m, par);
+    const int N = L + 1 - (m < 0 ? -m : m);
+    const int Np = (N - par + 1) >> 1;
+    if (Np <= 0) return;
+    const int base = block_off(L, m);
+    const int nc = d.ncplx;
+    const int pole = g * 32 + lane;
+    const bool valid = pole < d.npoles;
+    const double2 a = d.alpha[valid ? pole : 0];
+    const double2 bt = valid ? d.beta[pole] : make_double2(0, 0);
+    const double T = d.T, P = d.P, ir = d.ir;
+    const double2 a2 = c_mul(a, a), a3 = c_mul(a2, a);
+    const double2 ainv = c_div(make_double2(1, 0), a);
+    // right-hand side weights of the 10 pole-independent vectors (as rexi_phi)
+    double2 sw[10];
+    sw[0] = c_scale(a2, P);
+    sw[1] = c_scale(a, -P * T);
+    sw[2] = a3;
+    sw[3] = c_scale(a, 2.0 * T * T);
+    sw[4] = make_double2(T * T * P, 0);
+    sw[5] = c_scale(ainv, -P * T * T * T);
+    sw[6] = c_scale(ainv, T * T * T * T);
+    sw[7] = c_scale(a, -P * T * ir);
+    sw[8] = c_scale(ainv, P * T * T * T * ir);
+    sw[9] = make_double2(2.0 * P * T * T * ir, 0);
+    const double2* V = d.V;
+    double2* ph = PH + ((long long)g * nc + base) * 32 + lane;
+    double2* outp = d.part + (size_t)g * 3 * nc + base;
+    auto rhs = [&](int k, int) -> double2 {
+        const int row = base + par + 2 * k;
+        double2 v = make_double2(0, 0);
+#pragma unroll
+        for (int q = 0; q < 10; q++) v = c_add(v, c_mul(sw[q], ld(&V[(size_t)q * nc + row])));
+        return v;
+    };
+    auto out = [&](int k, int, double2 x) {
+        const int i = par + 2 * k;
+        ph[(long long)i * 32] = x;
+        rx_warp_sum(bt, x, outp + i, lane);
+    };
+    const long long gl = (long long)g * nc * 32 + lane;
+    band_solve_stored<2, (MAXN + 1) / 2, 1>(Np, band_ref(d.fphi, d.pphi, d, gl, base, N, par), rhs, out);
+}
+
+template <int MAXN>
+__global__ void __launch_bounds__(64) k_rexi_vel_st(RexiDev d, const double2* __restrict__ PH) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int L = d.L;
+    if (warp >= 2 * (2 * L + 1) * d.ngroups) return;
+    int g, m, par;
+    rx_warp_index(d, warp, g, m, par);
+    const int N = L + 1 - (m < 0 ? -m : m);
+    const int Np = (N - par + 1) >> 1;
+    if (Np <= 0) return;
+    const int base = block_off(L, m);
+    const int nc = d.ncplx;
+    const int pole = g * 32 + lane;
+    const bool valid = pole < d.npoles;
+    const double2 a = d.alpha[valid ? pole : 0];
+    const double2 bt = valid ? d.beta[pole] : make_double2(0, 0);
+    const double T = d.T, ir = d.ir, dm = m;
+    const double2* V = d.V;
+    const double2* ph = PH + ((long long)g * nc + base) * 32 + lane;
+    double2* outp = d.part + (size_t)g * 3 * nc + base;
+    auto P = [&](int i) -> double2 { return (i >= 0 && i < N) ? ph[(long long)i * 32] : make_double2(0, 0); };
+    auto cf = [&](int i, int q) -> double { return RX_LDG(d.coef + (size_t)(base + i) * 4 + q); };
+    // D phi of row i (truncated (1-mu^2) d/dmu), zero outside the block
+    auto Dp = [&](int i) -> double2 {
+        if (i < 0 || i >= N) return make_double2(0, 0);
+        return c_add(c_scale(P(i - 1), cf(i, 2)), c_scale(P(i + 1), cf(i, 3)));
+    };
+    // rhsa = a u0 + a ir i m phi - T mu(v0) - T ir mu(D phi)
+    // rhsb = T mu(u0) + T ir mu(i m phi) + a v0 + a ir D phi   (as rexi_lane)
+    int last = -1;
+    double2 xa = make_double2(0, 0), xb = make_double2(0, 0);
+    auto rhs2 = [&](int k, int r) -> double2 {
+        if (k != last) {
+            const int i = par + 2 * k, row = base + i;
+            const double Rl = cf(i, 0), Sh = cf(i, 1);
+            const double2 dcur = Dp(i), dprev = Dp(i - 1), dnext = Dp(i + 1);
+            const double2 pc = P(i), plo = P(i - 1), phi_hi = P(i + 1);
+            const double2 mud = c_add(c_scale(dprev, Rl), c_scale(dnext, Sh));
+            const double2 mup = c_add(c_scale(plo, Rl), c_scale(phi_hi, Sh));
+            const double2 u0 = ld(&V[(size_t)10 * nc + row]), v0 = ld(&V[(size_t)11 * nc + row]);
+            const double2 mv = ld(&V[(size_t)12 * nc + row]), mu0 = ld(&V[(size_t)13 * nc + row]);
+            xa = c_mul(a, u0);
+            xa = c_add(xa, c_mul(a, c_scale(c_im(pc, dm), ir)));
+            xa = c_sub(xa, c_scale(mv, T));
+            xa = c_sub(xa, c_scale(mud, T * ir));
+            xb = c_scale(mu0, T);
+            xb = c_add(xb, c_scale(c_im(mup, dm), T * ir));
+            xb = c_add(xb, c_mul(a, v0));
+            xb = c_add(xb, c_mul(a, c_scale(dcur, ir)));
+            last = k;
+        }
+        return r == 0 ? xa : xb;
+    };
+    auto out2 = [&](int k, int r, double2 x) {
+        const int i = par + 2 * k;
+        rx_warp_sum(bt, x, outp + (size_t)(1 + r) * nc + i, lane);
+    };
+    const long long gl = (long long)g * nc * 32 + lane;
+    band_solve_stored<1, (MAXN + 1) / 2, 2>(Np, band_ref(d.fvel, d.pvel, d, gl, base, N, par), rhs2, out2);
 }
 
 // ------------------------------------------------------------ non-Robert form (SWERexiSPH)
@@ -560,7 +705,21 @@ static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     const RexiDev d = rexi_dev(R);
     const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
     const unsigned nb = (unsigned)((nthreads + 63) / 64);
-    if (d.fphi) {  // factors stored at plan creation: substitutions only
+    if (d.fphi && R->PHr) {
+        // factors stored at plan creation: substitutions only, a Phi phase and
+        // a velocity phase of one warp per (pole group, m-block, parity)
+        const unsigned nb2 = 2 * nb;
+        if (L + 1 <= 64) {
+            k_rexi_phi_st<64><<<nb2, 64, 0, s>>>(d, R->PHr);
+            k_rexi_vel_st<64><<<nb2, 64, 0, s>>>(d, R->PHr);
+        } else if (L + 1 <= 128) {
+            k_rexi_phi_st<128><<<nb2, 64, 0, s>>>(d, R->PHr);
+            k_rexi_vel_st<128><<<nb2, 64, 0, s>>>(d, R->PHr);
+        } else {
+            k_rexi_phi_st<256><<<nb2, 64, 0, s>>>(d, R->PHr);
+            k_rexi_vel_st<256><<<nb2, 64, 0, s>>>(d, R->PHr);
+        }
+    } else if (d.fphi) {
         if (L + 1 <= 64) k_rexi_solve<64, false, true><<<nb, 64, 0, s>>>(d);
         else if (L + 1 <= 128) k_rexi_solve<128, false, true><<<nb, 64, 0, s>>>(d);
         else k_rexi_solve<256, false, true><<<nb, 64, 0, s>>>(d);
@@ -585,7 +744,8 @@ static void rexi_free(RexiPlan* R) {
     if (R->exec) cudaGraphExecDestroy(R->exec);
     if (R->graph) cudaGraphDestroy(R->graph);
     void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V,  R->part, R->X,  R->Xr, R->F,
-                    R->flag,  R->fphi, R->fvel, R->pphi, R->pvel, R->PH, R->XY,   R->FXY, R->Xs, R->Fs, R->glp};
+                    R->flag,  R->fphi, R->fvel, R->pphi, R->pvel, R->PH, R->XY,   R->FXY, R->Xs, R->Fs, R->glp,
+                    R->PHr};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete R;
@@ -723,6 +883,7 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
             RX_TRY(cudaMalloc(&R->fvel, sizeof(double2) * 4 * (size_t)plane));
             RX_TRY(cudaMalloc(&R->pphi, (size_t)plane));
             RX_TRY(cudaMalloc(&R->pvel, (size_t)plane));
+            if (p->robert) RX_TRY(cudaMalloc(&R->PHr, sizeof(double2) * (size_t)plane));
             R->plane = plane;
             const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
             k_rexi_factor<<<(unsigned)((nthreads + 63) / 64), 64>>>(rexi_dev(R));
