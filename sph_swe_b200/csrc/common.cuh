@@ -110,12 +110,13 @@ int ring_synthesis_cplx(const Handle* h, const double2* F, long long ldF, double
 // Legendre stage (FP64).  Real: spectral packed for degree lmax (L or L+1),
 // m = 0..min(lmax, L).  Complex: m = -L..L, layout n*n+n+m.
 int legendre_kernels_init();  // loads the FP64 Legendre kernels (lazy module loading)
-// exact_m0 != 0 (mixed handles): the m = 0 column in FP64 after the tensor-core
-// stage.  For spectra of Robert velocities U = u cos(phi), whose m = 0 part
-// vanishes like cos(phi)^2 at the poles while each term P_l^0 does not: the
-// mixed form's error there, relative to the terms, becomes a large relative
-// error of u = U / cos(phi) near the poles.  Orders m >= 1 vanish like the
-// terms (cos(phi)^m) and keep the mixed form's accuracy.
+// exact_m0 != 0 (mixed handles): the orders m = 0 and 1 in FP64 after the
+// tensor-core stage.  For spectra of Robert velocities U = u cos(phi): near the
+// poles their m = 0 part vanishes like cos(phi)^2 while each term P_l^0 does
+// not, and their m = 1 part is O(cos(phi)) while the largest term of a row
+// grows like l^1.5 cos(phi); the mixed form's error, relative to the terms,
+// would become a large relative error of u = U / cos(phi) at the polar rings.
+// Orders m >= 2 keep the mixed form's accuracy.
 // nobuf != 0: no kernel variant that needs the handle's prepared-operand
 // buffer (which a call may grow): the int8 kernel that stages B itself
 int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_spec, int lmax, double2* F,
@@ -123,7 +124,8 @@ int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_s
 // wmode 0: Gauss weights; 1: Gauss weights / cos(phi) -- the input then holds
 // cos(phi) times the integrand (e.g. u / cos(phi) analysed from u), which keeps
 // it bounded at the polar rings, where the mixed form's per-column scales would
-// otherwise be set by a 1/cos(phi) growth
+// otherwise be set by a 1/cos(phi) growth; on mixed handles these analyses of
+// velocity-derived fields also take the orders m = 0, 1 in FP64
 int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, double2* spec, long long ld_spec,
                            int lmax, int batch, cudaStream_t s, int wmode = 0);
 int legendre_synthesis_cplx(const Handle* h, const double2* spec, long long ld_spec, double2* F, long long ldF,
