@@ -238,66 +238,94 @@ __host__ __device__ bool band_factor_store(int Np, Entry entry, const BandRef& s
 }
 
 // Forward elimination and back substitution of band_solve with the factors
-// that band_factor_store wrote.
+// that band_factor_store wrote.  The factors of PF rows are loaded together
+// before those rows are processed (they do not depend on the right-hand
+// sides), so that a lane keeps several rows' loads in flight; the arithmetic
+// is that of band_solve, row by row in the same order.
 template <int H, int MAXR, int NR, class Rhs, class Out>
 __host__ __device__ void band_solve_stored(int Np, const BandRef& st, Rhs rhs, Out out) {
     constexpr int W = 2 * H + 1;
+    constexpr int PF = 4;                  // rows per prefetch group, forward
+    constexpr int PB = H >= 2 ? 2 : 4;     // rows per prefetch group, backward
     double2 y[MAXR][NR];
     double2 wr[H + 1][NR];
 #pragma unroll
     for (int i = 0; i <= H; i++)
 #pragma unroll
         for (int r = 0; r < NR; r++) wr[i][r] = i < Np ? rhs(i, r) : make_double2(0, 0);
-    for (int k = 0; k < Np; k++) {
-        const long long e = st.i0 + (long long)k * st.lanes;
-        const int p = RX_LDG(&st.pv[e]);
+    for (int k0 = 0; k0 < Np; k0 += PF) {
+        int pvs[PF];
+        double2 lm[PF][H];
 #pragma unroll
-        for (int i = 1; i <= H; i++) {
-            const bool sw = (p == i);
+        for (int u = 0; u < PF; u++) {
+            const int k = k0 + u < Np ? k0 + u : Np - 1;
+            const long long e = st.i0 + (long long)k * st.lanes;
+            pvs[u] = RX_LDG(&st.pv[e]);
 #pragma unroll
-            for (int r = 0; r < NR; r++) {
-                const double2 t0 = wr[0][r], ti = wr[i][r];
-                wr[0][r] = sw ? ti : t0;
-                wr[i][r] = sw ? t0 : ti;
+            for (int i = 1; i <= H; i++) lm[u][i - 1] = ld(&st.f[(2 * H + i) * st.plane + e]);
+        }
+#pragma unroll
+        for (int u = 0; u < PF; u++) {
+            const int k = k0 + u;
+            if (k >= Np) break;
+            const int p = pvs[u];
+#pragma unroll
+            for (int i = 1; i <= H; i++) {
+                const bool sw = (p == i);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const double2 t0 = wr[0][r], ti = wr[i][r];
+                    wr[0][r] = sw ? ti : t0;
+                    wr[i][r] = sw ? t0 : ti;
+                }
             }
+#pragma unroll
+            for (int r = 0; r < NR; r++) y[k][r] = wr[0][r];
+#pragma unroll
+            for (int i = 1; i <= H; i++) {
+                const double2 l = lm[u][i - 1];
+#pragma unroll
+                for (int r = 0; r < NR; r++) wr[i][r] = c_sub(wr[i][r], c_mul(l, wr[0][r]));
+            }
+#pragma unroll
+            for (int i = 0; i < H; i++)
+#pragma unroll
+                for (int r = 0; r < NR; r++) wr[i][r] = wr[i + 1][r];
+            const int rn = k + 1 + H;
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[H][r] = rn < Np ? rhs(rn, r) : make_double2(0, 0);
         }
-#pragma unroll
-        for (int r = 0; r < NR; r++) y[k][r] = wr[0][r];
-#pragma unroll
-        for (int i = 1; i <= H; i++) {
-            const double2 l = ld(&st.f[(2 * H + i) * st.plane + e]);
-#pragma unroll
-            for (int r = 0; r < NR; r++) wr[i][r] = c_sub(wr[i][r], c_mul(l, wr[0][r]));
-        }
-#pragma unroll
-        for (int i = 0; i < H; i++)
-#pragma unroll
-            for (int r = 0; r < NR; r++) wr[i][r] = wr[i + 1][r];
-        const int rn = k + 1 + H;
-#pragma unroll
-        for (int r = 0; r < NR; r++) wr[H][r] = rn < Np ? rhs(rn, r) : make_double2(0, 0);
     }
     double2 x[W][NR];
 #pragma unroll
     for (int j = 0; j < W; j++)
 #pragma unroll
         for (int r = 0; r < NR; r++) x[j][r] = make_double2(0, 0);
-    for (int k = Np - 1; k >= 0; k--) {
-        const long long e = st.i0 + (long long)k * st.lanes;
-        const double2 rd = ld(&st.f[e]);
-        double2 u[W];
+    for (int k1 = Np - 1; k1 >= 0; k1 -= PB) {
+        double2 rds[PB], us[PB][W];
 #pragma unroll
-        for (int j = 1; j < W; j++) u[j] = ld(&st.f[j * st.plane + e]);
+        for (int u = 0; u < PB; u++) {
+            const int k = k1 - u >= 0 ? k1 - u : 0;
+            const long long e = st.i0 + (long long)k * st.lanes;
+            rds[u] = ld(&st.f[e]);
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
-            double2 s = y[k][r];
+            for (int j = 1; j < W; j++) us[u][j] = ld(&st.f[j * st.plane + e]);
+        }
 #pragma unroll
-            for (int j = 1; j < W; j++) s = c_sub(s, c_mul(u[j], x[j - 1][r]));
-            const double2 xk = c_mul(s, rd);
+        for (int u = 0; u < PB; u++) {
+            const int k = k1 - u;
+            if (k < 0) break;
 #pragma unroll
-            for (int j = W - 1; j > 0; j--) x[j][r] = x[j - 1][r];
-            x[0][r] = xk;
-            out(k, r, xk);
+            for (int r = 0; r < NR; r++) {
+                double2 s = y[k][r];
+#pragma unroll
+                for (int j = 1; j < W; j++) s = c_sub(s, c_mul(us[u][j], x[j - 1][r]));
+                const double2 xk = c_mul(s, rds[u]);
+#pragma unroll
+                for (int j = W - 1; j > 0; j--) x[j][r] = x[j - 1][r];
+                x[0][r] = xk;
+                out(k, r, xk);
+            }
         }
     }
 }
