@@ -32,7 +32,7 @@ constexpr int BYTES = OFF_BAR + 256;
 constexpr int NCONS = 256;
 constexpr int CONS_WARP0 = 2;
 constexpr int NT = 64 + NCONS;
-constexpr int PREP_NT = 384;
+constexpr int PREP_NT = 256;
 static_assert(STAGE % 1024 == 0 && BYTES <= 227 * 1024, "shared memory plan");
 }  // namespace li8b
 
@@ -40,160 +40,47 @@ static_assert(STAGE % 1024 == 0 && BYTES <= 227 * 1024, "shared memory plan");
 __host__ __device__ constexpr int i8b_chunk(int nc) { return 2 * li8::ND * 2 * nc * 16; }
 
 // ------------------------------------------------------------------ B preparation
-// CTA per (order m = blockIdx.x, column tile ct = blockIdx.y).  A task is one
-// field and one 16-K group of one parity (synthesis) or 8 latitudes of one
-// 16-K group of both parities (analysis): its values come in with contiguous
-// loads, its digit planes go out as 16-byte (8-byte) rows.  A first pass takes
-// the column maxima (the same as the in-kernel producers': the synthesis over
-// all degrees of the order, the analysis max_j |north_j| + |south_j|), a
-// second writes the digits; when every task of the CTA fits in one trip the
-// values stay in registers between the passes, otherwise they are read again.
-__device__ __forceinline__ void i8b_colmax(unsigned long long* cmax, int c, double mr, double mi) {
-    if (mr > 0.0) atomicMax(&cmax[c], i8_bits(mr));
-    if (mi > 0.0) atomicMax(&cmax[c + 1], i8_bits(mi));
-}
-
-// column exponents of the CTA's columns into ecol, their scales into scl
-template <int NC>
-__device__ __forceinline__ void i8b_exps(const I8Args& a, const unsigned long long* cmax, double2* scl, int m, int ct) {
+// CTA per (order m = blockIdx.x, column tile ct = blockIdx.y).  Dir is SynI8 or
+// AnaI8: their scan / digits are the producer passes of the kernel that stages
+// B itself, here over the whole K range of the order at once (a first pass
+// takes the column maxima, a second re-reads the values, mostly from L1/L2,
+// and writes the digits).  Small CTAs of 64 registers a thread keep several
+// per SM; tasks that kept their values in registers between the passes, with
+// 16-byte digit rows, measured slower (their larger CTAs fit once per SM).
+template <class Dir, int NC>
+__global__ void __launch_bounds__(li8b::PREP_NT) k_i8b_prep(I8Args a, const double2* __restrict__ in) {
+    __shared__ unsigned long long cmax[NC];
+    __shared__ double2 scl[NC];
+    I8Tile p;
+    p.t = 0;
+    p.m = blockIdx.x;
+    p.ct = blockIdx.y;
+    p.rt = 0;
+    p.nch = Dir::prep_nch(a, p.m);
+    if (threadIdx.x < NC) cmax[threadIdx.x] = 0ull;
+    __syncthreads();
+    const int ns = Dir::tasks(2 * p.nch);
+    // the same trip count on every thread: the maxima are reduced with warp shuffles
+    const int trips = (ns + li8b::PREP_NT - 1) / li8b::PREP_NT;
+    for (int it = 0; it < trips; it++) {
+        const int task = threadIdx.x + it * li8b::PREP_NT;
+        Dir::scan(a, p, task, task < ns, in, cmax);
+    }
+    __syncthreads();
     if (threadIdx.x < NC) {
         const int e = i8_exp(__longlong_as_double((long long)cmax[threadIdx.x]));
-        a.ecol[((long long)ct * a.nm + m) * NC + threadIdx.x] = e;
+        a.ecol[((long long)p.ct * a.nm + p.m) * NC + threadIdx.x] = e;
         scl[threadIdx.x] = i8_scale(e);
     }
-}
-
-template <int NC>
-__global__ void __launch_bounds__(li8b::PREP_NT) k_i8b_prep_syn(I8Args a, const double2* __restrict__ spec) {
-    constexpr int NF = NC / 2;
-    __shared__ unsigned long long cmax[NC];
-    __shared__ double2 scl[NC];
-    const int m = blockIdx.x, ct = blockIdx.y;
-    const int nz = 2 * ((a.lmax - m) / 64 + 1);  // 16-K groups per parity (2 per chunk)
-    const int ntask = 2 * nz * NF;
-    const bool one = ntask <= li8b::PREP_NT;
-    if (threadIdx.x < NC) cmax[threadIdx.x] = 0ull;
     __syncthreads();
-    double2 v[16];
-    // task t: parity t & 1, group zl, field fl; degrees l = m + 32 zl + parity + 2 k
-    auto load = [&](int t) {
-        const int par = t & 1, zl = (t >> 1) % nz, f = ct * NF + (t >> 1) / nz;
-        const double2* src = spec + (long long)(f < a.batch ? f : 0) * a.ld_spec;
-        const int l0 = m + 32 * zl + par;
+    unsigned char* out = a.B + ((long long)p.ct * a.cpt + Dir::prep_coff(a, p.m)) * i8b_chunk(NC);
+    auto put = [out](int par, int zl, int c, int q, const uint32_t* o) {
+        unsigned char* ch = out + (long long)(zl >> 1) * i8b_chunk(NC);
 #pragma unroll
-        for (int k = 0; k < 16; k++) {
-            const int l = l0 + 2 * k;
-            v[k] = (f < a.batch && l <= a.lmax) ? src[pidx(a.lmax, l, m)] : make_double2(0.0, 0.0);
-        }
+        for (int d = 0; d < li8::ND; d++)
+            *reinterpret_cast<uint32_t*>(ch + (((par * li8::ND + d) * 2 + (zl & 1)) * NC + c) * 16 + 4 * q) = o[d];
     };
-    for (int t = threadIdx.x; t < ntask; t += li8b::PREP_NT) {
-        load(t);
-        double mr = 0.0, mi = 0.0;
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            mr = fmax(mr, fabs(v[k].x));
-            mi = fmax(mi, fabs(v[k].y));
-        }
-        i8b_colmax(cmax, 2 * ((t >> 1) / nz), mr, mi);
-    }
-    __syncthreads();
-    i8b_exps<NC>(a, cmax, scl, m, ct);
-    __syncthreads();
-    unsigned char* out = a.B + ((long long)ct * a.cpt + i8b_syn_coff(a.lmax, m)) * i8b_chunk(NC);
-    for (int t = threadIdx.x; t < ntask; t += li8b::PREP_NT) {
-        if (!one) load(t);
-        const int par = t & 1, zl = (t >> 1) % nz, fl = (t >> 1) / nz;
-        unsigned char* row = out + (long long)(zl >> 1) * i8b_chunk(NC) + ((par * li8::ND * 2 + (zl & 1)) * NC + 2 * fl) * 16;
-#pragma unroll
-        for (int ri = 0; ri < 2; ri++) {
-            const double2 sc = scl[2 * fl + ri];
-            uint32_t o[4][4];  // [group of 4 K][plane]
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int k = 4 * q;
-                const double x0 = ri ? v[k].y : v[k].x, x1 = ri ? v[k + 1].y : v[k + 1].x;
-                const double x2 = ri ? v[k + 2].y : v[k + 2].x, x3 = ri ? v[k + 3].y : v[k + 3].x;
-                i8_planes4(i8_word(x0, sc.x, sc.y), i8_word(x1, sc.x, sc.y), i8_word(x2, sc.x, sc.y),
-                           i8_word(x3, sc.x, sc.y), o[q]);
-            }
-#pragma unroll
-            for (int d = 0; d < li8::ND; d++)
-                *reinterpret_cast<uint4*>(row + (d * 2 * NC + ri) * 16) = make_uint4(o[0][d], o[1][d], o[2][d], o[3][d]);
-        }
-    }
-}
-
-template <int NC>
-__global__ void __launch_bounds__(li8b::PREP_NT) k_i8b_prep_ana(I8Args a, const double2* __restrict__ F) {
-    constexpr int NF = NC / 2;
-    __shared__ unsigned long long cmax[NC];
-    __shared__ double2 scl[NC];
-    const int m = blockIdx.x, ct = blockIdx.y;
-    const int nz = 2 * i8b_ana_nch(a.nh);  // 16-latitude groups
-    const int ntask = 2 * nz * NF;
-    const bool one = ntask <= li8b::PREP_NT;
-    if (threadIdx.x < NC) cmax[threadIdx.x] = 0ull;
-    __syncthreads();
-    double2 n[8], sv[8];
-    // task t: half t & 1 of group zl, field fl: latitudes j = 16 zl + 8 half + k
-    auto load = [&](int t) {
-        const int zl = (t >> 1) % nz, f = ct * NF + (t >> 1) / nz;
-        const int j0 = 16 * zl + 8 * (t & 1);
-        const double2* src = F + (long long)(f < a.batch ? f : 0) * a.ldF + (long long)m * a.nlat;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const bool in = f < a.batch && j0 + k < a.nh;
-            n[k] = in ? src[j0 + k] : make_double2(0.0, 0.0);
-            sv[k] = in ? src[a.nlat - 1 - j0 - k] : make_double2(0.0, 0.0);
-        }
-    };
-    for (int t = threadIdx.x; t < ntask; t += li8b::PREP_NT) {
-        load(t);
-        double mr = 0.0, mi = 0.0;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            mr = fmax(mr, fabs(n[k].x) + fabs(sv[k].x));
-            mi = fmax(mi, fabs(n[k].y) + fabs(sv[k].y));
-        }
-        i8b_colmax(cmax, 2 * ((t >> 1) / nz), mr, mi);
-    }
-    __syncthreads();
-    i8b_exps<NC>(a, cmax, scl, m, ct);
-    __syncthreads();
-    unsigned char* out = a.B + ((long long)ct * a.cpt + (long long)m * i8b_ana_nch(a.nh)) * i8b_chunk(NC);
-    // the scale is applied to north and south first (exact), so north +/- south
-    // is rounded once, as in the in-kernel producers
-    auto w = [](double t, double s2) {
-        const uint32_t v = (uint32_t)__double2loint(fma(t, s2, 0x1.8p52));
-        return (v + 0x808080u) ^ 0x808080u;
-    };
-    for (int t = threadIdx.x; t < ntask; t += li8b::PREP_NT) {
-        if (!one) load(t);
-        const int h = t & 1, zl = (t >> 1) % nz, fl = (t >> 1) / nz;
-        unsigned char* grp = out + (long long)(zl >> 1) * i8b_chunk(NC) + 8 * h;
-#pragma unroll
-        for (int ri = 0; ri < 2; ri++) {
-            const double2 sc = scl[2 * fl + ri];
-            double p[8], q[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const double a_ = (ri ? n[k].y : n[k].x) * sc.x, b_ = (ri ? sv[k].y : sv[k].x) * sc.x;
-                p[k] = a_ + b_;
-                q[k] = a_ - b_;
-            }
-#pragma unroll
-            for (int par = 0; par < 2; par++) {
-                const double* x = par ? q : p;
-                uint32_t o0[4], o1[4];
-                i8_planes4(w(x[0], sc.y), w(x[1], sc.y), w(x[2], sc.y), w(x[3], sc.y), o0);
-                i8_planes4(w(x[4], sc.y), w(x[5], sc.y), w(x[6], sc.y), w(x[7], sc.y), o1);
-#pragma unroll
-                for (int d = 0; d < li8::ND; d++)
-                    *reinterpret_cast<uint2*>(grp + (((par * li8::ND + d) * 2 + (zl & 1)) * NC + 2 * fl + ri) * 16) =
-                        make_uint2(o0[d], o1[d]);
-            }
-        }
-    }
+    for (int task = threadIdx.x; task < ns; task += li8b::PREP_NT) Dir::digits(a, p, task, 0, in, scl, put);
 }
 
 // ------------------------------------------------------------------ main kernel

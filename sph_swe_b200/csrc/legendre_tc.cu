@@ -1240,8 +1240,8 @@ static int tc_attr() {
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8b<AnaI8<NC>, NC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, li8b::BYTES));
     cudaFuncAttributes fa;  // load the preparation kernels now (lazy module loading)
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep_syn<NC>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep_ana<NC>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep<SynI8<NC>, NC>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep<AnaI8<NC>, NC>));
     return SPH_OK;
 }
 
@@ -1531,16 +1531,13 @@ static int i8b_launch(const Handle* h, const MixedTables* Tc, bool syn, const CU
     const dim3 pg((unsigned)a.nm, (unsigned)a.nct);
     const int grid = std::max(1, std::min(a.ntiles, g_tc_sms > 0 ? g_tc_sms : 148));
     if (nc == 16) {
-        if (syn) k_i8b_prep_syn<16><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
-        else k_i8b_prep_ana<16><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
+        k_i8b_prep<Dir<16>, 16><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
         k_legendre_i8b<Dir<16>, 16><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
     } else if (nc == 32) {
-        if (syn) k_i8b_prep_syn<32><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
-        else k_i8b_prep_ana<32><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
+        k_i8b_prep<Dir<32>, 32><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
         k_legendre_i8b<Dir<32>, 32><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
     } else {
-        if (syn) k_i8b_prep_syn<64><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
-        else k_i8b_prep_ana<64><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
+        k_i8b_prep<Dir<64>, 64><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
         k_legendre_i8b<Dir<64>, 64><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
     }
     SPH_CUDA_TRY(cudaGetLastError());
