@@ -310,6 +310,12 @@ def run_ours(args, rank, world):
         "vector_u_vs_fp64_area_weighted": _per_field_rel_area(mx.u, f64.u, mx.s.w),
         "vector_v_vs_fp64_area_weighted": _per_field_rel_area(mx.v, f64.v, mx.s.w),
     }
+    # the forward vector transform alone: the mixed analysis of the FP64 grids
+    # against the FP64 analysis of the same grids
+    zm, dm = mx.s.vec_spat_to_SH(f64.u, f64.v)
+    accuracy["vorticity_analysis_vs_fp64"] = _per_field_rel(zm, f64.z)
+    accuracy["divergence_analysis_vs_fp64"] = _per_field_rel(dm, f64.d)
+    del zm, dm
 
     ms = {}
     clocks = None
