@@ -22,22 +22,31 @@
 // each) combine the four exact int32 group sums of a finished tile in FP64
 // and write it.  Every wait is bounded as in the other tensor-core kernels.
 
+// bytes of one B chunk of nc columns
+__host__ __device__ constexpr int i8b_chunk(int nc) { return 2 * li8::ND * 2 * nc * 16; }
+
 namespace li8b {
-constexpr int NSTAGE = 4;
-constexpr int A_STAGE = li8::A_STAGE;                  // 32 KB: both parities' A of a chunk
-constexpr int B_MAX = 2 * li8::ND * 2 * 64 * 16;       // 16 KB: one B chunk of 64 columns
-constexpr int STAGE = A_STAGE + B_MAX;
-constexpr int OFF_BAR = NSTAGE * STAGE;
-constexpr int BYTES = OFF_BAR + 256;
+constexpr int A_STAGE = li8::A_STAGE;  // 32 KB: both parities' A of a chunk
+constexpr int SMEM_MAX = 227 * 1024;
+// A load takes ~2 us to land under full load, so the ring holds as many
+// stages (A + B of one chunk) as the shared memory allows: 6, 5 or 4 at 16,
+// 32 or 64 columns
+template <int NC>
+constexpr int stage() { return A_STAGE + i8b_chunk(NC); }
+template <int NC>
+constexpr int nstage() { return (SMEM_MAX - 256) / stage<NC>(); }
+template <int NC>
+constexpr int off_bar() { return nstage<NC>() * stage<NC>(); }
+template <int NC>
+constexpr int bytes() { return off_bar<NC>() + 256; }
+constexpr int MAXSTAGE = 8;
 constexpr int NCONS = 256;
 constexpr int CONS_WARP0 = 2;
 constexpr int NT = 64 + NCONS;
 constexpr int PREP_NT = 256;
-static_assert(STAGE % 1024 == 0 && BYTES <= 227 * 1024, "shared memory plan");
+static_assert(stage<16>() % 1024 == 0 && stage<32>() % 1024 == 0 && stage<64>() % 1024 == 0, "stage alignment");
+static_assert(nstage<16>() <= MAXSTAGE && nstage<64>() >= 4, "stage count");
 }  // namespace li8b
-
-// bytes of one B chunk of nc columns
-__host__ __device__ constexpr int i8b_chunk(int nc) { return 2 * li8::ND * 2 * nc * 16; }
 
 // ------------------------------------------------------------------ B preparation
 // CTA per (order m = blockIdx.x, column tile ct = blockIdx.y).  Dir is SynI8 or
@@ -92,11 +101,12 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
     constexpr uint32_t NCOLS = (uint32_t)(NACC * TCOLS) <= 256u ? 256u : 512u;
     constexpr int BCH = i8b_chunk(NC);
     constexpr int HALF = NC / 2;
-    static_assert(NC % 16 == 0 && NC <= 64 && BCH <= li8b::B_MAX, "tile shape");
+    constexpr int NSTAGE = li8b::nstage<NC>(), STAGE = li8b::stage<NC>();
+    static_assert(NC % 16 == 0 && NC <= 64, "tile shape");
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(smem + li8b::OFF_BAR);
-    unsigned long long* empty = full + li8b::NSTAGE;
-    unsigned long long* accfull = empty + li8b::NSTAGE;  // [NACC]
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(smem + li8b::off_bar<NC>());
+    unsigned long long* empty = full + NSTAGE;
+    unsigned long long* accfull = empty + NSTAGE;  // [NACC]
     unsigned long long* accempty = accfull + 2;           // [NACC]
     volatile int* abort = reinterpret_cast<volatile int*>(accempty + 2);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(accempty + 2) + 1;
@@ -107,7 +117,7 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
 
     if (warp == 0) tmem_alloc(smem_u32(tslot), NCOLS);
     if (tid == 32) {
-        for (int i = 0; i < li8b::NSTAGE; i++) {
+        for (int i = 0; i < NSTAGE; i++) {
             mbar_init(smem_u32(&full[i]), 1);
             mbar_init(smem_u32(&empty[i]), 1);
         }
@@ -133,14 +143,14 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
             for (I8Tile p = first; p.t < a.ntiles && ok; p = i8_tile<Dir>(a, p.t + gridDim.x)) {
                 const unsigned char* bsrc = a.B + ((long long)p.ct * a.cpt + Dir::prep_coff(a, p.m)) * BCH;
                 for (int kc = 0; kc < p.nch; kc++, q++) {
-                    const int s = q % li8b::NSTAGE;
-                    if (q >= li8b::NSTAGE &&
-                        !mbar_wait_abort(smem_u32(&empty[s]), (uint32_t)((q / li8b::NSTAGE - 1) & 1), abort)) {
+                    const int s = q % NSTAGE;
+                    if (q >= NSTAGE &&
+                        !mbar_wait_abort(smem_u32(&empty[s]), (uint32_t)((q / NSTAGE - 1) & 1), abort)) {
                         ok = false;
                         break;
                     }
                     const uint32_t fb = smem_u32(&full[s]);
-                    unsigned char* st = smem + s * li8b::STAGE;
+                    unsigned char* st = smem + s * STAGE;
                     mbar_expect_tx(fb, (uint32_t)(li8::A_STAGE + BCH));
 #pragma unroll
                     for (int par = 0; par < 2; par++) {
@@ -167,13 +177,13 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
                 }
                 const uint32_t tacc = tmem + (uint32_t)(b * TCOLS);
                 for (int kc = 0; kc < p.nch; kc++, q++) {
-                    const int s = q % li8b::NSTAGE;
-                    if (!mbar_wait_abort(smem_u32(&full[s]), (uint32_t)((q / li8b::NSTAGE) & 1), abort)) {
+                    const int s = q % NSTAGE;
+                    if (!mbar_wait_abort(smem_u32(&full[s]), (uint32_t)((q / NSTAGE) & 1), abort)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t As = smem_u32(smem + s * li8b::STAGE);
+                    const uint32_t As = smem_u32(smem + s * STAGE);
                     const uint32_t Bs = As + (uint32_t)li8b::A_STAGE;
                     constexpr uint32_t bplane = 2u * NC * 16u;
 #pragma unroll
@@ -227,8 +237,8 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
         if (tid == 32) {
             // let the last issued chunk finish before its tensor memory is freed
             if (issued >= 0) {
-                const uint32_t bar = smem_u32(&empty[issued % li8b::NSTAGE]);
-                const uint32_t ph = (uint32_t)((issued / li8b::NSTAGE) & 1);
+                const uint32_t bar = smem_u32(&empty[issued % NSTAGE]);
+                const uint32_t ph = (uint32_t)((issued / NSTAGE) & 1);
                 const uint64_t t0 = globaltimer();
                 while (!mbar_try(bar, ph) && globaltimer() - t0 < tc::WAIT_NS) {
                 }
@@ -237,9 +247,9 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
         }
         if (tid == 0) {
             // the loads still in flight land before the CTA's shared memory is released
-            for (int c = loaded - 1; c >= 0 && c >= loaded - li8b::NSTAGE; c--) {
-                const uint32_t bar = smem_u32(&full[c % li8b::NSTAGE]);
-                const uint32_t ph = (uint32_t)((c / li8b::NSTAGE) & 1);
+            for (int c = loaded - 1; c >= 0 && c >= loaded - NSTAGE; c--) {
+                const uint32_t bar = smem_u32(&full[c % NSTAGE]);
+                const uint32_t ph = (uint32_t)((c / NSTAGE) & 1);
                 const uint64_t t0 = globaltimer();
                 while (!mbar_try(bar, ph) && globaltimer() - t0 < tc::WAIT_NS) {
                 }

@@ -1236,9 +1236,9 @@ static int tc_attr() {
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8<AnaI8<NC>, NC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, li8::BYTES));
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8b<SynI8<NC>, NC>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8b::BYTES));
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8b::bytes<NC>()));
     SPH_CUDA_TRY(cudaFuncSetAttribute((const void*)k_legendre_i8b<AnaI8<NC>, NC>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8b::BYTES));
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, li8b::bytes<NC>()));
     cudaFuncAttributes fa;  // load the preparation kernels now (lazy module loading)
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep<SynI8<NC>, NC>));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_i8b_prep<AnaI8<NC>, NC>));
@@ -1532,13 +1532,13 @@ static int i8b_launch(const Handle* h, const MixedTables* Tc, bool syn, const CU
     const int grid = std::max(1, std::min(a.ntiles, g_tc_sms > 0 ? g_tc_sms : 148));
     if (nc == 16) {
         k_i8b_prep<Dir<16>, 16><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
-        k_legendre_i8b<Dir<16>, 16><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
+        k_legendre_i8b<Dir<16>, 16><<<grid, li8b::NT, li8b::bytes<16>(), s>>>(map, a, out);
     } else if (nc == 32) {
         k_i8b_prep<Dir<32>, 32><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
-        k_legendre_i8b<Dir<32>, 32><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
+        k_legendre_i8b<Dir<32>, 32><<<grid, li8b::NT, li8b::bytes<32>(), s>>>(map, a, out);
     } else {
         k_i8b_prep<Dir<64>, 64><<<pg, li8b::PREP_NT, 0, s>>>(a, in);
-        k_legendre_i8b<Dir<64>, 64><<<grid, li8b::NT, li8b::BYTES, s>>>(map, a, out);
+        k_legendre_i8b<Dir<64>, 64><<<grid, li8b::NT, li8b::bytes<64>(), s>>>(map, a, out);
     }
     SPH_CUDA_TRY(cudaGetLastError());
     return SPH_OK;
