@@ -17,10 +17,11 @@
 //
 // The main kernel has no per-chunk work besides the MMAs: warp 0 issues the
 // loads (A by the 4-D tensor map of the digit tables, B by one bulk copy into
-// the same stage), warp 1 the 10 digit-product MMAs per parity, and 8
-// consumer warps (two per tensor-memory lane quadrant, half of the columns
-// each) combine the four exact int32 group sums of a finished tile in FP64
-// and write it.  Every wait is bounded as in the other tensor-core kernels.
+// the same stage), warp 1 the 10 digit-product MMAs per parity, and 16
+// consumer warps (four per tensor-memory lane quadrant, a quarter of the
+// columns each) combine the four exact int32 group sums of a finished tile in
+// FP64 and write it: the stores of a tile, not the MMAs, pace the kernel, so
+// they are spread over as many warps as possible.  Every wait is bounded as in the other tensor-core kernels.
 
 // bytes of one B chunk of nc columns
 __host__ __device__ constexpr int i8b_chunk(int nc) { return 2 * li8::ND * 2 * nc * 16; }
@@ -40,7 +41,7 @@ constexpr int off_bar() { return nstage<NC>() * stage<NC>(); }
 template <int NC>
 constexpr int bytes() { return off_bar<NC>() + 256; }
 constexpr int MAXSTAGE = 8;
-constexpr int NCONS = 256;
+constexpr int NCONS = 512;  // 16 consumer warps: 4 per tensor-memory lane quadrant
 constexpr int CONS_WARP0 = 2;
 constexpr int NT = 64 + NCONS;
 constexpr int PREP_NT = 256;
@@ -100,7 +101,8 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
     constexpr int NACC = TCOLS <= 256 ? 2 : 1;               // tiles in flight in tensor memory
     constexpr uint32_t NCOLS = (uint32_t)(NACC * TCOLS) <= 256u ? 256u : 512u;
     constexpr int BCH = i8b_chunk(NC);
-    constexpr int HALF = NC / 2;
+    constexpr int PART = NC >= 32 ? NC / 4 : NC / 2;  // columns per consumer warp (multiples of 8)
+    constexpr int NPART = NC / PART;
     constexpr int NSTAGE = li8b::nstage<NC>(), STAGE = li8b::stage<NC>();
     static_assert(NC % 16 == 0 && NC <= 64, "tile shape");
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -200,32 +202,36 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
     } else {
         // ---------------------------------------------------------------- consumers
         // a warp reads the tensor-memory lane quadrant warp % 4 (the only one
-        // tcgen05.ld lets it access); warps 2-5 take the first half of the
-        // columns, warps 6-9 the second
+        // tcgen05.ld lets it access); warps 2-5 take the first part of the
+        // columns, warps 6-9 the second, ...; with fewer parts than warp sets
+        // (16 columns) the last sets only release the accumulator
         const int cw = warp - li8b::CONS_WARP0;
         const int qd = warp & 3, half = cw >> 2;
+        const bool active = half < NPART;
         const int r = qd * 32 + lane;
         int j = 0;
         for (I8Tile p = first; p.t < a.ntiles; p = i8_tile<Dir>(a, p.t + gridDim.x), j++) {
             const int b = j % NACC;
             // row and column exponents of this thread's outputs: loaded before the
             // wait, so their latency overlaps the tile's MMAs
-            int er[2], ec[HALF];
+            int er[2], ec[PART];
             Dir::row_exp(a, p, r, er);
-            const int* ecol = a.ecol + ((long long)p.ct * a.nm + p.m) * NC + half * HALF;
+            const int* ecol = a.ecol + ((long long)p.ct * a.nm + p.m) * NC + (active ? half : 0) * PART;
 #pragma unroll
-            for (int c = 0; c < HALF; c++) ec[c] = __ldg(ecol + c);
+            for (int c = 0; c < PART; c++) ec[c] = __ldg(ecol + c);
             const bool v = mbar_wait_abort(smem_u32(&accfull[b]), (uint32_t)((j / NACC) & 1), abort);
             if (!__all_sync(0xffffffffu, v)) break;
             tc_fence_after();
             const uint32_t base = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * TCOLS);
+            if (active) {
 #pragma unroll
-            for (int cb = 0; cb < HALF; cb += 8) {
-                const int c0 = half * HALF + cb;
-                double e[8], o[8];
-                i8_ld_combine<NC>(base + (uint32_t)c0, e);
-                i8_ld_combine<NC>(base + (uint32_t)(li8::NG * NC + c0), o);
-                Dir::epilogue(a, p, r, c0, er, ec + cb, e, o, out);
+                for (int cb = 0; cb < PART; cb += 8) {
+                    const int c0 = half * PART + cb;
+                    double e[8], o[8];
+                    i8_ld_combine<NC>(base + (uint32_t)c0, e);
+                    i8_ld_combine<NC>(base + (uint32_t)(li8::NG * NC + c0), o);
+                    Dir::epilogue(a, p, r, c0, er, ec + cb, e, o, out);
+                }
             }
             tc_fence_before();
             mbar_arrive(smem_u32(&accempty[b]));
