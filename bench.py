@@ -213,6 +213,10 @@ class Cfg1:
 
         self.s = Sph(L_CFG1, precision=prec)
         assert (self.s.nlat, self.s.nphi) == (384, 768)
+        # the autotuner picks the kernel variants for the step's batches (untimed
+        # set-up): Legendre 64 fields (scalars; the 32 pairs' U, V), rings 64 / 32
+        for b in sorted({N_SCALAR, 2 * N_PAIRS, N_PAIRS}):
+            self.s.autotune(b)
         self.spec, self.vort, self.div = spec, vort, div
         self.grid = torch.empty(N_SCALAR, self.s.nphi, self.s.nlat, dtype=torch.float64, device=dev)
         self.spec_out = torch.empty_like(spec)
@@ -450,6 +454,8 @@ def rk4_rates(dev, args):
         s0.close()
         for name, prec in (("fp64", capi.SPH_PREC_FP64), ("mixed", capi.SPH_PREC_MIXED)):
             s = Sph(L, precision=prec)
+            for b in Sph.rk4_batches(1, form):  # kernel variants per batch (untimed set-up)
+                s.autotune(b)
             p = Sph.swe_params(radius=6.371e6, dt=dt, viscosity=visc, nonlinear=form)
             st = st0.clone()
             s.swe_rk4(p, st, 3)
@@ -531,6 +537,8 @@ def t1023_rates(dev, args):
                                     robert=True)
             st0 = torch.stack([s.spat_to_SH(torch.from_numpy(h).to(dev)), z[0] / a, d[0] / a])
         p = Sph.swe_params(radius=a, dt=dt, nonlinear=2)
+        for b in Sph.rk4_batches(1, 2):  # kernel variants per batch (untimed set-up)
+            s.autotune(b)
         st = st0.clone()
         s.swe_rk4(p, st, 3)
         torch.cuda.synchronize()
@@ -601,6 +609,8 @@ def ensemble_rates(dev, args):
         groups = []
         for L, n in ENSEMBLE:
             s = Sph(L, precision=prec)
+            for b in Sph.rk4_batches(n, 2):  # variants per truncation and batch (untimed set-up)
+                s.autotune(b)
             groups.append((s, Sph.swe_params(radius=6.371e6, dt=120.0 * 63 / L, nonlinear=2), init[L].clone(), None))
         e = Ensemble(groups)
         e.step(3)

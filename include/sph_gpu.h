@@ -326,6 +326,14 @@ int sph_spat_op(sph_handle* h, int op, const double* x, const double* y, double*
  * counterpart in the reference (SHTNS picks its own algorithm at
  * shtns_set_grid, SPHConfig.hpp:324-352). */
 int sph_autotune(sph_handle* h, int batch, char* json, int cap, void* stream);
+/* Kernel families of sph_autotune_ex (bit mask).  sph_autotune takes
+ * SPH_TUNE_INT8 | SPH_TUNE_FP64: the families whose transforms of
+ * velocity-derived fields stay within the mixed form's relL2 <= 1e-6; the
+ * split-TF32 family (~3e-7 per transform) meets it for scalar fields only. */
+enum sph_tune_family { SPH_TUNE_INT8 = 1, SPH_TUNE_TF32 = 2, SPH_TUNE_FP64 = 4 };
+/* sph_autotune over the given kernel families of the tensor-core Legendre
+ * stages (the ring-FFT tile widths are always timed). */
+int sph_autotune_ex(sph_handle* h, int batch, int families, char* json, int cap, void* stream);
 /* Re-apply a table written by sph_autotune (same truncation, grid, precision). */
 int sph_tune_load(sph_handle* h, const char* json);
 /* Back to the built-in rules. */

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libsphgpu.so")
 
 SPH_OK, SPH_ERR_ARG, SPH_ERR_CUDA, SPH_ERR_SINGULAR, SPH_ERR_NAN, SPH_ERR_TIMEOUT, SPH_ERR_NOMEM = range(7)
 SPH_PREC_FP64, SPH_PREC_MIXED = 0, 1
+SPH_TUNE_INT8, SPH_TUNE_TF32, SPH_TUNE_FP64 = 1, 2, 4
 OPS = dict(diff_lon=0, d1mu2=1, mu=2, mu2=3, laplace=4, helmholtz=5, scale=6, axpy=7)
 
 # every symbol declared in include/sph_gpu.h
@@ -24,7 +25,7 @@ EXPORTS = (
     "sph_spec_copy_modes",
     "sph_swe_tendency", "sph_swe_rk4", "sph_swe_rk4_batched", "sph_swe_rk4_launches",
     "sph_ensemble_create", "sph_ensemble_step", "sph_ensemble_launches", "sph_ensemble_destroy",
-    "sph_autotune", "sph_tune_load", "sph_tune_clear",
+    "sph_autotune", "sph_autotune_ex", "sph_tune_load", "sph_tune_clear",
     "sph_spat_op", "sph_rexi_coefficients", "sph_rexi_create", "sph_rexi_destroy", "sph_rexi_step", "sph_sync", "sph_wait_selftest",
     "sph_last_error",
 )
@@ -82,6 +83,7 @@ def lib():
                                           ctypes.POINTER(dp), ctypes.POINTER(vp)]
         L.sph_swe_rk4_launches.argtypes = [vp]
         L.sph_autotune.argtypes = [vp, i, ctypes.c_char_p, i, vp]
+        L.sph_autotune_ex.argtypes = [vp, i, i, ctypes.c_char_p, i, vp]
         L.sph_tune_load.argtypes = [vp, ctypes.c_char_p]
         L.sph_tune_clear.argtypes = [vp]
         L.sph_ensemble_step.argtypes = [vp, i, vp]

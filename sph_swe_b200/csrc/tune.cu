@@ -20,8 +20,10 @@
 // column tile nor the m order changes any arithmetic, the two P sources of the
 // split-TF32 form differ in the last bits of P_l^m only.  Across families the
 // results differ by the families' rounding (int8 ~1e-8, split TF32 ~3e-7
-// relative); the tuner takes the fastest of all of them, each of which meets
-// the mixed form's relL2 <= 1e-6 per transform.
+// relative).  sph_autotune takes the int8 and FP64 families, which keep every
+// transform of velocity-derived fields within the mixed form's relL2 <= 1e-6;
+// sph_autotune_ex chooses the families (the split-TF32 family meets 1e-6 for
+// scalar fields only).
 #include "common.cuh"
 
 #include <cstdio>
@@ -74,7 +76,7 @@ static int time_us(cudaStream_t s, F&& fn, float* us) {
     return rc;
 }
 
-static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
+static int autotune(Handle* h, int batch, int families, std::string& json, cudaStream_t s) {
     const int L = h->L, mF = L + 1;
     const long long fou = (long long)mF * h->nlat;
     const size_t bspec = sizeof(double2) * (size_t)h->nlm * batch, bF = sizeof(double2) * (size_t)fou * batch,
@@ -99,9 +101,14 @@ static int autotune(Handle* h, int batch, std::string& json, cudaStream_t s) {
             // warps (128), in ascending or paired (+64) m order; split TF32 with
             // B staged by producer warps (32), both operands loaded by the TMA unit
             // (8), P regenerated (4)
-            for (int src : {0, 64, 128, 192, 32, 8, 4})
-                for (int c = 1; c <= 3; c++) cand.push_back(src | c);
-            cand.push_back(16);  // FP64 CUDA-core kernel
+            if (families & SPH_TUNE_INT8)
+                for (int src : {0, 64, 128, 192})
+                    for (int c = 1; c <= 3; c++) cand.push_back(src | c);
+            if (families & SPH_TUNE_TF32)
+                for (int src : {32, 8, 4})
+                    for (int c = 1; c <= 3; c++) cand.push_back(src | c);
+            if (families & SPH_TUNE_FP64) cand.push_back(16);  // FP64 CUDA-core kernel
+            if (cand.empty()) continue;
         } else {
             if (!fixed_ring(h->nphi)) continue;
             cand = {0, 1, 2};
@@ -187,14 +194,15 @@ using namespace sphgpu;
 
 extern "C" {
 
-int sph_autotune(sph_handle* hh, int batch, char* json, int cap, void* stream) {
+int sph_autotune_ex(sph_handle* hh, int batch, int families, char* json, int cap, void* stream) {
     Handle* h = reinterpret_cast<Handle*>(hh);
-    if (!h || batch <= 0 || batch > 65535 || (json && cap <= 0)) {
+    if (!h || batch <= 0 || batch > 65535 || (json && cap <= 0) || families <= 0 ||
+        (families & ~(SPH_TUNE_INT8 | SPH_TUNE_TF32 | SPH_TUNE_FP64))) {
         set_error("sph_autotune: bad arguments");
         return SPH_ERR_ARG;
     }
     std::string out;
-    if (int rc = autotune(h, batch, out, reinterpret_cast<cudaStream_t>(stream))) return rc;
+    if (int rc = autotune(h, batch, families, out, reinterpret_cast<cudaStream_t>(stream))) return rc;
     if (json) {
         if ((int)out.size() + 1 > cap) {
             set_error("sph_autotune: json buffer too small (" + std::to_string(out.size() + 1) + " bytes needed)");
@@ -203,6 +211,10 @@ int sph_autotune(sph_handle* hh, int batch, char* json, int cap, void* stream) {
         std::memcpy(json, out.c_str(), out.size() + 1);
     }
     return SPH_OK;
+}
+
+int sph_autotune(sph_handle* hh, int batch, char* json, int cap, void* stream) {
+    return sph_autotune_ex(hh, batch, SPH_TUNE_INT8 | SPH_TUNE_FP64, json, cap, stream);
 }
 
 int sph_tune_load(sph_handle* hh, const char* json) {

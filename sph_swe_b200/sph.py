@@ -148,13 +148,17 @@ class Sph:
         return out
 
     # ------------------------------------------------------------ autotuner
-    def autotune(self, batch: int) -> dict:
+    def autotune(self, batch: int, families: int | None = None) -> dict:
         """Time the kernel variants for `batch` fields per launch, keep the
-        fastest in the handle, return the table (see sph_autotune)."""
+        fastest in the handle, return the table (see sph_autotune; families: a
+        mask of capi.SPH_TUNE_*, default int8 and FP64)."""
         import json
 
         buf = ctypes.create_string_buffer(1 << 16)
-        capi.check(capi.lib().sph_autotune(self.h, batch, buf, len(buf), _stream()))
+        if families is None:
+            capi.check(capi.lib().sph_autotune(self.h, batch, buf, len(buf), _stream()))
+        else:
+            capi.check(capi.lib().sph_autotune_ex(self.h, batch, families, buf, len(buf), _stream()))
         return json.loads(buf.value.decode())
 
     def tune_load(self, table) -> None:

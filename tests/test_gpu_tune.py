@@ -30,7 +30,12 @@ def test_autotune_table_and_results(gpu, oracle_mod, L, prec):
     if prec == capi.SPH_PREC_MIXED:
         assert {"legendre_synthesis_tc", "legendre_analysis_tc"} <= names
         tc = [k for k in table["kernels"] if k["name"].endswith("_tc")]
-        assert all(len(k["candidates"]) == 22 for k in tc)
+        # the default families: int8 (4 kernels x 3 tiles) and the FP64 kernel
+        assert all(len(k["candidates"]) == 13 for k in tc)
+        full = s.autotune(nb, families=capi.SPH_TUNE_INT8 | capi.SPH_TUNE_TF32 | capi.SPH_TUNE_FP64)
+        tcf = [k for k in full["kernels"] if k["name"].endswith("_tc")]
+        assert all(len(k["candidates"]) == 22 for k in tcf)
+        s.tune_load(table)
     for k in table["kernels"]:
         assert k["us"] > 0 and k["us"] == min(c["us"] for c in k["candidates"])
     grid1 = s.SH_to_spat(spec)
