@@ -60,6 +60,8 @@ struct RexiPlan {
     // Coriolis case): planes of [ngroups][ncplx][32 lanes]
     double2* fphi = nullptr;    // 7 planes
     double2* fvel = nullptr;    // 4 planes
+    float2* fphi32 = nullptr;   // mixed form: the same factors in complex FP32, 7 planes
+    float2* fvel32 = nullptr;   // 4 planes
     signed char* pphi = nullptr;
     signed char* pvel = nullptr;
     long long plane = 0;
@@ -80,6 +82,21 @@ struct RexiPlan {
     double* state = nullptr;
     cudaStream_t stream = nullptr;
 };
+
+// factor every (pole, m-block, parity) system once into the stored FP32 planes (mixed form)
+__global__ void __launch_bounds__(64) k_rexi_factor_f(RexiDev d) {
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int nblk = 2 * d.L + 1;
+    if (warp >= nblk * d.ngroups) return;
+    const int g = warp % d.ngroups, kk = warp / d.ngroups;
+    const int m = (kk & 1) ? -((kk + 1) >> 1) : (kk >> 1);
+    const int pole = g * 32 + lane;
+    const bool valid = pole < d.npoles;
+    const double2 a = d.alpha[valid ? pole : 0];
+    const long long gl = (long long)g * d.ncplx * 32 + lane;
+    if (!rexi_factor_lane_f(d, m, a, gl) && valid) atomicOr(d.flag, 2);
+}
 
 // factor every (pole, m-block, parity) system once into the stored planes
 __global__ void __launch_bounds__(64) k_rexi_factor(RexiDev d) {
@@ -167,7 +184,7 @@ __device__ __forceinline__ void rx_warp_sum(double2 bt, double2 x, double2* dst,
     if (lane == 0) *dst = v;
 }
 
-template <int MAXN>
+template <int MAXN, bool MX>
 __global__ void __launch_bounds__(64) k_rexi_phi_st(RexiDev d, double2* __restrict__ PH) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -185,7 +202,7 @@ __global__ void __launch_bounds__(64) k_rexi_phi_st(RexiDev d, double2* __restri
     const double2 a = d.alpha[valid ? pole : 0];
     const double2 bt = valid ? d.beta[pole] : make_double2(0, 0);
     const double T = d.T, P = d.P, ir = d.ir;
-    const double2 a2 = c_mul(a, a), a3 = c_mul(a2, a);
+    const double2 a2 = c_mul(a, a), a3 = c_mul(a2, a), a4 = c_mul(a2, a2);
     const double2 ainv = c_div(make_double2(1, 0), a);
     // right-hand side weights of the 10 pole-independent vectors (as rexi_phi)
     double2 sw[10];
@@ -215,10 +232,16 @@ __global__ void __launch_bounds__(64) k_rexi_phi_st(RexiDev d, double2* __restri
         rx_warp_sum(bt, x, outp + i, lane);
     };
     const long long gl = (long long)g * nc * 32 + lane;
-    band_solve_stored<2, (MAXN + 1) / 2, 1>(Np, band_ref(d.fphi, d.pphi, d, gl, base, N, par), rhs, out);
+    if constexpr (MX) {
+        auto entry = [&](int k, int dd) -> double2 { return phi_entry(d, base, par, a, a2, ainv, a4, k, dd); };
+        band_solve_stored_mixed<2, (MAXN + 1) / 2, 1>(Np, band_ref_f(d.fphi32, d.pphi, d, gl, base, N, par), d.refine,
+                                                     entry, rhs, out);
+    } else {
+        band_solve_stored<2, (MAXN + 1) / 2, 1>(Np, band_ref(d.fphi, d.pphi, d, gl, base, N, par), rhs, out);
+    }
 }
 
-template <int MAXN>
+template <int MAXN, bool MX>
 __global__ void __launch_bounds__(64) k_rexi_vel_st(RexiDev d, const double2* __restrict__ PH) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -277,7 +300,14 @@ __global__ void __launch_bounds__(64) k_rexi_vel_st(RexiDev d, const double2* __
         rx_warp_sum(bt, x, outp + (size_t)(1 + r) * nc + i, lane);
     };
     const long long gl = (long long)g * nc * 32 + lane;
-    band_solve_stored<1, (MAXN + 1) / 2, 2>(Np, band_ref(d.fvel, d.pvel, d, gl, base, N, par), rhs2, out2);
+    if constexpr (MX) {
+        const double2 a2 = c_mul(a, a);
+        auto entry = [&](int k, int dd) -> double2 { return vel_entry(d, base, par, a2, k, dd); };
+        band_solve_stored_mixed<1, (MAXN + 1) / 2, 2>(Np, band_ref_f(d.fvel32, d.pvel, d, gl, base, N, par), d.refine,
+                                                     entry, rhs2, out2);
+    } else {
+        band_solve_stored<1, (MAXN + 1) / 2, 2>(Np, band_ref(d.fvel, d.pvel, d, gl, base, N, par), rhs2, out2);
+    }
 }
 
 // ------------------------------------------------------------ non-Robert form (SWERexiSPH)
@@ -541,8 +571,10 @@ static RexiDev rexi_dev(const RexiPlan* R) {
     d.ngroups = R->ngroups;
     d.ncplx = h->ncplx;
     d.coriolis = (R->p.coriolis && R->p.omega != 0.0) ? 1 : 0;
-    // mixed form: complex FP32 factorisation and solves, two FP64 refinement steps
-    d.refine = R->p.precision == SPH_PREC_MIXED ? 2 : 0;
+    // mixed form: complex FP32 factorisation and solves with FP64 refinement:
+    // one step after substitutions with stored FP32 factors, two after an FP32
+    // factorisation in the step
+    d.refine = R->p.precision == SPH_PREC_MIXED ? (R->fphi32 ? 1 : 2) : 0;
     d.r = R->p.radius;
     d.ir = 1.0 / R->p.radius;
     d.T = 2.0 * R->p.omega;
@@ -559,6 +591,8 @@ static RexiDev rexi_dev(const RexiPlan* R) {
     d.pphi = R->pphi;
     d.fvel = R->fvel;
     d.pvel = R->pvel;
+    d.fphi32 = R->fphi32;
+    d.fvel32 = R->fvel32;
     d.plane = R->plane;
     d.lanes = 32;
     return d;
@@ -705,20 +739,28 @@ static int rexi_step_launch(RexiPlan* R, double2* state, cudaStream_t s) {
     const RexiDev d = rexi_dev(R);
     const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
     const unsigned nb = (unsigned)((nthreads + 63) / 64);
-    if (d.fphi && R->PHr) {
-        // factors stored at plan creation: substitutions only, a Phi phase and
+    if ((d.fphi || d.fphi32) && R->PHr) {
+        // factors stored at plan creation (FP64, or FP32 with one FP64
+        // refinement step in the mixed form): substitutions only, a Phi phase and
         // a velocity phase of one warp per (pole group, m-block, parity)
         const unsigned nb2 = 2 * nb;
+#define RX_ST(MAXN, MX)                                          \
+    do {                                                         \
+        k_rexi_phi_st<MAXN, MX><<<nb2, 64, 0, s>>>(d, R->PHr);   \
+        k_rexi_vel_st<MAXN, MX><<<nb2, 64, 0, s>>>(d, R->PHr);   \
+    } while (0)
+        const bool mx = d.fphi32 != nullptr;
         if (L + 1 <= 64) {
-            k_rexi_phi_st<64><<<nb2, 64, 0, s>>>(d, R->PHr);
-            k_rexi_vel_st<64><<<nb2, 64, 0, s>>>(d, R->PHr);
+            if (mx) RX_ST(64, true);
+            else RX_ST(64, false);
         } else if (L + 1 <= 128) {
-            k_rexi_phi_st<128><<<nb2, 64, 0, s>>>(d, R->PHr);
-            k_rexi_vel_st<128><<<nb2, 64, 0, s>>>(d, R->PHr);
+            if (mx) RX_ST(128, true);
+            else RX_ST(128, false);
         } else {
-            k_rexi_phi_st<256><<<nb2, 64, 0, s>>>(d, R->PHr);
-            k_rexi_vel_st<256><<<nb2, 64, 0, s>>>(d, R->PHr);
+            if (mx) RX_ST(256, true);
+            else RX_ST(256, false);
         }
+#undef RX_ST
     } else if (d.fphi) {
         if (L + 1 <= 64) k_rexi_solve<64, false, true><<<nb, 64, 0, s>>>(d);
         else if (L + 1 <= 128) k_rexi_solve<128, false, true><<<nb, 64, 0, s>>>(d);
@@ -745,7 +787,7 @@ static void rexi_free(RexiPlan* R) {
     if (R->graph) cudaGraphDestroy(R->graph);
     void* bufs[] = {R->alpha, R->beta, R->Cphi, R->Cvel, R->coef, R->V,  R->part, R->X,  R->Xr, R->F,
                     R->flag,  R->fphi, R->fvel, R->pphi, R->pvel, R->PH, R->XY,   R->FXY, R->Xs, R->Fs, R->glp,
-                    R->PHr};
+                    R->PHr,   R->fphi32, R->fvel32};
     for (void* p : bufs)
         if (p) cudaFree(p);
     delete R;
@@ -887,6 +929,31 @@ int sph_rexi_create(sph_handle* hh, const double* alpha, const double* beta, int
             R->plane = plane;
             const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
             k_rexi_factor<<<(unsigned)((nthreads + 63) / 64), 64>>>(rexi_dev(R));
+            RX_TRY(cudaGetLastError());
+            int flag = 0;
+            RX_TRY(cudaMemcpy(&flag, R->flag, sizeof(int), cudaMemcpyDeviceToHost));
+            R->singular = (flag & 2) != 0;
+            RX_TRY(cudaMemset(R->flag, 0, sizeof(int)));
+        }
+    }
+    // mixed form, Robert form with Coriolis: the same once-per-plan factoring in
+    // complex FP32 (half the bytes); each step substitutes in FP32 and refines
+    // once with FP64 residuals
+    if (cor && p->precision == SPH_PREC_MIXED && p->robert && !p->factor_each_step &&
+        !(store_env && store_env[0] == '0')) {
+        const long long plane = (long long)R->ngroups * nc * 32;
+        const size_t bytes = (size_t)plane * (11 * sizeof(float2) + 2 + sizeof(double2));
+        size_t free_b = 0, total_b = 0;
+        RX_TRY(cudaMemGetInfo(&free_b, &total_b));
+        if (bytes <= free_b / 2) {
+            RX_TRY(cudaMalloc(&R->fphi32, sizeof(float2) * 7 * (size_t)plane));
+            RX_TRY(cudaMalloc(&R->fvel32, sizeof(float2) * 4 * (size_t)plane));
+            RX_TRY(cudaMalloc(&R->pphi, (size_t)plane));
+            RX_TRY(cudaMalloc(&R->pvel, (size_t)plane));
+            RX_TRY(cudaMalloc(&R->PHr, sizeof(double2) * (size_t)plane));
+            R->plane = plane;
+            const long long nthreads = (long long)(2 * L + 1) * R->ngroups * 32;
+            k_rexi_factor_f<<<(unsigned)((nthreads + 63) / 64), 64>>>(rexi_dev(R));
             RX_TRY(cudaGetLastError());
             int flag = 0;
             RX_TRY(cudaMemcpy(&flag, R->flag, sizeof(int), cudaMemcpyDeviceToHost));

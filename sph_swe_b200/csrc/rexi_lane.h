@@ -35,6 +35,9 @@ struct RexiDev {
     signed char* pphi;   // [plane] pivot offsets
     double2* fvel;       // [4 planes][plane]: 1/U_kk, U_k,k+1..k+2, multiplier
     signed char* pvel;   // [plane]
+    // the same factors in complex FP32 (mixed form), pivots in pphi / pvel
+    float2* fphi32;      // [7 planes][plane]
+    float2* fvel32;      // [4 planes][plane]
     long long plane;     // ngroups * ncplx * lanes
     int lanes;           // poles per group (32 on the device, 1 on the host)
 };
@@ -44,6 +47,13 @@ struct RexiDev {
 // g, lane `lane`: i0 = ((g * ncplx + base + (par ? (N + 1) / 2 : 0)) * lanes + lane.
 struct BandRef {
     double2* f;
+    signed char* pv;
+    long long plane, i0;
+    int lanes;
+};
+// the same for factors stored in complex FP32
+struct BandRefF {
+    float2* f;
     signed char* pv;
     long long plane, i0;
     int lanes;
@@ -483,6 +493,174 @@ __host__ __device__ bool band_solve_mixed(int Np, int refine, Entry entry, Rhs r
     return ok;
 }
 
+// The FP32 factorisation of band_solve_mixed alone, stored (complex FP32
+// planes: 1/U_kk, the U row's 2H off-diagonal entries, the H multipliers; the
+// pivot offset): the operations of band_solve_mixed in the same order.
+// Returns false on a zero pivot.
+template <int H, class Entry>
+__host__ __device__ bool band_factor_store_f(int Np, Entry entry, const BandRefF& st) {
+    constexpr int W = 2 * H + 1;
+    float2 win[H + 1][W];
+#pragma unroll
+    for (int i = 0; i <= H; i++)
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - i;
+            win[i][j] = (i < Np && d >= -H && d <= H && j < Np) ? to_f(entry(i, d)) : make_float2(0.f, 0.f);
+        }
+    bool ok = true;
+    for (int k = 0; k < Np; k++) {
+        int p = 0;
+        float best = f_abs1(win[0][0]);
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const float v = (k + i < Np) ? f_abs1(win[i][0]) : -1.f;
+            if (v > best) {
+                best = v;
+                p = i;
+            }
+        }
+        if (best == 0.f) ok = false;
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < W; j++) {
+                const float2 t0 = win[0][j], ti = win[i][j];
+                win[0][j] = sw ? ti : t0;
+                win[i][j] = sw ? t0 : ti;
+            }
+        }
+        const float2 rp = best == 0.f ? make_float2(0.f, 0.f) : f_div(make_float2(1.f, 0.f), win[0][0]);
+        const long long e = st.i0 + (long long)k * st.lanes;
+        st.pv[e] = (signed char)p;
+        st.f[e] = rp;
+#pragma unroll
+        for (int j = 1; j < W; j++) st.f[j * st.plane + e] = win[0][j];
+#pragma unroll
+        for (int i = 1; i <= H; i++) {
+            const float2 l = f_mul(win[i][0], rp);
+            st.f[(2 * H + i) * st.plane + e] = l;
+#pragma unroll
+            for (int j = 1; j < W; j++) win[i][j] = f_sub(win[i][j], f_mul(l, win[0][j]));
+        }
+#pragma unroll
+        for (int i = 0; i < H; i++) {
+#pragma unroll
+            for (int j = 0; j < W - 1; j++) win[i][j] = win[i + 1][j + 1];
+            win[i][W - 1] = make_float2(0.f, 0.f);
+        }
+        const int rn = k + 1 + H;
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const int d = j - H;
+            win[H][j] = (rn < Np && k + 1 + j < Np) ? to_f(entry(rn, d)) : make_float2(0.f, 0.f);
+        }
+    }
+    return ok;
+}
+
+// Mixed solve with stored FP32 factors: x = U^-1 L^-1 P b in FP32 from the
+// FP64 right-hand side, then `refine` steps of FP64 iterative refinement
+// (r = b - A x with A = entry(k, d) and b = rhs(k, r) in FP64, correction
+// solved with the FP32 factors, x += correction in FP64), as band_solve_mixed
+// with the factorisation read instead of recomputed.  The factors of several
+// rows are loaded together as in band_solve_stored.
+template <int H, int MAXR, int NR, class Entry, class Rhs, class Out>
+__host__ __device__ void band_solve_stored_mixed(int Np, const BandRefF& st, int refine, Entry entry, Rhs rhs,
+                                                 Out out) {
+    constexpr int W = 2 * H + 1;
+    constexpr int PF = 4;
+    double2 x[MAXR][NR];
+    auto lu_solve = [&](auto b, bool add) {
+        float2 y[MAXR][NR];
+        float2 wr[H + 1][NR];
+#pragma unroll
+        for (int i = 0; i <= H; i++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) wr[i][r] = i < Np ? to_f(b(i, r)) : make_float2(0.f, 0.f);
+        for (int k0 = 0; k0 < Np; k0 += PF) {
+            int pvs[PF];
+            float2 lm[PF][H];
+#pragma unroll
+            for (int u = 0; u < PF; u++) {
+                const int k = k0 + u < Np ? k0 + u : Np - 1;
+                const long long e = st.i0 + (long long)k * st.lanes;
+                pvs[u] = RX_LDG(&st.pv[e]);
+#pragma unroll
+                for (int i = 1; i <= H; i++) lm[u][i - 1] = RX_LDG(&st.f[(2 * H + i) * st.plane + e]);
+            }
+#pragma unroll
+            for (int u = 0; u < PF; u++) {
+                const int k = k0 + u;
+                if (k >= Np) break;
+                const int p = pvs[u];
+#pragma unroll
+                for (int i = 1; i <= H; i++) {
+                    const bool sw = (p == i);
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        const float2 t0 = wr[0][r], ti = wr[i][r];
+                        wr[0][r] = sw ? ti : t0;
+                        wr[i][r] = sw ? t0 : ti;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < NR; r++) y[k][r] = wr[0][r];
+#pragma unroll
+                for (int i = 1; i <= H; i++)
+#pragma unroll
+                    for (int r = 0; r < NR; r++) wr[i][r] = f_sub(wr[i][r], f_mul(lm[u][i - 1], wr[0][r]));
+#pragma unroll
+                for (int i = 0; i < H; i++)
+#pragma unroll
+                    for (int r = 0; r < NR; r++) wr[i][r] = wr[i + 1][r];
+                const int rn = k + 1 + H;
+#pragma unroll
+                for (int r = 0; r < NR; r++) wr[H][r] = rn < Np ? to_f(b(rn, r)) : make_float2(0.f, 0.f);
+            }
+        }
+        float2 xs[W][NR];
+#pragma unroll
+        for (int j = 0; j < W; j++)
+#pragma unroll
+            for (int r = 0; r < NR; r++) xs[j][r] = make_float2(0.f, 0.f);
+        for (int k = Np - 1; k >= 0; k--) {
+            const long long e = st.i0 + (long long)k * st.lanes;
+            const float2 rd = RX_LDG(&st.f[e]);
+            float2 uu[W];
+#pragma unroll
+            for (int j = 1; j < W; j++) uu[j] = RX_LDG(&st.f[j * st.plane + e]);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                float2 sm = y[k][r];
+#pragma unroll
+                for (int j = 1; j < W; j++) sm = f_sub(sm, f_mul(uu[j], xs[j - 1][r]));
+                const float2 xk = f_mul(sm, rd);
+#pragma unroll
+                for (int j = W - 1; j > 0; j--) xs[j][r] = xs[j - 1][r];
+                xs[0][r] = xk;
+                x[k][r] = add ? c_add(x[k][r], to_d(xk)) : to_d(xk);
+            }
+        }
+    };
+    lu_solve([&](int k, int r) { return rhs(k, r); }, false);
+    for (int it = 0; it < refine; it++) {
+        lu_solve(
+            [&](int k, int r) {
+                double2 v = rhs(k, r);
+#pragma unroll
+                for (int d = -H; d <= H; d++)
+                    if (k + d >= 0 && k + d < Np) v = c_sub(v, c_mul(entry(k, d), x[k + d][r]));
+                return v;
+            },
+            true);
+    }
+    for (int k = 0; k < Np; k++)
+#pragma unroll
+        for (int r = 0; r < NR; r++) out(k, r, x[k][r]);
+}
+
 // Entry (k, dd) of the parity-`par` Phi system of the m-block at block row
 // base: alpha^4 I + alpha^2 C2 + alpha C1 + alpha^-1 Cm1 + C0 (rows par + 2k).
 __host__ __device__ inline double2 phi_entry(const RexiDev& d, int base, int par, double2 a, double2 a2, double2 ainv,
@@ -508,6 +686,10 @@ __host__ __device__ inline BandRef band_ref(double2* f, signed char* pv, const R
                                             int N, int par) {
     return BandRef{f, pv, d.plane, gl + (long long)(base + (par ? (N + 1) / 2 : 0)) * d.lanes, d.lanes};
 }
+__host__ __device__ inline BandRefF band_ref_f(float2* f, signed char* pv, const RexiDev& d, long long gl, int base,
+                                               int N, int par) {
+    return BandRefF{f, pv, d.plane, gl + (long long)(base + (par ? (N + 1) / 2 : 0)) * d.lanes, d.lanes};
+}
 
 // Factor the Phi and velocity systems of one pole and one m-block (both
 // parities) into the stored planes of d; gl = g * ncplx * lanes + lane.
@@ -528,6 +710,28 @@ __host__ __device__ inline bool rexi_factor_lane(const RexiDev& d, int m, double
         ok = band_factor_store<1>(
                  Np, [&](int k, int dd) { return vel_entry(d, base, par, a2, k, dd); },
                  band_ref(d.fvel, d.pvel, d, gl, base, N, par)) && ok;
+    }
+    return ok;
+}
+
+// The FP32 factors of the Phi and velocity systems of one pole and one m-block
+// (both parities), for the mixed form's stored-factor solves.
+__host__ __device__ inline bool rexi_factor_lane_f(const RexiDev& d, int m, double2 a, long long gl) {
+    const int am = m < 0 ? -m : m;
+    const int N = d.L + 1 - am;
+    const int base = block_off(d.L, m);
+    const double2 a2 = c_mul(a, a), a4 = c_mul(a2, a2);
+    const double2 ainv = c_div(make_double2(1, 0), a);
+    bool ok = true;
+    for (int par = 0; par < 2; par++) {
+        const int Np = (N - par + 1) >> 1;
+        if (Np <= 0) continue;
+        ok = band_factor_store_f<2>(
+                 Np, [&](int k, int dd) { return phi_entry(d, base, par, a, a2, ainv, a4, k, dd); },
+                 band_ref_f(d.fphi32, d.pphi, d, gl, base, N, par)) && ok;
+        ok = band_factor_store_f<1>(
+                 Np, [&](int k, int dd) { return vel_entry(d, base, par, a2, k, dd); },
+                 band_ref_f(d.fvel32, d.pvel, d, gl, base, N, par)) && ok;
     }
     return ok;
 }
