@@ -95,18 +95,6 @@ __device__ __forceinline__ void mma_s8(uint32_t tmem_d, uint64_t a, uint64_t b, 
         "l"(a), "l"(b), "r"(idesc), "r"(accum));
 }
 
-// shared -> global bulk copy (the async proxy's store), grouped per issuing thread
-__device__ __forceinline__ void bulk_store(void* gdst, uint32_t ssrc, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(reinterpret_cast<uint64_t>(gdst)),
-                 "r"(ssrc), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// the bulk stores issued by this thread have finished reading shared memory
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// ... and are complete
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
 // balanced base-256 digit word of v = rint(t s1 s2), s1 s2 = 2^(31 - e) split in
 // two powers of two so that neither overflows (|v| < 2^31): t s1 is exact, and
 // adding 1.5 2^52 in the same FMA rounds t s1 s2 to the nearest integer (half
@@ -306,34 +294,6 @@ struct SynI8 {
             out[a.nlat - 1 - j] = make_double2(er - orr, ei - oi);
         }
     }
-    // the same values into the tile's shared-memory image stg[field][256]:
-    // north rows at r, south rows at 255 - r (ascending global addresses)
-    __device__ static void stage(const I8Args& a, const I8Tile& p, int r, int c0, const int* er, const int* ec8,
-                                 const double* e, const double* o, double2* stg) {
-        const int ea = er[0];
-        const int fl = c0 / 2;
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const double sr = i8_pow2(ea + ec8[2 * u]), si = i8_pow2(ea + ec8[2 * u + 1]);
-            const double ev = e[2 * u] * sr, ei = e[2 * u + 1] * si, ov = o[2 * u] * sr, oi = o[2 * u + 1] * si;
-            double2* row = stg + (fl + u) * 256;
-            row[r] = make_double2(ev + ov, ei + oi);
-            row[255 - r] = make_double2(ev - ov, ei - oi);
-        }
-    }
-    // one thread: bulk stores of the staged tile, per field one northern and
-    // one southern run of the valid rows
-    __device__ static void flush(const I8Args& a, const I8Tile& p, uint32_t stg, double2* __restrict__ F) {
-        const int j0 = p.rt * li8::M, rv = min(li8::M, a.nh - j0);
-        if (rv <= 0) return;
-        for (int fl = 0; fl < NF; fl++) {
-            const int f = p.ct * NF + fl;
-            if (f >= a.batch) break;
-            double2* out = F + (long long)f * a.ldF + (long long)p.m * a.nlat;
-            bulk_store(out + j0, stg + (uint32_t)(fl * 256) * 16u, (uint32_t)rv * 16u);
-            bulk_store(out + (a.nlat - j0 - rv), stg + (uint32_t)(fl * 256 + 256 - rv) * 16u, (uint32_t)rv * 16u);
-        }
-    }
 };
 
 // ------------------------------------------------------------------ analysis
@@ -437,32 +397,6 @@ struct AnaI8 {
             if (odd)
                 out[pidx(a.lmax, le + 1, p.m)] =
                     make_double2(o[2 * u] * i8_pow2(eao + cr), o[2 * u + 1] * i8_pow2(eao + ci));
-        }
-    }
-    // the same values into stg[field][256]: degree m + 256 rt + 2 r + parity at 2 r + parity
-    __device__ static void stage(const I8Args& a, const I8Tile& p, int r, int c0, const int* er, const int* ec8,
-                                 const double* e, const double* o, double2* stg) {
-        const int eae = er[0], eao = er[1];
-        const int fl = c0 / 2;
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int cr = ec8[2 * u], ci = ec8[2 * u + 1];
-            double2* row = stg + (fl + u) * 256;
-            row[2 * r] = make_double2(e[2 * u] * i8_pow2(eae + cr), e[2 * u + 1] * i8_pow2(eae + ci));
-            row[2 * r + 1] = make_double2(o[2 * u] * i8_pow2(eao + cr), o[2 * u + 1] * i8_pow2(eao + ci));
-        }
-    }
-    // one thread: per field one bulk store of the tile's degrees
-    // m + 256 rt .. min(lmax, m + 256 rt + 255), contiguous in the packed layout
-    __device__ static void flush(const I8Args& a, const I8Tile& p, uint32_t stg, double2* __restrict__ spec) {
-        const int l0 = p.m + 2 * li8::M * p.rt;
-        const int cnt = min(2 * li8::M, a.lmax - l0 + 1);
-        if (cnt <= 0) return;
-        for (int fl = 0; fl < NF; fl++) {
-            const int f = p.ct * NF + fl;
-            if (f >= a.batch) break;
-            bulk_store(spec + (long long)f * a.ld_spec + pidx(a.lmax, l0, p.m), stg + (uint32_t)(fl * 256) * 16u,
-                       (uint32_t)cnt * 16u);
         }
     }
 };

@@ -29,23 +29,15 @@ __host__ __device__ constexpr int i8b_chunk(int nc) { return 2 * li8::ND * 2 * n
 namespace li8b {
 constexpr int A_STAGE = li8::A_STAGE;  // 32 KB: both parities' A of a chunk
 constexpr int SMEM_MAX = 227 * 1024;
-// Up to 32 columns a tile's FP64 results are staged in shared memory (16
-// fields x 256 entries of 16 B at 32 columns) and written by bulk copies, so
-// that the accumulator is released as soon as it has been read; the ring
-// holds as many operand stages (A + B of one chunk) as the rest allows: 5 at
-// 16 columns, 4 at 32 and 64.
-template <int NC>
-constexpr bool staged() { return NC <= 32; }
-template <int NC>
-constexpr int stg_bytes() { return staged<NC>() ? (NC / 2) * 256 * 16 : 0; }
+// A load takes ~2 us to land under full load, so the ring holds as many
+// stages (A + B of one chunk) as the shared memory allows: 6, 5 or 4 at 16,
+// 32 or 64 columns
 template <int NC>
 constexpr int stage() { return A_STAGE + i8b_chunk(NC); }
 template <int NC>
-constexpr int nstage() { return (SMEM_MAX - 256 - stg_bytes<NC>()) / stage<NC>(); }
+constexpr int nstage() { return (SMEM_MAX - 256) / stage<NC>(); }
 template <int NC>
-constexpr int off_stg() { return nstage<NC>() * stage<NC>(); }
-template <int NC>
-constexpr int off_bar() { return off_stg<NC>() + stg_bytes<NC>(); }
+constexpr int off_bar() { return nstage<NC>() * stage<NC>(); }
 template <int NC>
 constexpr int bytes() { return off_bar<NC>() + 256; }
 constexpr int MAXSTAGE = 8;
@@ -54,7 +46,7 @@ constexpr int CONS_WARP0 = 2;
 constexpr int NT = 64 + NCONS;
 constexpr int PREP_NT = 256;
 static_assert(stage<16>() % 1024 == 0 && stage<32>() % 1024 == 0 && stage<64>() % 1024 == 0, "stage alignment");
-static_assert(nstage<16>() <= MAXSTAGE && nstage<32>() >= 4 && nstage<64>() >= 4, "stage count");
+static_assert(nstage<16>() <= MAXSTAGE && nstage<64>() >= 4, "stage count");
 }  // namespace li8b
 
 // ------------------------------------------------------------------ B preparation
@@ -112,18 +104,14 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
     constexpr int PART = NC >= 32 ? NC / 4 : NC / 2;  // columns per consumer warp (multiples of 8)
     constexpr int NPART = NC / PART;
     constexpr int NSTAGE = li8b::nstage<NC>(), STAGE = li8b::stage<NC>();
-    constexpr bool STG = li8b::staged<NC>();
     static_assert(NC % 16 == 0 && NC <= 64, "tile shape");
     extern __shared__ __align__(1024) unsigned char smem[];
-    double2* stg = reinterpret_cast<double2*>(smem + li8b::off_stg<NC>());  // staged tile (STG)
     unsigned long long* full = reinterpret_cast<unsigned long long*>(smem + li8b::off_bar<NC>());
     unsigned long long* empty = full + NSTAGE;
     unsigned long long* accfull = empty + NSTAGE;  // [NACC]
-    unsigned long long* accempty = accfull + 2;    // [NACC]
-    unsigned long long* stgfull = accempty + 2;    // staged tile written (consumers -> storer)
-    unsigned long long* stgfree = stgfull + 1;     // staged tile read by its bulk stores (storer -> consumers)
-    volatile int* abort = reinterpret_cast<volatile int*>(stgfree + 1);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(stgfree + 1) + 1;
+    unsigned long long* accempty = accfull + 2;           // [NACC]
+    volatile int* abort = reinterpret_cast<volatile int*>(accempty + 2);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(accempty + 2) + 1;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     const I8Tile first = i8_tile<Dir>(a, blockIdx.x);
@@ -139,8 +127,6 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
             mbar_init(smem_u32(&accfull[i]), 1);
             mbar_init(smem_u32(&accempty[i]), li8b::NCONS);
         }
-        mbar_init(smem_u32(stgfull), li8b::NCONS);
-        mbar_init(smem_u32(stgfree), 1);
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map)) : "memory");
@@ -177,19 +163,6 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
                     loaded = q + 1;
                 }
             }
-        } else if (STG && lane == 1) {
-            // ---------------------------------------------------------------- stores
-            // each staged tile goes out by bulk copies; the staging buffer is
-            // released once the copies have read it
-            int j = 0;
-            for (I8Tile p = first; p.t < a.ntiles; p = i8_tile<Dir>(a, p.t + gridDim.x), j++) {
-                if (!mbar_wait_abort(smem_u32(stgfull), (uint32_t)(j & 1), abort)) break;
-                Dir::flush(a, p, smem_u32(stg), out);
-                bulk_commit();
-                bulk_wait_read();
-                mbar_arrive(smem_u32(stgfree));
-            }
-            bulk_wait_all();
         }
         __syncwarp();
     } else if (warp == 1) {
@@ -246,9 +219,7 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
             const int* ecol = a.ecol + ((long long)p.ct * a.nm + p.m) * NC + (active ? half : 0) * PART;
 #pragma unroll
             for (int c = 0; c < PART; c++) ec[c] = __ldg(ecol + c);
-            bool v = mbar_wait_abort(smem_u32(&accfull[b]), (uint32_t)((j / NACC) & 1), abort);
-            // the previous staged tile has been read by its bulk stores
-            if (STG && j > 0) v = v && mbar_wait_abort(smem_u32(stgfree), (uint32_t)((j - 1) & 1), abort);
+            const bool v = mbar_wait_abort(smem_u32(&accfull[b]), (uint32_t)((j / NACC) & 1), abort);
             if (!__all_sync(0xffffffffu, v)) break;
             tc_fence_after();
             const uint32_t base = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * TCOLS);
@@ -259,16 +230,11 @@ __global__ void __launch_bounds__(li8b::NT, 1) k_legendre_i8b(const __grid_const
                     double e[8], o[8];
                     i8_ld_combine<NC>(base + (uint32_t)c0, e);
                     i8_ld_combine<NC>(base + (uint32_t)(li8::NG * NC + c0), o);
-                    if constexpr (STG) Dir::stage(a, p, r, c0, er, ec + cb, e, o, stg);
-                    else Dir::epilogue(a, p, r, c0, er, ec + cb, e, o, out);
+                    Dir::epilogue(a, p, r, c0, er, ec + cb, e, o, out);
                 }
             }
             tc_fence_before();
             mbar_arrive(smem_u32(&accempty[b]));
-            if constexpr (STG) {
-                fence_async_smem();  // the staged values, to the bulk copies' proxy
-                mbar_arrive(smem_u32(stgfull));
-            }
         }
     }
     tc_fence_before();
