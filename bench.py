@@ -247,6 +247,69 @@ def _time(fn, steps, st):
     return e0.elapsed_time(e1) / steps
 
 
+def _e2e_pipelined(sph, h_spec, h_vort, h_div, o_spec, o_vort, o_div, steps, dev):
+    """Milliseconds per step of config 1 end to end with host buffers, the
+    copies of neighbouring steps overlapping the compute (see the caller)."""
+    import torch
+
+    s_in, s_cmp, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    sets = []
+    for _ in range(2):
+        b = {"spec": torch.empty(h_spec.shape, dtype=h_spec.dtype, device=dev),
+             "vort": torch.empty(h_vort.shape, dtype=h_vort.dtype, device=dev),
+             "div": torch.empty(h_div.shape, dtype=h_div.dtype, device=dev)}
+        b["grid"] = torch.empty(N_SCALAR, sph.nphi, sph.nlat, dtype=torch.float64, device=dev)
+        b["spec_out"] = torch.empty_like(b["spec"])
+        b["u"] = torch.empty(N_PAIRS, sph.nphi, sph.nlat, dtype=torch.float64, device=dev)
+        b["v"] = torch.empty_like(b["u"])
+        b["z"] = torch.empty_like(b["vort"])
+        b["d"] = torch.empty_like(b["div"])
+        sets.append(b)
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_cmp = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
+
+    def run(n):
+        for k in range(n):
+            i = k % 2
+            b = sets[i]
+            with torch.cuda.stream(s_in):
+                if k >= 2:
+                    s_in.wait_event(ev_cmp[i])  # step k - 2 has consumed this set's inputs
+                b["spec"].copy_(h_spec, non_blocking=True)
+                b["vort"].copy_(h_vort, non_blocking=True)
+                b["div"].copy_(h_div, non_blocking=True)
+                ev_in[i].record(s_in)
+            with torch.cuda.stream(s_cmp):
+                s_cmp.wait_event(ev_in[i])
+                if k >= 2:
+                    s_cmp.wait_event(ev_out[i])  # step k - 2's results have left this set
+                sph.SH_to_spat(b["spec"], out=b["grid"])
+                sph.spat_to_SH(b["grid"], out=b["spec_out"])
+                sph.vec_SH_to_spat(b["vort"], b["div"], out=(b["u"], b["v"]))
+                sph.vec_spat_to_SH(b["u"], b["v"], out=(b["z"], b["d"]))
+                ev_cmp[i].record(s_cmp)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_cmp[i])
+                o_spec.copy_(b["spec_out"], non_blocking=True)
+                o_vort.copy_(b["z"], non_blocking=True)
+                o_div.copy_(b["d"], non_blocking=True)
+                ev_out[i].record(s_out)
+
+    run(3)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s_in)
+    run(steps)
+    s_out.wait_stream(s_in)
+    s_out.wait_stream(s_cmp)
+    e1.record(s_out)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    del sets
+    return ms
+
+
 def _max_over_ranks(ms, world, dev):
     """the slowest rank's time (NCCL on the device, or gloo on the host)"""
     import torch
@@ -395,7 +458,14 @@ def run_ours(args, rank, world):
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
-    ms_e2e = _max_over_ranks(_time(e2e_step, args.steps, st), world, dev)
+    ms_e2e_serial = _max_over_ranks(_time(e2e_step, args.steps, st), world, dev)
+
+    # the same steps pipelined: three streams (upload, compute, download) and two
+    # device buffer sets, so that the upload of step k + 1 and the download of
+    # step k - 1 overlap the compute of step k; every step still copies its own
+    # inputs from pinned host memory and its results back
+    ms_e2e = _max_over_ranks(_e2e_pipelined(mx.s, h_spec, h_vort, h_div, o_spec, o_vort, o_div, args.steps, dev),
+                             world, dev)
     e2e_value = flops_step * world / (ms_e2e * 1e-3) / 1e9
     for c in forms.values():
         c.s.close()
@@ -411,7 +481,8 @@ def run_ours(args, rank, world):
         extra["T1023"] = t1023_rates(dev, args)
     return dict(value=value, ms=ms["mixed"], roofline=roofline, clocks=clocks,
                 e2e={"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                     "ms_per_step": ms_e2e},
+                     "ms_per_step": ms_e2e, "pipelined": "upload / compute / download streams, two buffer sets",
+                     "ms_per_step_serial": ms_e2e_serial},
                 launches=Cfg1.LAUNCHES * args.steps, accuracy=accuracy, extra=extra)
 
 
@@ -705,7 +776,8 @@ def profile_case(which="all"):
     family (no timing): transforms of 64 scalar fields at T255 in both forms,
     one nonlinear RK4 step at T255 (advective and vorticity-divergence forms),
     one REXI step at T127 (M = 64) and one spectral operator pass.  which:
-    "all", or one workload alone: "mixed64" (two inverse + forward transforms
+    "all", or one workload alone: "cfg1" (two steps of the transform
+    configuration in each form, built-in kernel variants), "mixed64" (two inverse + forward transforms
     of the 64 scalar T255 fields in the mixed form), "rexi" (two REXI steps at
     T127, M = 64, FP64 with stored factors, Robert form), "rexi_s0" (the same
     in the non-Robert form)."""
@@ -717,6 +789,20 @@ def profile_case(which="all"):
     from sph_swe_b200.sph import Sph, rexi_coefficients
 
     dev = torch.device("cuda", 0)
+    if which == "cfg1":
+        # two steps of the transform-throughput configuration in each form, with
+        # the built-in kernel variants (the launch-list case)
+        spec, vort, div = _cfg1_inputs(dev, 0)
+        for prec in (capi.SPH_PREC_FP64, capi.SPH_PREC_MIXED):
+            s = Sph(L_CFG1, precision=prec)
+            grid = torch.empty(N_SCALAR, s.nphi, s.nlat, dtype=torch.float64, device=dev)
+            for _ in range(2):
+                s.spat_to_SH(s.SH_to_spat(spec, out=grid))
+                s.vec_spat_to_SH(*s.vec_SH_to_spat(vort, div))
+            capi.check(capi.lib().sph_sync(s.h, None))
+            s.close()
+        print(json.dumps({"profile_case": which}))
+        return
     if which == "mixed64":
         s = Sph(L_CFG1, precision=capi.SPH_PREC_MIXED)
         spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1)).to(dev)
@@ -837,7 +923,7 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel (default: the committed capture)")
     ap.add_argument("--profile-case", nargs="?", const="all", default=None,
-                    help="run one small instance of each workload (for ncu); optionally one of mixed64, rexi, rexi_s0")
+                    help="run one small instance of each workload (for ncu); optionally one of cfg1, mixed64, rexi, rexi_s0")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

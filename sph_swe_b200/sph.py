@@ -99,18 +99,24 @@ class Sph:
         capi.check(capi.lib().sph_cplx_SH_to_spat(self.h, _ptr(spec), _ptr(out), batch, 0, 0, _stream()))
         return out
 
-    def vec_SH_to_spat(self, vort: torch.Tensor, div: torch.Tensor, robert: bool = False):
+    def vec_SH_to_spat(self, vort: torch.Tensor, div: torch.Tensor, robert: bool = False, out=None):
         batch = vort.numel() // self.nlm
-        u = torch.empty(vort.shape[:-1] + (self.nphi, self.nlat), dtype=torch.float64, device=vort.device)
-        v = torch.empty_like(u)
+        if out is None:
+            u = torch.empty(vort.shape[:-1] + (self.nphi, self.nlat), dtype=torch.float64, device=vort.device)
+            v = torch.empty_like(u)
+        else:
+            u, v = out
         capi.check(capi.lib().sph_vec_SH_to_spat(self.h, _ptr(vort), _ptr(div), _ptr(u), _ptr(v), batch, int(robert),
                                                  _stream()))
         return u, v
 
-    def vec_spat_to_SH(self, u: torch.Tensor, v: torch.Tensor, robert: bool = False):
+    def vec_spat_to_SH(self, u: torch.Tensor, v: torch.Tensor, robert: bool = False, out=None):
         batch = u.numel() // (self.nlat * self.nphi)
-        vort = torch.empty(u.shape[:-2] + (self.nlm,), dtype=torch.complex128, device=u.device)
-        div = torch.empty_like(vort)
+        if out is None:
+            vort = torch.empty(u.shape[:-2] + (self.nlm,), dtype=torch.complex128, device=u.device)
+            div = torch.empty_like(vort)
+        else:
+            vort, div = out
         capi.check(capi.lib().sph_vec_spat_to_SH(self.h, _ptr(u), _ptr(v), _ptr(vort), _ptr(div), batch, int(robert),
                                                  _stream()))
         return vort, div
