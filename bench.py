@@ -19,6 +19,13 @@ same step, the per-field relative L2 of the mixed form against the FP64 path,
 nonlinear RK4 steps/s at T255 and T63 (plain-method configuration) in both
 forms, and REXI steps/s at T127 (M = 256, 535 poles, FP64 direct solves).
 
+End to end (`e2e`): the same step through the public transform calls with
+the input spectra in pinned host memory and the output spectra copied back to
+pinned host memory every step (67 MB each way).  The reported figure runs the
+steps pipelined (upload, compute and download streams; two device buffer
+sets, so step k + 1's upload and step k - 1's download overlap step k's
+transforms); `ms_per_step_serial` is the same steps one after another.
+
 --impl reference times the CPU restatement of the same algorithm (the oracle;
 the reference's SHTNS/FFTW/LAPACK build is unavailable on this machine) on the
 host cores, on a bounded sample of the same workload.
