@@ -558,7 +558,7 @@ def rexi_rates(dev, args):
     """REXI configuration: T127 192x384, Robert linear SWE about h0 = 1e4 m,
     Gaussian-approximation REXI h = 0.2, M = 256 (535 poles), tau = 3600 s,
     24 steps from the Gaussian bump; FP64 direct and the mixed form (complex
-    FP32 factorisation and solves, two FP64 refinement steps), with the
+    FP32 factors stored per plan, one FP64 refinement step), with the
     relative L2 of the mixed state against the FP64 state."""
     import torch
 
@@ -784,7 +784,8 @@ def profile_case(which="all"):
     one nonlinear RK4 step at T255 (advective and vorticity-divergence forms),
     one REXI step at T127 (M = 64) and one spectral operator pass.  which:
     "all", or one workload alone: "cfg1" (two steps of the transform
-    configuration in each form, built-in kernel variants), "mixed64" (two inverse + forward transforms
+    configuration in each form, built-in kernel variants), "rk4" (two
+    nonlinear RK4 steps at T255 in each form, tuned variants), "mixed64" (two inverse + forward transforms
     of the 64 scalar T255 fields in the mixed form), "rexi" (two REXI steps at
     T127, M = 64, FP64 with stored factors, Robert form), "rexi_s0" (the same
     in the non-Robert form)."""
@@ -806,6 +807,23 @@ def profile_case(which="all"):
             for _ in range(2):
                 s.spat_to_SH(s.SH_to_spat(spec, out=grid))
                 s.vec_spat_to_SH(*s.vec_SH_to_spat(vort, div))
+            capi.check(capi.lib().sph_sync(s.h, None))
+            s.close()
+        print(json.dumps({"profile_case": which}))
+        return
+    if which == "rk4":
+        # two nonlinear RK4 steps at T255 (reference advective form, dt 10 s,
+        # viscosity 1e5) in each form, kernel variants tuned per batch
+        s0 = Sph(255)
+        st0 = _bump_state(s0, dev)
+        s0.close()
+        for prec in (capi.SPH_PREC_FP64, capi.SPH_PREC_MIXED):
+            s = Sph(255, precision=prec)
+            for nb in Sph.rk4_batches(1, 1):
+                s.autotune(nb)
+            p = Sph.swe_params(radius=6.371e6, dt=10.0, viscosity=1e5, nonlinear=1)
+            st = st0.clone()
+            s.swe_rk4(p, st, 2)
             capi.check(capi.lib().sph_sync(s.h, None))
             s.close()
         print(json.dumps({"profile_case": which}))
@@ -930,7 +948,7 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel (default: the committed capture)")
     ap.add_argument("--profile-case", nargs="?", const="all", default=None,
-                    help="run one small instance of each workload (for ncu); optionally one of cfg1, mixed64, rexi, rexi_s0")
+                    help="run one small instance of each workload (for ncu); optionally one of cfg1, rk4, mixed64, rexi, rexi_s0")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

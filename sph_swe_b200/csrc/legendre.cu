@@ -403,6 +403,232 @@ __global__ void __launch_bounds__(WNT) k_legendre_analysis_w(const double* __res
     }
 }
 
+// Small-batch variants (batch <= NB <= 8).  With one to a few fields the
+// tiled kernels above fill 1/16 .. 1/2 of their column tile and walk the
+// degrees in short chunks, each a global-load round trip and two barriers
+// long: bound by latency (54-70 us per launch at T255 for 1-8 fields, where
+// the 50 MB table streams in ~8 us).  Here the table is streamed with 8 to
+// 16 independent loads per thread in flight (the next 8 rows' loads go out
+// before the current 8 rows' sums) and the fields' values come from shared
+// memory, staged for the whole degree (latitude) range of the m at once where
+// it fits in 48 KB:
+//   synthesis: a CTA takes 32 latitudes of one m; warp q sums the degrees
+//     l = |m| + q (mod 8), so that a thread's terms all have the parity of q;
+//     the eight classes meet in shared memory, E = even q, O = odd q.
+//   analysis: a CTA takes 32 degrees of one m, 8 lanes per degree, each lane
+//     a strided eighth of the latitudes, against the weighted north + south
+//     (even degrees) and north - south (odd) values of the fields; the 8
+//     lanes of a degree are summed by shuffles at the end.
+// Shared arrays are field-major with the degree / latitude innermost, so
+// that the lanes of a warp read consecutive 16-byte words.
+namespace {
+constexpr int SNT = 256;              // threads
+constexpr int SJ = 32;                // latitudes per CTA (synthesis)
+constexpr int SQ = SNT / SJ;          // degree classes (synthesis)
+constexpr int AL = 32;                // degrees per CTA (analysis)
+constexpr int ALANES = 8;             // lanes per degree (analysis)
+constexpr int NB_SMEM = 48 * 1024;    // shared-memory budget of both kernels
+constexpr int NBATCH = 4;             // staging loads in flight per thread
+#ifndef SPH_NB_MAX
+#define SPH_NB_MAX 8
+#endif
+constexpr int NB_MAX = SPH_NB_MAX;    // largest batch given to the small-batch kernels
+// degrees (synthesis) or latitudes (analysis) staged per chunk: the whole
+// range where it fits, else the largest multiple of 64 that does
+inline int nb_chunk(int n, int bytes_per) {
+    const int cap = (NB_SMEM / bytes_per) / 64 * 64;
+    const int want = (n + 63) / 64 * 64;
+    return want < cap ? want : cap;
+}
+}  // namespace
+
+template <int NB>
+__global__ void __launch_bounds__(SNT) k_legendre_synthesis_nb(const double* __restrict__ plm,
+                                                               const long long* __restrict__ poff, int nh, int nlat,
+                                                               const double2* __restrict__ spec, SpecMap sm,
+                                                               double2* __restrict__ F, long long ldF, int batch,
+                                                               int cq) {
+    extern __shared__ double2 sh[];  // Q[NB][cq] during the sums, then R[SQ][NB][SJ]
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int tid = threadIdx.x;
+    const int jl = tid % SJ, q = tid / SJ;
+    const int j = blockIdx.x * SJ + jl;
+    const bool jv = j < nh;
+    const double* P = plm + poff[am] + (jv ? j : 0);
+    double2 acc[NB];
+#pragma unroll
+    for (int f = 0; f < NB; f++) acc[f] = make_double2(0, 0);
+    for (int lc = am; lc <= lmax; lc += cq) {
+        const int nk = min(cq, lmax + 1 - lc);
+        // stage the chunk's spectra, NBATCH loads in flight per thread
+        for (int base = tid; base < cq * NB; base += NBATCH * SNT) {
+            double2 v[NBATCH];
+#pragma unroll
+            for (int u = 0; u < NBATCH; u++) {
+                const int idx = base + u * SNT;
+                const int f = idx / cq, kk = idx - f * cq;
+                v[u] = (idx < cq * NB && kk < nk && f < batch) ? spec[(long long)f * sm.ld + spec_index(sm, lc + kk, m)]
+                                                               : make_double2(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < NBATCH; u++) {
+                const int idx = base + u * SNT;
+                if (idx < cq * NB) sh[idx] = make_double2(v[u].x * sg, v[u].y * sg);
+            }
+        }
+        __syncthreads();
+        // degrees kk = q + 8 i of the chunk; the table loads of the next 8 are
+        // issued before the sums of the current 8
+        const int ni = nk > q ? (nk - q + SQ - 1) / SQ : 0;
+        auto ldp = [&](int i) -> double {
+            return (jv && i < ni) ? __ldg(P + (long long)(lc + q + SQ * i - am) * nh) : 0.0;
+        };
+        double pc[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) pc[u] = ldp(u);
+        for (int i0 = 0; i0 < ni; i0 += 8) {
+            double pn[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) pn[u] = ldp(i0 + 8 + u);
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int i = i0 + u;
+                if (i >= ni) break;
+                const int kk = q + SQ * i;
+#pragma unroll
+                for (int f = 0; f < NB; f++) {
+                    const double2 c = sh[f * cq + kk];
+                    acc[f].x = fma(pc[u], c.x, acc[f].x);
+                    acc[f].y = fma(pc[u], c.y, acc[f].y);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) pc[u] = pn[u];
+        }
+        __syncthreads();
+    }
+    double2* R = sh;  // [SQ][NB][SJ]
+#pragma unroll
+    for (int f = 0; f < NB; f++) R[(q * NB + f) * SJ + jl] = acc[f];
+    __syncthreads();
+    double2* out = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+    for (int idx = tid; idx < SJ * NB; idx += SNT) {
+        const int jj = idx % SJ, f = idx / SJ;
+        const int jo = blockIdx.x * SJ + jj;
+        if (jo >= nh || f >= batch) continue;
+        double er = 0, ei = 0, orr = 0, oi = 0;
+#pragma unroll
+        for (int c = 0; c < SQ; c += 2) {
+            const double2 e = R[(c * NB + f) * SJ + jj], o = R[((c + 1) * NB + f) * SJ + jj];
+            er += e.x;
+            ei += e.y;
+            orr += o.x;
+            oi += o.y;
+        }
+        double2* o = out + (long long)f * ldF;
+        o[jo] = make_double2(er + orr, ei + oi);
+        o[nlat - 1 - jo] = make_double2(er - orr, ei - oi);
+    }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(SNT) k_legendre_analysis_nb(const double* __restrict__ plm,
+                                                              const long long* __restrict__ poff, int nh, int nlat,
+                                                              const double* __restrict__ w,
+                                                              const double2* __restrict__ F, long long ldF,
+                                                              double2* __restrict__ spec, SpecMap sm, int batch,
+                                                              int cj) {
+    extern __shared__ double2 sh[];  // G[2][NB][cj]: weighted north + south, north - south
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int lbase = am + blockIdx.x * AL;
+    if (lbase > lmax) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane / ALANES, t = lane % ALANES;
+    const int l = lbase + warp * (32 / ALANES) + g;
+    const bool lv = l <= lmax;
+    const int par = (l - am) & 1;
+    const double* Pl = plm + poff[am] + (long long)((lv ? l : am) - am) * nh;
+    const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+    double2 acc[NB];
+#pragma unroll
+    for (int f = 0; f < NB; f++) acc[f] = make_double2(0, 0);
+    for (int jc = 0; jc < nh; jc += cj) {
+        const int nj = min(cj, nh - jc);
+        // stage the chunk's weighted sums and differences, NBATCH entries in flight per thread
+        for (int base = tid; base < cj * NB; base += NBATCH * SNT) {
+            double2 n[NBATCH], so[NBATCH];
+            double wj[NBATCH];
+#pragma unroll
+            for (int u = 0; u < NBATCH; u++) {
+                const int idx = base + u * SNT;
+                const int f = idx / cj, jj = idx - f * cj;
+                const bool v = idx < cj * NB && jj < nj && f < batch;
+                const double2* Ff = Fm + (long long)(v ? f : 0) * ldF;
+                const int j = jc + (v ? jj : 0);
+                n[u] = v ? Ff[j] : make_double2(0, 0);
+                so[u] = v ? Ff[nlat - 1 - j] : make_double2(0, 0);
+                wj[u] = v ? w[j] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < NBATCH; u++) {
+                const int idx = base + u * SNT;
+                if (idx >= cj * NB) break;
+                sh[idx] = make_double2(wj[u] * (n[u].x + so[u].x), wj[u] * (n[u].y + so[u].y));
+                sh[NB * cj + idx] = make_double2(wj[u] * (n[u].x - so[u].x), wj[u] * (n[u].y - so[u].y));
+            }
+        }
+        __syncthreads();
+        // latitudes jj = t + 8 i of the chunk; the table loads of the next 8
+        // are issued before the sums of the current 8
+        const double2* G = sh + par * NB * cj;
+        const int ni = nj > t ? (nj - t + ALANES - 1) / ALANES : 0;
+        auto ldp = [&](int i) -> double { return (lv && i < ni) ? __ldg(Pl + jc + t + ALANES * i) : 0.0; };
+        double pc[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) pc[u] = ldp(u);
+        for (int i0 = 0; i0 < ni; i0 += 8) {
+            double pn[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) pn[u] = ldp(i0 + 8 + u);
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int i = i0 + u;
+                if (i >= ni) break;
+                const int jj = t + ALANES * i;
+#pragma unroll
+                for (int f = 0; f < NB; f++) {
+                    const double2 c = G[f * cj + jj];
+                    acc[f].x = fma(pc[u], c.x, acc[f].x);
+                    acc[f].y = fma(pc[u], c.y, acc[f].y);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) pc[u] = pn[u];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int f = 0; f < NB; f++) {
+#pragma unroll
+        for (int o = ALANES / 2; o > 0; o >>= 1) {
+            acc[f].x += __shfl_xor_sync(0xffffffffu, acc[f].x, o);
+            acc[f].y += __shfl_xor_sync(0xffffffffu, acc[f].y, o);
+        }
+    }
+    if (!lv) return;
+    // lane t of the degree writes field t
+#pragma unroll
+    for (int f = 0; f < NB; f++)
+        if (f == t && f < batch)
+            spec[(long long)f * sm.ld + spec_index(sm, l, m)] = make_double2(acc[f].x * sg, acc[f].y * sg);
+}
+
 // zero the m = L+1 column of a degree-(L+1) packed spectrum (no wavenumber L+1 exists)
 __global__ void k_zero_top(double2* spec, long long ld, int lmax, int batch) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -505,6 +731,21 @@ static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double
         SPH_CUDA_TRY(cudaGetLastError());
         return SPH_OK;
     }
+    if (batch <= NB_MAX) {
+        const dim3 grid((h->nh + SJ - 1) / SJ, 1, nm);
+        const int nb = batch == 1 ? 1 : batch == 2 ? 2 : batch <= 4 ? 4 : 8;
+        const int cq = nb_chunk(sm.lmax + 1, nb * (int)sizeof(double2));
+        const size_t smem = (size_t)std::max(cq, SQ * SJ) * nb * sizeof(double2);
+#define SYN_NB(NB) \
+    k_legendre_synthesis_nb<NB><<<grid, SNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch, cq)
+        if (nb == 1) SYN_NB(1);
+        else if (nb == 2) SYN_NB(2);
+        else if (nb == 4) SYN_NB(4);
+        else SYN_NB(8);
+#undef SYN_NB
+        SPH_CUDA_TRY(cudaGetLastError());
+        return SPH_OK;
+    }
     dim3 grid((h->nh + TJ - 1) / TJ, (batch + TC / 2 - 1) / (TC / 2), nm);
     k_legendre_synthesis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
     SPH_CUDA_TRY(cudaGetLastError());
@@ -528,6 +769,19 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
         dim3 grid((sm.lmax + 1 + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
         k_legendre_analysis_w<<<grid, WNT, WSMEM_ANA, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm,
                                                         batch);
+    } else if (batch <= NB_MAX) {
+        const dim3 grid((sm.lmax + 1 + AL - 1) / AL, 1, nm);
+        const int nb = batch == 1 ? 1 : batch == 2 ? 2 : batch <= 4 ? 4 : 8;
+        const int cj = nb_chunk(h->nh, 2 * nb * (int)sizeof(double2));
+        const size_t smem = (size_t)2 * nb * cj * sizeof(double2);
+#define ANA_NB(NB)                                                                                                   \
+    k_legendre_analysis_nb<NB><<<grid, SNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch, \
+                                                       cj)
+        if (nb == 1) ANA_NB(1);
+        else if (nb == 2) ANA_NB(2);
+        else if (nb == 4) ANA_NB(4);
+        else ANA_NB(8);
+#undef ANA_NB
     } else {
         dim3 grid((sm.lmax + 1 + TLT - 1) / TLT, (batch + TC / 2 - 1) / (TC / 2), nm);
         k_legendre_analysis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch);
@@ -553,6 +807,14 @@ int legendre_kernels_init() {
     // the wide analysis needs its shared-memory opt-in on this device before any
     // launch, also before launches inside a stream capture
     SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_w, cudaFuncAttributeMaxDynamicSharedMemorySize, WSMEM_ANA));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<1>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<2>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<4>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<8>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<1>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<2>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<4>));
+    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<8>));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_zero_top));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_m01));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_m01));

@@ -165,6 +165,14 @@ __global__ void __launch_bounds__(64) k_rexi_solve(RexiDev d) {
 // row's right-hand sides from a window phi[i-2 .. i+2] of both parities read
 // back from PH, solves, and sums beta u, beta v.  The arithmetic of every row
 // is that of rexi_phi / rexi_lane.
+// resident 64-thread blocks per SM asked of the compiler for the substitution
+// kernels, which caps their registers: FP64 8 (at most 128 registers), mixed
+// 16 (64 registers, some spills).  T127, M = 256, 535 poles: the mixed step
+// took 1.58 ms with the compiler's own choice (166 / 96 registers), 1.34 ms
+// at 16; the FP64 step is the same at 8 to 16.
+template <bool MX>
+constexpr int rx_minb() { return MX ? 16 : 8; }
+
 __device__ __forceinline__ void rx_warp_index(const RexiDev& d, int warp, int& g, int& m, int& par) {
     par = warp & 1;
     const int w2 = warp >> 1;
@@ -185,7 +193,7 @@ __device__ __forceinline__ void rx_warp_sum(double2 bt, double2 x, double2* dst,
 }
 
 template <int MAXN, bool MX>
-__global__ void __launch_bounds__(64) k_rexi_phi_st(RexiDev d, double2* __restrict__ PH) {
+__global__ void __launch_bounds__(64, rx_minb<MX>()) k_rexi_phi_st(RexiDev d, double2* __restrict__ PH) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     const int L = d.L;
@@ -242,7 +250,7 @@ __global__ void __launch_bounds__(64) k_rexi_phi_st(RexiDev d, double2* __restri
 }
 
 template <int MAXN, bool MX>
-__global__ void __launch_bounds__(64) k_rexi_vel_st(RexiDev d, const double2* __restrict__ PH) {
+__global__ void __launch_bounds__(64, rx_minb<MX>()) k_rexi_vel_st(RexiDev d, const double2* __restrict__ PH) {
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     const int L = d.L;
