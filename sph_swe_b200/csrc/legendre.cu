@@ -629,6 +629,280 @@ __global__ void __launch_bounds__(SNT) k_legendre_analysis_nb(const double* __re
             spec[(long long)f * sm.ld + spec_index(sm, l, m)] = make_double2(acc[f].x * sg, acc[f].y * sg);
 }
 
+// FP64 tensor-core variants (mma.sync m8n8k4 f64, the FP64 MMA of sm_100;
+// tcgen05 has no FP64 kind).  One instruction is an 8 x 8 x 4 product, 256
+// FMAs from one table value and one field value per lane, where the FMA
+// kernels above need a shared-memory load per one or two FMAs.  Per m the
+// columns (field, re/im) are cut in blocks of CN = 8 RN (4 RN fields); a
+// warp owns 16 rows of one l - m parity and all CN columns (2 x RN
+// accumulator fragments of 2 doubles per lane).
+//   analysis: A = P (8 degrees x 4 latitudes, straight from the table, rows
+//     two degrees apart), B = the weighted north + south (even degrees) or
+//     north - south (odd) values of the column block, staged column-major in
+//     shared memory; a CTA of 8 warps takes 128 degrees (4 warps per parity).
+//   synthesis: A = P^T (8 latitudes x 4 degrees of one parity), B = the
+//     spectra of the column block staged per parity column-major; a CTA of 8
+//     warps takes 64 latitudes, even warps summing the even degrees and odd
+//     warps the odd ones, which meet in shared memory for north E + O, south E - O.
+// Shared rows are padded to 4 (mod 16) doubles, so that the 32 lanes of a B
+// fragment load (8 columns x 4 consecutive entries) take two wavefronts.
+// Fragment layout of m8n8k4 f64 (lane = 4 g + t): A row g col t, B row t col
+// g, C row g cols 2 t, 2 t + 1.
+namespace {
+constexpr int MNT = 256;                  // threads (8 warps)
+#ifndef SPH_MSMEM
+#define SPH_MSMEM 100352
+#endif
+constexpr int MSMEM = SPH_MSMEM;          // dynamic shared-memory budget per CTA (2 CTAs per SM)
+constexpr int MSTAGE = 8;                 // staging loads in flight per thread (synthesis)
+constexpr int MSTAGE_A = 4;               // staging entries in flight per thread (analysis: 3 loads each)
+constexpr int MCHUNK = 192;               // most entries staged per column and parity
+// entries staged per column and parity: the whole range where it fits (up to
+// MCHUNK), else the largest multiple of 16 that does; the row stride is that + 4
+inline int mma_chunk(int n, int cn) {
+    const int cap = std::min(MCHUNK, ((MSMEM / (2 * cn * (int)sizeof(double)) - 4) / 16) * 16);
+    const int want = (n + 15) / 16 * 16;
+    return want < cap ? want : cap;
+}
+}  // namespace
+
+#ifdef SPH_MMA_MINB
+#define MMA_LB __launch_bounds__(MNT, SPH_MMA_MINB)
+#else
+#define MMA_LB __launch_bounds__(MNT)
+#endif
+
+__device__ __forceinline__ void dmma8844(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int RN>
+__global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
+                                                               const long long* __restrict__ poff, int nh, int nlat,
+                                                               const double* __restrict__ w,
+                                                               const double2* __restrict__ F, long long ldF,
+                                                               double2* __restrict__ spec, SpecMap sm, int batch,
+                                                               int cj) {
+    constexpr int CN = 8 * RN, NFB = CN / 2;
+    extern __shared__ double msh[];  // G[parity][CN][cj + 4]
+    const int S = cj + 4;
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int lbase = am + blockIdx.x * (MNT / 2);
+    if (lbase > lmax) return;
+    const int f0 = blockIdx.y * NFB;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int p = warp & 1, hw = warp >> 1;
+    const bool busy = lbase + p + 2 * 16 * hw <= lmax;  // some row of this warp is a degree
+    // A rows of this lane: degrees lbase + p + 2 (16 hw + 8 rm + g); rows past
+    // lmax read row |m| (their sums are not stored)
+    const double* prow[2];
+#pragma unroll
+    for (int rm = 0; rm < 2; rm++) {
+        const int l = lbase + p + 2 * (16 * hw + 8 * rm + g);
+        prow[rm] = plm + poff[am] + (long long)((l <= lmax ? l : am) - am) * nh + t;
+    }
+    const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+    double acc[2][RN][2];
+#pragma unroll
+    for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+        for (int nb = 0; nb < RN; nb++) acc[rm][nb][0] = acc[rm][nb][1] = 0.0;
+
+    for (int jc = 0; jc < nh; jc += cj) {
+        const int nj = min(cj, nh - jc);
+        // stage the column block's weighted sums / differences, latitude-minor:
+        // segment `row` = (field, 32 latitudes), warp w takes rows w, w + 8, ...
+        const int nseg = (cj + 31) / 32;
+#pragma unroll 4
+        for (int row = warp; row < NFB * nseg; row += MNT / 32) {
+            const int fl = row / nseg, jj = (row - fl * nseg) * 32 + lane;
+            if (jj >= cj) continue;
+            const bool v = f0 + fl < batch && jj < nj;
+            const double2* Ff = Fm + (long long)(v ? f0 + fl : 0) * ldF;
+            const int j = jc + (v ? jj : 0);
+            const double2 n = v ? Ff[j] : make_double2(0, 0);
+            const double2 so = v ? Ff[nlat - 1 - j] : make_double2(0, 0);
+            const double wj = v ? w[j] : 0.0;
+            double* s0 = msh + (2 * fl) * S + jj;          // parity 0, column re
+            double* s1 = msh + (CN + 2 * fl) * S + jj;     // parity 1, column re
+            s0[0] = wj * (n.x + so.x);
+            s0[S] = wj * (n.y + so.y);
+            s1[0] = wj * (n.x - so.x);
+            s1[S] = wj * (n.y - so.y);
+        }
+        __syncthreads();
+        const double* G = msh + (p * CN + g) * S + t;  // column 8 nb + g, latitude j0 + t
+        // latitudes past nh - 1 read latitude nh - 1 (their staged values are zero)
+        const int jlast = nh - 1 - jc - t;
+        double a[4][2];
+        auto lda = [&](int j0) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int j = min(j0 + 4 * k, jlast);
+#pragma unroll
+                for (int rm = 0; rm < 2; rm++) a[k][rm] = __ldg(prow[rm] + jc + j);
+            }
+        };
+        if (busy) lda(0);
+        for (int j0 = 0; busy && j0 < nj; j0 += 16) {
+            double an[4][2];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+#pragma unroll
+                for (int rm = 0; rm < 2; rm++) an[k][rm] = a[k][rm];
+            if (j0 + 16 < nj) lda(j0 + 16);  // next step's table values, ahead of this step's MMAs
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                double b[RN];
+#pragma unroll
+                for (int nb = 0; nb < RN; nb++) b[nb] = G[nb * 8 * S + j0 + 4 * k];
+#pragma unroll
+                for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+                    for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], an[k][rm], b[nb]);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int rm = 0; rm < 2; rm++) {
+        const int l = lbase + p + 2 * (16 * hw + 8 * rm + g);
+        if (l > lmax) continue;
+#pragma unroll
+        for (int nb = 0; nb < RN; nb++) {
+            const int f = f0 + 4 * nb + t;
+            if (f < batch)
+                spec[(long long)f * sm.ld + spec_index(sm, l, m)] =
+                    make_double2(acc[rm][nb][0] * sg, acc[rm][nb][1] * sg);
+        }
+    }
+}
+
+template <int RN>
+__global__ void MMA_LB k_legendre_synthesis_mma(const double* __restrict__ plm,
+                                                                const long long* __restrict__ poff, int nh, int nlat,
+                                                                const double2* __restrict__ spec, SpecMap sm,
+                                                                double2* __restrict__ F, long long ldF, int batch,
+                                                                int kc) {
+    constexpr int CN = 8 * RN, NFB = CN / 2;
+    extern __shared__ double msh[];  // Q[parity][CN][kc + 4] (entry i: degree |m| + parity + 2 (i0 + i))
+    const int S = kc + 4;
+    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
+    const int am = m < 0 ? -m : m;
+    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+    const int lmax = sm.lmax;
+    const int jbase = blockIdx.x * (MNT / 4);
+    const int f0 = blockIdx.y * NFB;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int p = warp & 1, hw = warp >> 1;
+    const bool busy = jbase + 16 * hw < nh;  // some row of this warp is a latitude
+    // A rows of this lane: latitudes jbase + 16 hw + 8 rm + g; rows past nh - 1
+    // read latitude nh - 1 (their sums are not stored)
+    const int j0r = jbase + 16 * hw + g;
+    const double* P = plm + poff[am] + min(j0r, nh - 1);
+    const int d1 = min(j0r + 8, nh - 1) - min(j0r, nh - 1);  // second row, relative
+    const int npair = (lmax + 2 - am) / 2;  // degree pairs (even + odd) from |m|
+    const int last = lmax - am;             // last table row of this m
+    double acc[2][RN][2];
+#pragma unroll
+    for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+        for (int nb = 0; nb < RN; nb++) acc[rm][nb][0] = acc[rm][nb][1] = 0.0;
+
+    for (int ic = 0; ic < npair; ic += kc) {
+        const int ni = min(kc, npair - ic);
+        // stage the spectra of the chunk, both parities, column-major: entry r =
+        // 2 i + parity is degree l0 + r
+        const int l0 = am + 2 * ic;
+        const long long b0 = sm.cplx ? 0 : (long long)pidx(lmax, l0, m);  // packed index of l0 (real)
+        for (int r = tid; r < 2 * kc; r += MNT) {
+            const int l = l0 + r;
+            const bool vr = (r >> 1) < ni && l <= lmax;
+            const long long si = sm.cplx ? (long long)cidx(vr ? l : am, m) : b0 + (vr ? r : 0);
+            double* q = msh + ((r & 1) * CN) * S + (r >> 1);
+#pragma unroll 8
+            for (int fl = 0; fl < NFB; fl++) {
+                const bool v = vr && f0 + fl < batch;
+                const double2 x = v ? spec[(long long)(f0 + fl) * sm.ld + si] : make_double2(0, 0);
+                q[(2 * fl) * S] = x.x * sg;
+                q[(2 * fl + 1) * S] = x.y * sg;
+            }
+        }
+        __syncthreads();
+        const double* Q = msh + (p * CN + g) * S + t;  // column 8 nb + g, entry i0 + t
+        // table row of entry i: p + 2 (ic + i); rows past lmax read row lmax - |m|
+        // (their staged spectra are zero)
+        const int r0 = p + 2 * (ic + t);
+        double a[4][2];
+        auto lda = [&](int i0) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int r = min(r0 + 2 * (i0 + 4 * k), last);
+                const double* q = P + (long long)r * nh;
+                a[k][0] = __ldg(q);
+                a[k][1] = __ldg(q + d1);
+            }
+        };
+        if (busy) lda(0);
+        for (int i0 = 0; busy && i0 < ni; i0 += 16) {
+            double an[4][2];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                an[k][0] = a[k][0];
+                an[k][1] = a[k][1];
+            }
+            if (i0 + 16 < ni) lda(i0 + 16);  // next step's table values, ahead of this step's MMAs
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                double b[RN];
+#pragma unroll
+                for (int nb = 0; nb < RN; nb++) b[nb] = Q[nb * 8 * S + i0 + 4 * k];
+#pragma unroll
+                for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+                    for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], an[k][rm], b[nb]);
+            }
+        }
+        __syncthreads();
+    }
+    // odd sums to shared memory; the even warps combine and store
+    double* X = msh + (size_t)hw * (2 * RN * 2 * 32);
+    if (p == 1) {
+#pragma unroll
+        for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+            for (int nb = 0; nb < RN; nb++) {
+                X[((rm * RN + nb) * 2 + 0) * 32 + lane] = acc[rm][nb][0];
+                X[((rm * RN + nb) * 2 + 1) * 32 + lane] = acc[rm][nb][1];
+            }
+    }
+    __syncthreads();
+    if (p == 1) return;
+    double2* outm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
+#pragma unroll
+    for (int rm = 0; rm < 2; rm++) {
+        const int j = j0r + 8 * rm;
+        if (j >= nh) continue;
+#pragma unroll
+        for (int nb = 0; nb < RN; nb++) {
+            const int f = f0 + 4 * nb + t;
+            if (f >= batch) continue;
+            const double er = acc[rm][nb][0], ei = acc[rm][nb][1];
+            const double orr = X[((rm * RN + nb) * 2 + 0) * 32 + lane], oi = X[((rm * RN + nb) * 2 + 1) * 32 + lane];
+            double2* out = outm + (long long)f * ldF;
+            out[j] = make_double2(er + orr, ei + oi);
+            out[nlat - 1 - j] = make_double2(er - orr, ei - oi);
+        }
+    }
+}
+
 // zero the m = L+1 column of a degree-(L+1) packed spectrum (no wavenumber L+1 exists)
 __global__ void k_zero_top(double2* spec, long long ld, int lmax, int batch) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -721,10 +995,32 @@ __global__ void __launch_bounds__(128) k_legendre_analysis_m01(const double* __r
     if (lane == 0) spec[(long long)f * ld_spec + pidx(lmax, l, m)] = acc;
 }
 
+#ifndef SPH_LEG_MMA
+#define SPH_LEG_MMA 1
+#endif
+
+// column-block width of the tensor-core kernels for a batch: 4, 8 or 16 fields
+static int mma_rn(int batch) { return batch <= 4 ? 1 : batch <= 8 ? 2 : 4; }
+
 static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double2* F, long long ldF, int batch,
                         cudaStream_t s) {
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
+    if (SPH_LEG_MMA) {
+        const int rn = mma_rn(batch), cn = 8 * rn;
+        const int kc = mma_chunk((sm.lmax + 2) / 2, cn);
+        // staged spectra, then the odd sums of the 4 warp pairs
+        const size_t smem = (size_t)std::max(2 * cn * (kc + 4), 4 * 2 * rn * 2 * 32) * sizeof(double);
+        const dim3 grid((h->nh + MNT / 4 - 1) / (MNT / 4), (2 * batch + cn - 1) / cn, nm);
+#define SYN_MMA(RN) \
+    k_legendre_synthesis_mma<RN><<<grid, MNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch, kc)
+        if (rn == 1) SYN_MMA(1);
+        else if (rn == 2) SYN_MMA(2);
+        else SYN_MMA(4);
+#undef SYN_MMA
+        SPH_CUDA_TRY(cudaGetLastError());
+        return SPH_OK;
+    }
     if (batch > 16) {
         dim3 grid((h->nh + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
         k_legendre_synthesis_w<<<grid, WNT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
@@ -757,7 +1053,19 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
     if (!wts) wts = h->w;
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
-    if (batch > 16) {
+    if (SPH_LEG_MMA) {
+        const int rn = mma_rn(batch), cn = 8 * rn;
+        const int cj = mma_chunk(h->nh, cn);
+        const size_t smem = (size_t)2 * cn * (cj + 4) * sizeof(double);
+        const dim3 grid((sm.lmax + 1 + MNT / 2 - 1) / (MNT / 2), (2 * batch + cn - 1) / cn, nm);
+#define ANA_MMA(RN)                                                                                                  \
+    k_legendre_analysis_mma<RN><<<grid, MNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch, \
+                                                        cj)
+        if (rn == 1) ANA_MMA(1);
+        else if (rn == 2) ANA_MMA(2);
+        else ANA_MMA(4);
+#undef ANA_MMA
+    } else if (batch > 16) {
         // the shared-memory opt-in is a per-device attribute: once per device
         static std::atomic<unsigned long long> attr_done{0};
         const unsigned long long bit = h->device >= 0 && h->device < 64 ? 1ull << h->device : 0ull;
@@ -815,6 +1123,13 @@ int legendre_kernels_init() {
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<2>));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<4>));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<8>));
+    // the tensor-core kernels take up to MSMEM of dynamic shared memory
+    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_synthesis_mma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
+    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_synthesis_mma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
+    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_synthesis_mma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
+    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_mma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
+    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_mma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
+    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_mma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_zero_top));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_m01));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_m01));
