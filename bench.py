@@ -426,6 +426,18 @@ def run_ours(args, rank, world):
         leg[name] = {"synthesis_us": t_syn * 1e6, "analysis_us": t_ana * 1e6,
                      "synthesis_tflops": per_contr * N_SCALAR / t_syn / 1e12,
                      "analysis_tflops": per_contr * N_SCALAR / t_ana / 1e12}
+        # the small batches of the RK4 stages (first fields of the same spectra;
+        # built-in kernel variants): synthesis / analysis us
+        small = {}
+        for nb in (1, 4, 8, 16):
+            sp, fo, so = spec[:nb], four[:nb], c.spec_out[:nb]
+            c.s.legendre_synthesis(sp, fo)
+            c.s.legendre_analysis(fo, so)
+            t1 = _time(lambda: c.s.legendre_synthesis(sp, fo), nrep, st) * 1e3
+            t2 = _time(lambda: c.s.legendre_analysis(fo, so), nrep, st) * 1e3
+            small[str(nb)] = [_sig(t1), _sig(t2)]
+        c.sync_ok()
+        leg[name]["small_batches_us_syn_ana"] = small
         del four
     # the dominant stage, the int8 Legendre analysis (B preparation + contraction
     # of 64 fields): its tensor work is a few microseconds at int8 rate, so it is
@@ -785,7 +797,9 @@ def profile_case(which="all"):
     one REXI step at T127 (M = 64) and one spectral operator pass.  which:
     "all", or one workload alone: "cfg1" (two steps of the transform
     configuration in each form, built-in kernel variants), "rk4" (two
-    nonlinear RK4 steps at T255 in each form, tuned variants), "mixed64" (two inverse + forward transforms
+    nonlinear RK4 steps at T255 in each form, tuned variants), "fp64x64" (two
+    inverse + forward transforms of the 64 scalar T255 fields in the FP64
+    form), "mixed64" (two inverse + forward transforms
     of the 64 scalar T255 fields in the mixed form), "rexi" (two REXI steps at
     T127, M = 64, FP64 with stored factors, Robert form), "rexi_s0" (the same
     in the non-Robert form)."""
@@ -828,8 +842,8 @@ def profile_case(which="all"):
             s.close()
         print(json.dumps({"profile_case": which}))
         return
-    if which == "mixed64":
-        s = Sph(L_CFG1, precision=capi.SPH_PREC_MIXED)
+    if which in ("mixed64", "fp64x64"):
+        s = Sph(L_CFG1, precision=capi.SPH_PREC_MIXED if which == "mixed64" else capi.SPH_PREC_FP64)
         spec = torch.from_numpy(random_spec(L_CFG1, N_SCALAR, 1)).to(dev)
         for _ in range(2):
             s.spat_to_SH(s.SH_to_spat(spec))
@@ -948,7 +962,7 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel (default: the committed capture)")
     ap.add_argument("--profile-case", nargs="?", const="all", default=None,
-                    help="run one small instance of each workload (for ncu); optionally one of cfg1, rk4, mixed64, rexi, rexi_s0")
+                    help="run one small instance of each workload (for ncu); optionally one of cfg1, rk4, fp64x64, mixed64, rexi, rexi_s0")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

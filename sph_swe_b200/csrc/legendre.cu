@@ -1,7 +1,7 @@
 // Legendre stage of the spherical-harmonic transforms in FP64 (the plain
 // method): per zonal wavenumber m a dense contraction between the table
 // P_l^m(mu_j) (northern rings only, equatorial symmetry) and the batch of
-// fields, tiled as a small GEMM on the FP64 pipe.
+// fields, run on the FP64 tensor cores.
 //
 //   synthesis  E_j = sum_{l-m even} Q_l P_l(mu_j),  O_j = sum_{l-m odd} Q_l P_l(mu_j)
 //              F(mu_j) = E_j + O_j,  F(-mu_j) = E_j - O_j
@@ -13,17 +13,7 @@
 // Columns of the GEMM are (field, re/im) pairs.
 #include "common.cuh"
 
-#include <atomic>
-
 namespace sphgpu {
-
-namespace {
-constexpr int TJ = 64;   // latitudes per CTA tile (synthesis)
-constexpr int TLT = 64;  // degrees per CTA tile (analysis)
-constexpr int TC = 32;   // real columns per tile (16 complex fields)
-constexpr int TK = 16;   // contraction chunk
-constexpr int NT = 256;  // threads
-}  // namespace
 
 struct SpecMap {
     int cplx;      // 0 real packed(lmax), 1 complex n*n+n+m
@@ -36,603 +26,13 @@ __device__ __forceinline__ long long spec_index(const SpecMap& s, int l, int m) 
     return s.cplx ? (long long)cidx(l, m) : (long long)pidx(s.lmax, l, m);
 }
 
-// grid: x = j tile, y = column tile, z = m slot (real: m, complex: m + L)
-__global__ void __launch_bounds__(NT) k_legendre_synthesis(const double* __restrict__ plm, const long long* __restrict__ poff,
-                                                           int nh, int nlat, const double2* __restrict__ spec, SpecMap sm,
-                                                           double2* __restrict__ F, long long ldF, int batch) {
-    __shared__ double As[TK][TJ];
-    __shared__ double Bs[TK][TC + 1];
-    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
-    const int am = m < 0 ? -m : m;
-    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
-    const int lmax = sm.lmax;
-    const int j0 = blockIdx.x * TJ;
-    const int f0 = blockIdx.y * (TC / 2);
-    const int tid = threadIdx.x;
-    const int tx = tid & 15;   // field within tile
-    const int ty = tid >> 4;   // 4 latitudes: ty*4 .. ty*4+3
-    const double* P = plm + poff[am];
-
-    double eR[4] = {0, 0, 0, 0}, eI[4] = {0, 0, 0, 0}, oR[4] = {0, 0, 0, 0}, oI[4] = {0, 0, 0, 0};
-
-    for (int l0 = am; l0 <= lmax; l0 += TK) {
-        // A tile: P rows l0..l0+TK-1, latitudes j0..j0+TJ-1
-        for (int idx = tid; idx < TK * TJ; idx += NT) {
-            const int kk = idx / TJ, jj = idx - kk * TJ;
-            const int l = l0 + kk, j = j0 + jj;
-            As[kk][jj] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
-        }
-        // B tile: coefficients of 16 fields, degrees l0..l0+TK-1
-        {
-            const int kk = tid & 15, ff = tid >> 4;
-            const int l = l0 + kk, f = f0 + ff;
-            double2 q = make_double2(0, 0);
-            if (l <= lmax && f < batch) q = spec[(long long)f * sm.ld + spec_index(sm, l, m)];
-            Bs[kk][2 * ff] = q.x;
-            Bs[kk][2 * ff + 1] = q.y;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < TK; kk += 2) {
-            const double br0 = Bs[kk][2 * tx], bi0 = Bs[kk][2 * tx + 1];
-            const double br1 = Bs[kk + 1][2 * tx], bi1 = Bs[kk + 1][2 * tx + 1];
-#pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const double a0 = As[kk][ty * 4 + r], a1 = As[kk + 1][ty * 4 + r];
-                eR[r] = fma(a0, br0, eR[r]);
-                eI[r] = fma(a0, bi0, eI[r]);
-                oR[r] = fma(a1, br1, oR[r]);
-                oI[r] = fma(a1, bi1, oI[r]);
-            }
-        }
-        __syncthreads();
-    }
-    const int f = f0 + tx;
-    if (f >= batch) return;
-    double2* out = F + (long long)f * ldF + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const int j = j0 + ty * 4 + r;
-        if (j >= nh) continue;
-        out[j] = make_double2(eR[r] + oR[r], eI[r] + oI[r]);
-        out[nlat - 1 - j] = make_double2(eR[r] - oR[r], eI[r] - oI[r]);
-    }
-}
-
-// grid: x = degree tile, y = column tile, z = m slot
-__global__ void __launch_bounds__(NT) k_legendre_analysis(const double* __restrict__ plm, const long long* __restrict__ poff,
-                                                          int nh, int nlat, const double* __restrict__ w,
-                                                          const double2* __restrict__ F, long long ldF,
-                                                          double2* __restrict__ spec, SpecMap sm, int batch) {
-    __shared__ double Ps[TK][TLT + 1];
-    __shared__ double Ss[TK][TC + 1];
-    __shared__ double Ds[TK][TC + 1];
-    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
-    const int am = m < 0 ? -m : m;
-    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
-    const int lmax = sm.lmax;
-    const int lbase = am + blockIdx.x * TLT;
-    if (lbase > lmax) return;
-    const int f0 = blockIdx.y * (TC / 2);
-    const int tid = threadIdx.x;
-    const int tx = tid & 15;
-    const int ty = tid >> 4;  // degrees lbase + ty + 16 r, r = 0..3 (same parity)
-    const double* P = plm + poff[am];
-    const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
-    const bool odd = ((lbase + ty - am) & 1) != 0;
-
-    double aR[4] = {0, 0, 0, 0}, aI[4] = {0, 0, 0, 0};
-    for (int j0 = 0; j0 < nh; j0 += TK) {
-        for (int idx = tid; idx < TK * TLT; idx += NT) {
-            const int ll = idx / TK, kk = idx - ll * TK;
-            const int l = lbase + ll, j = j0 + kk;
-            Ps[kk][ll] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
-        }
-        {
-            const int kk = tid & 15, ff = tid >> 4;
-            const int j = j0 + kk, f = f0 + ff;
-            double2 s = make_double2(0, 0), d = make_double2(0, 0);
-            if (j < nh && f < batch) {
-                const double2* Ff = Fm + (long long)f * ldF;
-                const double2 n = Ff[j], so = Ff[nlat - 1 - j];
-                const double wj = w[j];
-                s = make_double2(wj * (n.x + so.x), wj * (n.y + so.y));
-                d = make_double2(wj * (n.x - so.x), wj * (n.y - so.y));
-            }
-            Ss[kk][2 * ff] = s.x;
-            Ss[kk][2 * ff + 1] = s.y;
-            Ds[kk][2 * ff] = d.x;
-            Ds[kk][2 * ff + 1] = d.y;
-        }
-        __syncthreads();
-        const double(*G)[TC + 1] = odd ? Ds : Ss;
-#pragma unroll
-        for (int kk = 0; kk < TK; kk++) {
-            const double gr = G[kk][2 * tx], gi = G[kk][2 * tx + 1];
-#pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const double p = Ps[kk][ty + 16 * r];
-                aR[r] = fma(p, gr, aR[r]);
-                aI[r] = fma(p, gi, aI[r]);
-            }
-        }
-        __syncthreads();
-    }
-    const int f = f0 + tx;
-    if (f >= batch) return;
-    double2* out = spec + (long long)f * sm.ld;
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const int l = lbase + ty + 16 * r;
-        if (l <= lmax) out[spec_index(sm, l, m)] = make_double2(aR[r], aI[r]);
-    }
-}
-
-// Wide-tile variants for larger batches: CTA tile 64 rows x 64 real columns
-// (32 fields), 128 threads with 8 rows x 4 columns each (64 / 32 FP64
-// accumulators), contraction chunks of 16 double-buffered in shared memory
-// with the next chunk's global loads issued before the current chunk's FMAs.
-// Per k step a thread loads 4 + 2 (+2) double2 from shared memory for 32 FMAs.
-namespace {
-constexpr int WR = 64;        // rows per CTA (latitudes, or degrees in the analysis)
-constexpr int WC = 64;        // real columns per CTA
-constexpr int WK = 16;        // contraction chunk
-constexpr int WNT = 128;      // threads
-constexpr int WP = WR + 2;    // padded shared-memory row (16-byte aligned, spreads banks)
-constexpr int WSMEM_ANA = 3 * 2 * WK * WP * (int)sizeof(double);  // analysis: P, sum, difference tiles
-}  // namespace
-
-__global__ void __launch_bounds__(WNT) k_legendre_synthesis_w(const double* __restrict__ plm,
-                                                                   const long long* __restrict__ poff, int nh, int nlat,
-                                                                   const double2* __restrict__ spec, SpecMap sm,
-                                                                   double2* __restrict__ F, long long ldF, int batch) {
-    __shared__ __align__(16) double As[2][WK][WP];
-    __shared__ __align__(16) double Bs[2][WK][WP];
-    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
-    const int am = m < 0 ? -m : m;
-    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
-    const int lmax = sm.lmax;
-    const int j0 = blockIdx.x * WR;
-    const int f0 = blockIdx.y * (WC / 2);
-    const int tid = threadIdx.x;
-    const int tx = tid & 15;  // columns 4 tx .. 4 tx + 3 (fields f0 + 2 tx, f0 + 2 tx + 1)
-    const int ty = tid >> 4;  // rows 8 ty .. 8 ty + 7
-    const double* P = plm + poff[am];
-
-    double ra[8];
-    double2 rb[4];
-    auto fetch = [&](int l0) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int idx = tid + WNT * i, kk = idx / WR, jj = idx % WR;
-            const int l = l0 + kk, j = j0 + jj;
-            ra[i] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
-            const int l = l0 + kk, f = f0 + ff;
-            rb[i] = (l <= lmax && f < batch) ? spec[(long long)f * sm.ld + spec_index(sm, l, m)] : make_double2(0, 0);
-        }
-    };
-    auto stash = [&](int b) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int idx = tid + WNT * i;
-            As[b][idx / WR][idx % WR] = ra[i];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
-            *reinterpret_cast<double2*>(&Bs[b][kk][2 * ff]) = rb[i];
-        }
-    };
-
-    double E[8][4], O[8][4];
-#pragma unroll
-    for (int r = 0; r < 8; r++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) E[r][c] = O[r][c] = 0.0;
-
-    fetch(am);
-    stash(0);
-    __syncthreads();
-    int cur = 0;
-    for (int l0 = am; l0 <= lmax; l0 += WK) {
-        const bool more = l0 + WK <= lmax;
-        if (more) fetch(l0 + WK);
-#pragma unroll
-        for (int kk = 0; kk < WK; kk++) {
-            double a[8], b[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const double2 v = *reinterpret_cast<const double2*>(&As[cur][kk][8 * ty + 2 * q]);
-                a[2 * q] = v.x;
-                a[2 * q + 1] = v.y;
-            }
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const double2 v = *reinterpret_cast<const double2*>(&Bs[cur][kk][4 * tx + 2 * q]);
-                b[2 * q] = v.x;
-                b[2 * q + 1] = v.y;
-            }
-            // degree l0 + kk has the parity of kk (l0 - am is a multiple of 16)
-#pragma unroll
-            for (int r = 0; r < 8; r++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    if (kk & 1) O[r][c] = fma(a[r], b[c], O[r][c]);
-                    else E[r][c] = fma(a[r], b[c], E[r][c]);
-                }
-        }
-        if (more) stash(cur ^ 1);
-        __syncthreads();
-        cur ^= 1;
-    }
-    double2* outm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
-#pragma unroll
-    for (int c = 0; c < 2; c++) {
-        const int f = f0 + 2 * tx + c;
-        if (f >= batch) continue;
-        double2* out = outm + (long long)f * ldF;
-#pragma unroll
-        for (int r = 0; r < 8; r++) {
-            const int j = j0 + 8 * ty + r;
-            if (j >= nh) continue;
-            out[j] = make_double2(E[r][2 * c] + O[r][2 * c], E[r][2 * c + 1] + O[r][2 * c + 1]);
-            out[nlat - 1 - j] = make_double2(E[r][2 * c] - O[r][2 * c], E[r][2 * c + 1] - O[r][2 * c + 1]);
-        }
-    }
-}
-
-__global__ void __launch_bounds__(WNT) k_legendre_analysis_w(const double* __restrict__ plm,
-                                                                  const long long* __restrict__ poff, int nh, int nlat,
-                                                                  const double* __restrict__ w,
-                                                                  const double2* __restrict__ F, long long ldF,
-                                                                  double2* __restrict__ spec, SpecMap sm, int batch) {
-    extern __shared__ __align__(16) double wsm[];
-    double(*Ps)[WK][WP] = reinterpret_cast<double(*)[WK][WP]>(wsm);
-    double(*Ss)[WK][WP] = Ps + 2;
-    double(*Ds)[WK][WP] = Ps + 4;
-    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
-    const int am = m < 0 ? -m : m;
-    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
-    const int lmax = sm.lmax;
-    const int lbase = am + blockIdx.x * WR;
-    if (lbase > lmax) return;
-    const int f0 = blockIdx.y * (WC / 2);
-    const int tid = threadIdx.x;
-    const int tx = tid & 15;
-    const int ty = tid >> 4;
-    // the 64 degrees of the tile by parity (lbase - am is a multiple of 64):
-    // degree lbase + 2 e + par is shared-memory row par * 32 + e; a thread
-    // takes 8 degrees of one parity, e = e0 .. e0 + 7, and so needs only the
-    // sum (even) or the difference (odd) columns
-    const int par = ty >> 2, e0 = 8 * (ty & 3);
-    const double* P = plm + poff[am];
-    const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
-
-    double rp[8];
-    double2 rs[4], rd[4];
-    auto fetch = [&](int j0) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int idx = tid + WNT * i, kk = idx & 15, ll = idx >> 4;
-            const int l = lbase + ll, j = j0 + kk;
-            rp[i] = (l <= lmax && j < nh) ? P[(long long)(l - am) * nh + j] * sg : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
-            const int j = j0 + kk, f = f0 + ff;
-            double2 sv = make_double2(0, 0), dv = make_double2(0, 0);
-            if (j < nh && f < batch) {
-                const double2* Ff = Fm + (long long)f * ldF;
-                const double2 n = Ff[j], so = Ff[nlat - 1 - j];
-                const double wj = w[j];
-                sv = make_double2(wj * (n.x + so.x), wj * (n.y + so.y));
-                dv = make_double2(wj * (n.x - so.x), wj * (n.y - so.y));
-            }
-            rs[i] = sv;
-            rd[i] = dv;
-        }
-    };
-    auto stash = [&](int b) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int idx = tid + WNT * i;
-            const int ll = idx >> 4;
-            Ps[b][idx & 15][(ll & 1) * 32 + (ll >> 1)] = rp[i];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int idx = tid + WNT * i, kk = idx & 15, ff = idx >> 4;
-            *reinterpret_cast<double2*>(&Ss[b][kk][2 * ff]) = rs[i];
-            *reinterpret_cast<double2*>(&Ds[b][kk][2 * ff]) = rd[i];
-        }
-    };
-
-    double acc[8][4];
-#pragma unroll
-    for (int r = 0; r < 8; r++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
-
-    fetch(0);
-    stash(0);
-    __syncthreads();
-    int cur = 0;
-    for (int j0 = 0; j0 < nh; j0 += WK) {
-        const bool more = j0 + WK < nh;
-        if (more) fetch(j0 + WK);
-        const double(*G)[WK][WP] = par ? Ds : Ss;
-#pragma unroll
-        for (int kk = 0; kk < WK; kk++) {
-            double p[8], g[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const double2 v = *reinterpret_cast<const double2*>(&Ps[cur][kk][par * 32 + e0 + 2 * q]);
-                p[2 * q] = v.x;
-                p[2 * q + 1] = v.y;
-            }
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const double2 u = *reinterpret_cast<const double2*>(&G[cur][kk][4 * tx + 2 * q]);
-                g[2 * q] = u.x;
-                g[2 * q + 1] = u.y;
-            }
-#pragma unroll
-            for (int r = 0; r < 8; r++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) acc[r][c] = fma(p[r], g[c], acc[r][c]);
-        }
-        if (more) stash(cur ^ 1);
-        __syncthreads();
-        cur ^= 1;
-    }
-#pragma unroll
-    for (int c = 0; c < 2; c++) {
-        const int f = f0 + 2 * tx + c;
-        if (f >= batch) continue;
-        double2* out = spec + (long long)f * sm.ld;
-#pragma unroll
-        for (int r = 0; r < 8; r++) {
-            const int l = lbase + 2 * (e0 + r) + par;
-            if (l <= lmax) out[spec_index(sm, l, m)] = make_double2(acc[r][2 * c], acc[r][2 * c + 1]);
-        }
-    }
-}
-
-// Small-batch variants (batch <= NB <= 8).  With one to a few fields the
-// tiled kernels above fill 1/16 .. 1/2 of their column tile and walk the
-// degrees in short chunks, each a global-load round trip and two barriers
-// long: bound by latency (54-70 us per launch at T255 for 1-8 fields, where
-// the 50 MB table streams in ~8 us).  Here the table is streamed with 8 to
-// 16 independent loads per thread in flight (the next 8 rows' loads go out
-// before the current 8 rows' sums) and the fields' values come from shared
-// memory, staged for the whole degree (latitude) range of the m at once where
-// it fits in 48 KB:
-//   synthesis: a CTA takes 32 latitudes of one m; warp q sums the degrees
-//     l = |m| + q (mod 8), so that a thread's terms all have the parity of q;
-//     the eight classes meet in shared memory, E = even q, O = odd q.
-//   analysis: a CTA takes 32 degrees of one m, 8 lanes per degree, each lane
-//     a strided eighth of the latitudes, against the weighted north + south
-//     (even degrees) and north - south (odd) values of the fields; the 8
-//     lanes of a degree are summed by shuffles at the end.
-// Shared arrays are field-major with the degree / latitude innermost, so
-// that the lanes of a warp read consecutive 16-byte words.
-namespace {
-constexpr int SNT = 256;              // threads
-constexpr int SJ = 32;                // latitudes per CTA (synthesis)
-constexpr int SQ = SNT / SJ;          // degree classes (synthesis)
-constexpr int AL = 32;                // degrees per CTA (analysis)
-constexpr int ALANES = 8;             // lanes per degree (analysis)
-constexpr int NB_SMEM = 48 * 1024;    // shared-memory budget of both kernels
-constexpr int NBATCH = 4;             // staging loads in flight per thread
-#ifndef SPH_NB_MAX
-#define SPH_NB_MAX 8
-#endif
-constexpr int NB_MAX = SPH_NB_MAX;    // largest batch given to the small-batch kernels
-// degrees (synthesis) or latitudes (analysis) staged per chunk: the whole
-// range where it fits, else the largest multiple of 64 that does
-inline int nb_chunk(int n, int bytes_per) {
-    const int cap = (NB_SMEM / bytes_per) / 64 * 64;
-    const int want = (n + 63) / 64 * 64;
-    return want < cap ? want : cap;
-}
-}  // namespace
-
-template <int NB>
-__global__ void __launch_bounds__(SNT) k_legendre_synthesis_nb(const double* __restrict__ plm,
-                                                               const long long* __restrict__ poff, int nh, int nlat,
-                                                               const double2* __restrict__ spec, SpecMap sm,
-                                                               double2* __restrict__ F, long long ldF, int batch,
-                                                               int cq) {
-    extern __shared__ double2 sh[];  // Q[NB][cq] during the sums, then R[SQ][NB][SJ]
-    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
-    const int am = m < 0 ? -m : m;
-    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
-    const int lmax = sm.lmax;
-    const int tid = threadIdx.x;
-    const int jl = tid % SJ, q = tid / SJ;
-    const int j = blockIdx.x * SJ + jl;
-    const bool jv = j < nh;
-    const double* P = plm + poff[am] + (jv ? j : 0);
-    double2 acc[NB];
-#pragma unroll
-    for (int f = 0; f < NB; f++) acc[f] = make_double2(0, 0);
-    for (int lc = am; lc <= lmax; lc += cq) {
-        const int nk = min(cq, lmax + 1 - lc);
-        // stage the chunk's spectra, NBATCH loads in flight per thread
-        for (int base = tid; base < cq * NB; base += NBATCH * SNT) {
-            double2 v[NBATCH];
-#pragma unroll
-            for (int u = 0; u < NBATCH; u++) {
-                const int idx = base + u * SNT;
-                const int f = idx / cq, kk = idx - f * cq;
-                v[u] = (idx < cq * NB && kk < nk && f < batch) ? spec[(long long)f * sm.ld + spec_index(sm, lc + kk, m)]
-                                                               : make_double2(0, 0);
-            }
-#pragma unroll
-            for (int u = 0; u < NBATCH; u++) {
-                const int idx = base + u * SNT;
-                if (idx < cq * NB) sh[idx] = make_double2(v[u].x * sg, v[u].y * sg);
-            }
-        }
-        __syncthreads();
-        // degrees kk = q + 8 i of the chunk; the table loads of the next 8 are
-        // issued before the sums of the current 8
-        const int ni = nk > q ? (nk - q + SQ - 1) / SQ : 0;
-        auto ldp = [&](int i) -> double {
-            return (jv && i < ni) ? __ldg(P + (long long)(lc + q + SQ * i - am) * nh) : 0.0;
-        };
-        double pc[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) pc[u] = ldp(u);
-        for (int i0 = 0; i0 < ni; i0 += 8) {
-            double pn[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) pn[u] = ldp(i0 + 8 + u);
-#pragma unroll
-            for (int u = 0; u < 8; u++) {
-                const int i = i0 + u;
-                if (i >= ni) break;
-                const int kk = q + SQ * i;
-#pragma unroll
-                for (int f = 0; f < NB; f++) {
-                    const double2 c = sh[f * cq + kk];
-                    acc[f].x = fma(pc[u], c.x, acc[f].x);
-                    acc[f].y = fma(pc[u], c.y, acc[f].y);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 8; u++) pc[u] = pn[u];
-        }
-        __syncthreads();
-    }
-    double2* R = sh;  // [SQ][NB][SJ]
-#pragma unroll
-    for (int f = 0; f < NB; f++) R[(q * NB + f) * SJ + jl] = acc[f];
-    __syncthreads();
-    double2* out = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
-    for (int idx = tid; idx < SJ * NB; idx += SNT) {
-        const int jj = idx % SJ, f = idx / SJ;
-        const int jo = blockIdx.x * SJ + jj;
-        if (jo >= nh || f >= batch) continue;
-        double er = 0, ei = 0, orr = 0, oi = 0;
-#pragma unroll
-        for (int c = 0; c < SQ; c += 2) {
-            const double2 e = R[(c * NB + f) * SJ + jj], o = R[((c + 1) * NB + f) * SJ + jj];
-            er += e.x;
-            ei += e.y;
-            orr += o.x;
-            oi += o.y;
-        }
-        double2* o = out + (long long)f * ldF;
-        o[jo] = make_double2(er + orr, ei + oi);
-        o[nlat - 1 - jo] = make_double2(er - orr, ei - oi);
-    }
-}
-
-template <int NB>
-__global__ void __launch_bounds__(SNT) k_legendre_analysis_nb(const double* __restrict__ plm,
-                                                              const long long* __restrict__ poff, int nh, int nlat,
-                                                              const double* __restrict__ w,
-                                                              const double2* __restrict__ F, long long ldF,
-                                                              double2* __restrict__ spec, SpecMap sm, int batch,
-                                                              int cj) {
-    extern __shared__ double2 sh[];  // G[2][NB][cj]: weighted north + south, north - south
-    const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
-    const int am = m < 0 ? -m : m;
-    const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
-    const int lmax = sm.lmax;
-    const int lbase = am + blockIdx.x * AL;
-    if (lbase > lmax) return;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g = lane / ALANES, t = lane % ALANES;
-    const int l = lbase + warp * (32 / ALANES) + g;
-    const bool lv = l <= lmax;
-    const int par = (l - am) & 1;
-    const double* Pl = plm + poff[am] + (long long)((lv ? l : am) - am) * nh;
-    const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
-    double2 acc[NB];
-#pragma unroll
-    for (int f = 0; f < NB; f++) acc[f] = make_double2(0, 0);
-    for (int jc = 0; jc < nh; jc += cj) {
-        const int nj = min(cj, nh - jc);
-        // stage the chunk's weighted sums and differences, NBATCH entries in flight per thread
-        for (int base = tid; base < cj * NB; base += NBATCH * SNT) {
-            double2 n[NBATCH], so[NBATCH];
-            double wj[NBATCH];
-#pragma unroll
-            for (int u = 0; u < NBATCH; u++) {
-                const int idx = base + u * SNT;
-                const int f = idx / cj, jj = idx - f * cj;
-                const bool v = idx < cj * NB && jj < nj && f < batch;
-                const double2* Ff = Fm + (long long)(v ? f : 0) * ldF;
-                const int j = jc + (v ? jj : 0);
-                n[u] = v ? Ff[j] : make_double2(0, 0);
-                so[u] = v ? Ff[nlat - 1 - j] : make_double2(0, 0);
-                wj[u] = v ? w[j] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < NBATCH; u++) {
-                const int idx = base + u * SNT;
-                if (idx >= cj * NB) break;
-                sh[idx] = make_double2(wj[u] * (n[u].x + so[u].x), wj[u] * (n[u].y + so[u].y));
-                sh[NB * cj + idx] = make_double2(wj[u] * (n[u].x - so[u].x), wj[u] * (n[u].y - so[u].y));
-            }
-        }
-        __syncthreads();
-        // latitudes jj = t + 8 i of the chunk; the table loads of the next 8
-        // are issued before the sums of the current 8
-        const double2* G = sh + par * NB * cj;
-        const int ni = nj > t ? (nj - t + ALANES - 1) / ALANES : 0;
-        auto ldp = [&](int i) -> double { return (lv && i < ni) ? __ldg(Pl + jc + t + ALANES * i) : 0.0; };
-        double pc[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) pc[u] = ldp(u);
-        for (int i0 = 0; i0 < ni; i0 += 8) {
-            double pn[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) pn[u] = ldp(i0 + 8 + u);
-#pragma unroll
-            for (int u = 0; u < 8; u++) {
-                const int i = i0 + u;
-                if (i >= ni) break;
-                const int jj = t + ALANES * i;
-#pragma unroll
-                for (int f = 0; f < NB; f++) {
-                    const double2 c = G[f * cj + jj];
-                    acc[f].x = fma(pc[u], c.x, acc[f].x);
-                    acc[f].y = fma(pc[u], c.y, acc[f].y);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 8; u++) pc[u] = pn[u];
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int f = 0; f < NB; f++) {
-#pragma unroll
-        for (int o = ALANES / 2; o > 0; o >>= 1) {
-            acc[f].x += __shfl_xor_sync(0xffffffffu, acc[f].x, o);
-            acc[f].y += __shfl_xor_sync(0xffffffffu, acc[f].y, o);
-        }
-    }
-    if (!lv) return;
-    // lane t of the degree writes field t
-#pragma unroll
-    for (int f = 0; f < NB; f++)
-        if (f == t && f < batch)
-            spec[(long long)f * sm.ld + spec_index(sm, l, m)] = make_double2(acc[f].x * sg, acc[f].y * sg);
-}
-
-// FP64 tensor-core variants (mma.sync m8n8k4 f64, the FP64 MMA of sm_100;
-// tcgen05 has no FP64 kind).  One instruction is an 8 x 8 x 4 product, 256
-// FMAs from one table value and one field value per lane, where the FMA
-// kernels above need a shared-memory load per one or two FMAs.  Per m the
+// The kernels use mma.sync m8n8k4 f64, the FP64 MMA of sm_100 (tcgen05 has
+// no FP64 kind; measured here 37 TFLOP/s against 34 for scalar FMA).  One
+// instruction is an 8 x 8 x 4 product, 256 FMAs from one table value and one
+// field value per lane, where register-tiled FMA kernels need a shared-memory
+// load per one to four FMAs (those measured 158 / 206 us for the 64-field
+// synthesis / analysis at T255, 33 / 48 us for 8 fields; these 139 / 124 and
+// 19 / 21 us).  Per m the
 // columns (field, re/im) are cut in blocks of CN = 8 RN (4 RN fields); a
 // warp owns 16 rows of one l - m parity and all CN columns (2 x RN
 // accumulator fragments of 2 doubles per lane).
@@ -995,10 +395,6 @@ __global__ void __launch_bounds__(128) k_legendre_analysis_m01(const double* __r
     if (lane == 0) spec[(long long)f * ld_spec + pidx(lmax, l, m)] = acc;
 }
 
-#ifndef SPH_LEG_MMA
-#define SPH_LEG_MMA 1
-#endif
-
 // column-block width of the tensor-core kernels for a batch: 4, 8 or 16 fields
 static int mma_rn(int batch) { return batch <= 4 ? 1 : batch <= 8 ? 2 : 4; }
 
@@ -1006,44 +402,17 @@ static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double
                         cudaStream_t s) {
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
-    if (SPH_LEG_MMA) {
-        const int rn = mma_rn(batch), cn = 8 * rn;
-        const int kc = mma_chunk((sm.lmax + 2) / 2, cn);
-        // staged spectra, then the odd sums of the 4 warp pairs
-        const size_t smem = (size_t)std::max(2 * cn * (kc + 4), 4 * 2 * rn * 2 * 32) * sizeof(double);
-        const dim3 grid((h->nh + MNT / 4 - 1) / (MNT / 4), (2 * batch + cn - 1) / cn, nm);
+    const int rn = mma_rn(batch), cn = 8 * rn;
+    const int kc = mma_chunk((sm.lmax + 2) / 2, cn);
+    // staged spectra, then the odd sums of the 4 warp pairs
+    const size_t smem = (size_t)std::max(2 * cn * (kc + 4), 4 * 2 * rn * 2 * 32) * sizeof(double);
+    const dim3 grid((h->nh + MNT / 4 - 1) / (MNT / 4), (2 * batch + cn - 1) / cn, nm);
 #define SYN_MMA(RN) \
     k_legendre_synthesis_mma<RN><<<grid, MNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch, kc)
-        if (rn == 1) SYN_MMA(1);
-        else if (rn == 2) SYN_MMA(2);
-        else SYN_MMA(4);
+    if (rn == 1) SYN_MMA(1);
+    else if (rn == 2) SYN_MMA(2);
+    else SYN_MMA(4);
 #undef SYN_MMA
-        SPH_CUDA_TRY(cudaGetLastError());
-        return SPH_OK;
-    }
-    if (batch > 16) {
-        dim3 grid((h->nh + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
-        k_legendre_synthesis_w<<<grid, WNT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
-        SPH_CUDA_TRY(cudaGetLastError());
-        return SPH_OK;
-    }
-    if (batch <= NB_MAX) {
-        const dim3 grid((h->nh + SJ - 1) / SJ, 1, nm);
-        const int nb = batch == 1 ? 1 : batch == 2 ? 2 : batch <= 4 ? 4 : 8;
-        const int cq = nb_chunk(sm.lmax + 1, nb * (int)sizeof(double2));
-        const size_t smem = (size_t)std::max(cq, SQ * SJ) * nb * sizeof(double2);
-#define SYN_NB(NB) \
-    k_legendre_synthesis_nb<NB><<<grid, SNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch, cq)
-        if (nb == 1) SYN_NB(1);
-        else if (nb == 2) SYN_NB(2);
-        else if (nb == 4) SYN_NB(4);
-        else SYN_NB(8);
-#undef SYN_NB
-        SPH_CUDA_TRY(cudaGetLastError());
-        return SPH_OK;
-    }
-    dim3 grid((h->nh + TJ - 1) / TJ, (batch + TC / 2 - 1) / (TC / 2), nm);
-    k_legendre_synthesis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, spec, sm, F, ldF, batch);
     SPH_CUDA_TRY(cudaGetLastError());
     return SPH_OK;
 }
@@ -1053,47 +422,17 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
     if (!wts) wts = h->w;
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
-    if (SPH_LEG_MMA) {
-        const int rn = mma_rn(batch), cn = 8 * rn;
-        const int cj = mma_chunk(h->nh, cn);
-        const size_t smem = (size_t)2 * cn * (cj + 4) * sizeof(double);
-        const dim3 grid((sm.lmax + 1 + MNT / 2 - 1) / (MNT / 2), (2 * batch + cn - 1) / cn, nm);
+    const int rn = mma_rn(batch), cn = 8 * rn;
+    const int cj = mma_chunk(h->nh, cn);
+    const size_t smem = (size_t)2 * cn * (cj + 4) * sizeof(double);
+    const dim3 grid((sm.lmax + 1 + MNT / 2 - 1) / (MNT / 2), (2 * batch + cn - 1) / cn, nm);
 #define ANA_MMA(RN)                                                                                                  \
     k_legendre_analysis_mma<RN><<<grid, MNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch, \
                                                         cj)
-        if (rn == 1) ANA_MMA(1);
-        else if (rn == 2) ANA_MMA(2);
-        else ANA_MMA(4);
+    if (rn == 1) ANA_MMA(1);
+    else if (rn == 2) ANA_MMA(2);
+    else ANA_MMA(4);
 #undef ANA_MMA
-    } else if (batch > 16) {
-        // the shared-memory opt-in is a per-device attribute: once per device
-        static std::atomic<unsigned long long> attr_done{0};
-        const unsigned long long bit = h->device >= 0 && h->device < 64 ? 1ull << h->device : 0ull;
-        if (!bit || !(attr_done.load() & bit)) {
-            SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_w, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              WSMEM_ANA));
-            attr_done.fetch_or(bit);
-        }
-        dim3 grid((sm.lmax + 1 + WR - 1) / WR, (batch + WC / 2 - 1) / (WC / 2), nm);
-        k_legendre_analysis_w<<<grid, WNT, WSMEM_ANA, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm,
-                                                        batch);
-    } else if (batch <= NB_MAX) {
-        const dim3 grid((sm.lmax + 1 + AL - 1) / AL, 1, nm);
-        const int nb = batch == 1 ? 1 : batch == 2 ? 2 : batch <= 4 ? 4 : 8;
-        const int cj = nb_chunk(h->nh, 2 * nb * (int)sizeof(double2));
-        const size_t smem = (size_t)2 * nb * cj * sizeof(double2);
-#define ANA_NB(NB)                                                                                                   \
-    k_legendre_analysis_nb<NB><<<grid, SNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch, \
-                                                       cj)
-        if (nb == 1) ANA_NB(1);
-        else if (nb == 2) ANA_NB(2);
-        else if (nb == 4) ANA_NB(4);
-        else ANA_NB(8);
-#undef ANA_NB
-    } else {
-        dim3 grid((sm.lmax + 1 + TLT - 1) / TLT, (batch + TC / 2 - 1) / (TC / 2), nm);
-        k_legendre_analysis<<<grid, NT, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch);
-    }
     SPH_CUDA_TRY(cudaGetLastError());
     if (!sm.cplx && sm.lmax > h->L) {
         k_zero_top<<<(batch + 127) / 128, 128, 0, s>>>(spec, sm.ld, sm.lmax, batch);
@@ -1105,24 +444,11 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
 // Query every FP64 Legendre kernel once.  Under lazy module loading (the
 // CUDA default) a kernel's code is loaded onto the device on first use; the
 // query loads it at handle creation instead, so that later calls (among them
-// the no-allocation synthesis) load nothing.
+// the no-allocation synthesis) load nothing.  The shared-memory opt-in of the
+// tensor-core kernels is set here too, before any launch, also before
+// launches inside a stream capture.
 int legendre_kernels_init() {
     cudaFuncAttributes fa;
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_w));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_w));
-    // the wide analysis needs its shared-memory opt-in on this device before any
-    // launch, also before launches inside a stream capture
-    SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_w, cudaFuncAttributeMaxDynamicSharedMemorySize, WSMEM_ANA));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<1>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<2>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<4>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_nb<8>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<1>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<2>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<4>));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_nb<8>));
     // the tensor-core kernels take up to MSMEM of dynamic shared memory
     SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_synthesis_mma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
     SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_synthesis_mma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
