@@ -427,9 +427,11 @@ def run_ours(args, rank, world):
                      "synthesis_tflops": per_contr * N_SCALAR / t_syn / 1e12,
                      "analysis_tflops": per_contr * N_SCALAR / t_ana / 1e12}
         # the small batches of the RK4 stages (first fields of the same spectra;
-        # built-in kernel variants): synthesis / analysis us
+        # mixed handle: variants autotuned per batch): synthesis / analysis us
         small = {}
-        for nb in (1, 4, 8, 16):
+        for nb in (1, 2, 4, 8):
+            if name == "mixed":
+                c.s.autotune(nb)
             sp, fo, so = spec[:nb], four[:nb], c.spec_out[:nb]
             c.s.legendre_synthesis(sp, fo)
             c.s.legendre_analysis(fo, so)
