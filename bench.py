@@ -556,8 +556,8 @@ def rk4_rates(dev, args):
             ms = _time(lambda: s.swe_rk4(p, st, n), 1, torch.cuda.current_stream()) / n
             capi.check(capi.lib().sph_sync(s.h, None))
             states[name] = st
-            res[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms}
             launches = capi.lib().sph_swe_rk4_launches(s.h)
+            res[name] = {"steps_per_s": 1000.0 / ms, "ms_per_step": ms, "kernel_launches_per_step": launches}
             s.close()
         names = ("h", "u", "v") if form == 1 else ("h", "vorticity", "divergence")
         rel = {q: float(torch.linalg.vector_norm(states["mixed"][k] - states["fp64"][k]) /
