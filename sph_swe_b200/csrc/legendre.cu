@@ -66,6 +66,13 @@ inline int mma_chunk(int n, int cn) {
 }
 }  // namespace
 
+// steps of table values in flight per warp (16 contraction terms each): two
+// in the synthesis with 16-field column blocks (T255 x 64 fields: 140 -> 117
+// us), one elsewhere (more registers cost the narrow blocks and the analysis
+// more occupancy than the extra loads in flight gain)
+constexpr int mma_depth_syn(int rn) { return rn == 4 ? 2 : 1; }
+constexpr int mma_depth_ana(int) { return 1; }
+
 #ifdef SPH_MMA_MINB
 #define MMA_LB __launch_bounds__(MNT, SPH_MMA_MINB)
 #else
@@ -140,32 +147,44 @@ __global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
         const double* G = msh + (p * CN + g) * S + t;  // column 8 nb + g, latitude j0 + t
         // latitudes past nh - 1 read latitude nh - 1 (their staged values are zero)
         const int jlast = nh - 1 - jc - t;
-        double a[4][2];
-        auto lda = [&](int j0) {
+        // a ring of D steps of table values: step s + D is loaded before the
+        // MMAs of step s
+        constexpr int D = mma_depth_ana(RN);
+        double a[D][4][2];
+        auto lda = [&](int j0, double(&dst)[4][2]) {
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const int j = min(j0 + 4 * k, jlast);
 #pragma unroll
-                for (int rm = 0; rm < 2; rm++) a[k][rm] = __ldg(prow[rm] + jc + j);
+                for (int rm = 0; rm < 2; rm++) dst[k][rm] = __ldg(prow[rm] + jc + j);
             }
         };
-        if (busy) lda(0);
-        for (int j0 = 0; busy && j0 < nj; j0 += 16) {
-            double an[4][2];
+        if (busy) {
 #pragma unroll
-            for (int k = 0; k < 4; k++)
+            for (int d = 0; d < D; d++)
+                if (16 * d < nj) lda(16 * d, a[d]);
+        }
+        for (int j0 = 0; busy && j0 < nj; j0 += 16 * D) {
 #pragma unroll
-                for (int rm = 0; rm < 2; rm++) an[k][rm] = a[k][rm];
-            if (j0 + 16 < nj) lda(j0 + 16);  // next step's table values, ahead of this step's MMAs
+            for (int d = 0; d < D; d++) {
+                const int js = j0 + 16 * d;
+                if (js >= nj) break;
+                double an[4][2];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                double b[RN];
+                for (int k = 0; k < 4; k++)
 #pragma unroll
-                for (int nb = 0; nb < RN; nb++) b[nb] = G[nb * 8 * S + j0 + 4 * k];
+                    for (int rm = 0; rm < 2; rm++) an[k][rm] = a[d][k][rm];
+                if (js + 16 * D < nj) lda(js + 16 * D, a[d]);
 #pragma unroll
-                for (int rm = 0; rm < 2; rm++)
+                for (int k = 0; k < 4; k++) {
+                    double b[RN];
 #pragma unroll
-                    for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], an[k][rm], b[nb]);
+                    for (int nb = 0; nb < RN; nb++) b[nb] = G[nb * 8 * S + js + 4 * k];
+#pragma unroll
+                    for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+                        for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], an[k][rm], b[nb]);
+                }
             }
         }
         __syncthreads();
@@ -240,34 +259,44 @@ __global__ void MMA_LB k_legendre_synthesis_mma(const double* __restrict__ plm,
         // table row of entry i: p + 2 (ic + i); rows past lmax read row lmax - |m|
         // (their staged spectra are zero)
         const int r0 = p + 2 * (ic + t);
-        double a[4][2];
-        auto lda = [&](int i0) {
+        constexpr int D = mma_depth_syn(RN);  // ring of D steps, as in the analysis
+        double a[D][4][2];
+        auto lda = [&](int i0, double(&dst)[4][2]) {
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const int r = min(r0 + 2 * (i0 + 4 * k), last);
                 const double* q = P + (long long)r * nh;
-                a[k][0] = __ldg(q);
-                a[k][1] = __ldg(q + d1);
+                dst[k][0] = __ldg(q);
+                dst[k][1] = __ldg(q + d1);
             }
         };
-        if (busy) lda(0);
-        for (int i0 = 0; busy && i0 < ni; i0 += 16) {
-            double an[4][2];
+        if (busy) {
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                an[k][0] = a[k][0];
-                an[k][1] = a[k][1];
-            }
-            if (i0 + 16 < ni) lda(i0 + 16);  // next step's table values, ahead of this step's MMAs
+            for (int d = 0; d < D; d++)
+                if (16 * d < ni) lda(16 * d, a[d]);
+        }
+        for (int i0 = 0; busy && i0 < ni; i0 += 16 * D) {
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                double b[RN];
+            for (int d = 0; d < D; d++) {
+                const int is = i0 + 16 * d;
+                if (is >= ni) break;
+                double an[4][2];
 #pragma unroll
-                for (int nb = 0; nb < RN; nb++) b[nb] = Q[nb * 8 * S + i0 + 4 * k];
+                for (int k = 0; k < 4; k++) {
+                    an[k][0] = a[d][k][0];
+                    an[k][1] = a[d][k][1];
+                }
+                if (is + 16 * D < ni) lda(is + 16 * D, a[d]);
 #pragma unroll
-                for (int rm = 0; rm < 2; rm++)
+                for (int k = 0; k < 4; k++) {
+                    double b[RN];
 #pragma unroll
-                    for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], an[k][rm], b[nb]);
+                    for (int nb = 0; nb < RN; nb++) b[nb] = Q[nb * 8 * S + is + 4 * k];
+#pragma unroll
+                    for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+                        for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], an[k][rm], b[nb]);
+                }
             }
         }
         __syncthreads();
