@@ -31,47 +31,67 @@ __device__ __forceinline__ long long spec_index(const SpecMap& s, int l, int m) 
 // instruction is an 8 x 8 x 4 product, 256 FMAs from one table value and one
 // field value per lane, where register-tiled FMA kernels need a shared-memory
 // load per one to four FMAs (those measured 158 / 206 us for the 64-field
-// synthesis / analysis at T255, 33 / 48 us for 8 fields; these 139 / 124 and
+// synthesis / analysis at T255, 33 / 48 us for 8 fields; these 116 / 117 and
 // 19 / 21 us).  Per m the
 // columns (field, re/im) are cut in blocks of CN = 8 RN (4 RN fields); a
 // warp owns 16 rows of one l - m parity and all CN columns (2 x RN
 // accumulator fragments of 2 doubles per lane).
-//   analysis: A = P (8 degrees x 4 latitudes, straight from the table, rows
-//     two degrees apart), B = the weighted north + south (even degrees) or
-//     north - south (odd) values of the column block, staged column-major in
-//     shared memory; a CTA of 8 warps takes 128 degrees (4 warps per parity).
+//   analysis: A = P (8 degrees x 4 latitudes, rows two degrees apart), each
+//     warp copying its 16 rows x 16 latitudes of a step into its own ring of
+//     MRING slots in shared memory with cp.async, two steps ahead of its MMAs
+//     (no registers held, no barrier between warps); B = the weighted north +
+//     south (even degrees) or north - south (odd) values of the column block,
+//     staged column-major in shared memory; a CTA of 8 warps takes 128
+//     degrees (4 warps per parity).
 //   synthesis: A = P^T (8 latitudes x 4 degrees of one parity), B = the
 //     spectra of the column block staged per parity column-major; a CTA of 8
 //     warps takes 64 latitudes, even warps summing the even degrees and odd
 //     warps the odd ones, which meet in shared memory for north E + O, south E - O.
-// Shared rows are padded to 4 (mod 16) doubles, so that the 32 lanes of a B
-// fragment load (8 columns x 4 consecutive entries) take two wavefronts.
+// Shared rows are padded to 4 (mod 16) doubles, so that the 32 lanes of an A
+// or B fragment load (8 rows or columns x 4 consecutive entries) take two
+// wavefronts.
 // Fragment layout of m8n8k4 f64 (lane = 4 g + t): A row g col t, B row t col
 // g, C row g cols 2 t, 2 t + 1.
 namespace {
 constexpr int MNT = 256;                  // threads (8 warps)
+constexpr int MRING = 3;                  // ring slots of table tiles per warp (steps in flight)
+constexpr int ASA = 20;                   // analysis tile row: 16 latitudes + 4 (two-wavefront fragment loads)
+constexpr int RING_A = 8 * MRING * 16 * ASA;  // doubles of the analysis rings of a CTA
 #ifndef SPH_MSMEM
-#define SPH_MSMEM 100352
+#define SPH_MSMEM 115712
 #endif
-constexpr int MSMEM = SPH_MSMEM;          // dynamic shared-memory budget per CTA (2 CTAs per SM)
-constexpr int MSTAGE = 8;                 // staging loads in flight per thread (synthesis)
-constexpr int MSTAGE_A = 4;               // staging entries in flight per thread (analysis: 3 loads each)
+constexpr int MSMEM = SPH_MSMEM;          // dynamic shared memory per CTA at most (2 CTAs per SM)
 constexpr int MCHUNK = 192;               // most entries staged per column and parity
 // entries staged per column and parity: the whole range where it fits (up to
-// MCHUNK), else the largest multiple of 16 that does; the row stride is that + 4
-inline int mma_chunk(int n, int cn) {
-    const int cap = std::min(MCHUNK, ((MSMEM / (2 * cn * (int)sizeof(double)) - 4) / 16) * 16);
+// MCHUNK) next to the rings of `ring` doubles, else the largest multiple of 16
+// that does; the row stride is that + 4
+inline int mma_chunk(int n, int cn, int ring) {
+    const int bytes = MSMEM - ring * (int)sizeof(double);
+    const int cap = std::min(MCHUNK, ((bytes / (2 * cn * (int)sizeof(double)) - 4) / 16) * 16);
     const int want = (n + 15) / 16 * 16;
     return want < cap ? want : cap;
 }
 }  // namespace
 
-// steps of table values in flight per warp (16 contraction terms each): two
-// in the synthesis with 16-field column blocks (T255 x 64 fields: 140 -> 117
-// us), one elsewhere (more registers cost the narrow blocks and the analysis
-// more occupancy than the extra loads in flight gain)
+// asynchronous global -> shared copies of 8 or 16 bytes (cp.async, through L1)
+__device__ __forceinline__ void acp(double* dst, const double* src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (bytes == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void acp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void acp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// steps of table values the synthesis keeps in flight per warp in registers
+// (16 contraction terms each): two with 16-field column blocks (T255 x 64
+// fields: 140 -> 117 us), one with the narrow blocks, where more registers
+// cost more occupancy than the extra loads gain.  (A shared-memory ring of
+// asynchronous copies, as in the analysis, measured slower here: its space
+// leaves less for the staged spectra, which then take more chunks.)
 constexpr int mma_depth_syn(int rn) { return rn == 4 ? 2 : 1; }
-constexpr int mma_depth_ana(int) { return 1; }
 
 #ifdef SPH_MMA_MINB
 #define MMA_LB __launch_bounds__(MNT, SPH_MMA_MINB)
@@ -87,13 +107,12 @@ __device__ __forceinline__ void dmma8844(double& c0, double& c1, double a, doubl
 
 template <int RN>
 __global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
-                                                               const long long* __restrict__ poff, int nh, int nlat,
-                                                               const double* __restrict__ w,
-                                                               const double2* __restrict__ F, long long ldF,
-                                                               double2* __restrict__ spec, SpecMap sm, int batch,
-                                                               int cj) {
+                                               const long long* __restrict__ poff, int nh, int nlat,
+                                               const double* __restrict__ w, const double2* __restrict__ F,
+                                               long long ldF, double2* __restrict__ spec, SpecMap sm, int batch,
+                                               int cj) {
     constexpr int CN = 8 * RN, NFB = CN / 2;
-    extern __shared__ double msh[];  // G[parity][CN][cj + 4]
+    extern __shared__ __align__(16) double msh[];  // G[parity][CN][cj + 4], then the warps' A rings
     const int S = cj + 4;
     const int m = sm.cplx ? (int)blockIdx.z - sm.L : (int)blockIdx.z;
     const int am = m < 0 ? -m : m;
@@ -106,14 +125,13 @@ __global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
     const int g = lane >> 2, t = lane & 3;
     const int p = warp & 1, hw = warp >> 1;
     const bool busy = lbase + p + 2 * 16 * hw <= lmax;  // some row of this warp is a degree
-    // A rows of this lane: degrees lbase + p + 2 (16 hw + 8 rm + g); rows past
-    // lmax read row |m| (their sums are not stored)
-    const double* prow[2];
-#pragma unroll
-    for (int rm = 0; rm < 2; rm++) {
-        const int l = lbase + p + 2 * (16 * hw + 8 * rm + g);
-        prow[rm] = plm + poff[am] + (long long)((l <= lmax ? l : am) - am) * nh + t;
-    }
+    // this warp's A rows: degrees lbase + p + 2 (16 hw + r), r = 8 rm + g; table
+    // row index of r (rows past lmax read the last row: their sums are not stored)
+    const double* P = plm + poff[am];
+    const int row0 = lbase - am + p + 32 * hw, last = lmax - am;
+    auto trow = [&](int r) -> const double* { return P + (long long)min(row0 + 2 * r, last) * nh; };
+    double* ring = msh + 2 * CN * S + (size_t)warp * MRING * 16 * ASA;
+    const bool v16 = (nh & 1) == 0;  // table rows 16-byte aligned: 16-byte copies
     const double2* Fm = F + (long long)(sm.cplx ? (m + sm.L) : m) * nlat;
     double acc[2][RN][2];
 #pragma unroll
@@ -123,6 +141,37 @@ __global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
 
     for (int jc = 0; jc < nh; jc += cj) {
         const int nj = min(cj, nh - jc);
+        // copy the 16 rows x 16 latitudes of step j0 into ring slot st (latitudes
+        // past nh - 1 read the row's first entry: their staged values are zero)
+        auto issue = [&](int st, int j0) {
+            double* dst = ring + st * 16 * ASA;
+            if (v16) {
+                const int c = (lane & 7) * 2, j = jc + j0 + c;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int r = (lane >> 3) + 4 * i;
+                    const double* src = trow(r) + (j < nh ? j : 0);
+                    acp(dst + r * ASA + c, src, 16);
+                }
+            } else {
+                const int c = lane & 15, j = jc + j0 + c;
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int r = (lane >> 4) + 2 * i;
+                    const double* src = trow(r) + (j < nh ? j : 0);
+                    acp(dst + r * ASA + c, src, 8);
+                }
+            }
+        };
+        const int nst = (nj + 15) / 16;
+        // the first ring slots go out before the fields are staged
+        if (busy) {
+#pragma unroll
+            for (int q = 0; q < MRING - 1; q++) {
+                if (q < nst) issue(q, 16 * q);
+                acp_commit();
+            }
+        }
         // stage the column block's weighted sums / differences, latitude-minor:
         // segment `row` = (field, 32 latitudes), warp w takes rows w, w + 8, ...
         const int nseg = (cj + 31) / 32;
@@ -145,48 +194,29 @@ __global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
         }
         __syncthreads();
         const double* G = msh + (p * CN + g) * S + t;  // column 8 nb + g, latitude j0 + t
-        // latitudes past nh - 1 read latitude nh - 1 (their staged values are zero)
-        const int jlast = nh - 1 - jc - t;
-        // a ring of D steps of table values: step s + D is loaded before the
-        // MMAs of step s
-        constexpr int D = mma_depth_ana(RN);
-        double a[D][4][2];
-        auto lda = [&](int j0, double(&dst)[4][2]) {
+        for (int q = 0; busy && q < nst; q++) {
+            // slot of step q + MRING - 1 was read at step q - 1 (the warp synced after it)
+            if (q + MRING - 1 < nst) issue((q + MRING - 1) % MRING, 16 * (q + MRING - 1));
+            acp_commit();
+            acp_wait<MRING - 1>();
+            __syncwarp();
+            const double* A = ring + (q % MRING) * 16 * ASA + g * ASA + t;
+            const int j0 = 16 * q;
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                const int j = min(j0 + 4 * k, jlast);
+                double a[2], b[RN];
 #pragma unroll
-                for (int rm = 0; rm < 2; rm++) dst[k][rm] = __ldg(prow[rm] + jc + j);
+                for (int rm = 0; rm < 2; rm++) a[rm] = A[8 * rm * ASA + 4 * k];
+#pragma unroll
+                for (int nb = 0; nb < RN; nb++) b[nb] = G[nb * 8 * S + j0 + 4 * k];
+#pragma unroll
+                for (int rm = 0; rm < 2; rm++)
+#pragma unroll
+                    for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], a[rm], b[nb]);
             }
-        };
-        if (busy) {
-#pragma unroll
-            for (int d = 0; d < D; d++)
-                if (16 * d < nj) lda(16 * d, a[d]);
+            __syncwarp();
         }
-        for (int j0 = 0; busy && j0 < nj; j0 += 16 * D) {
-#pragma unroll
-            for (int d = 0; d < D; d++) {
-                const int js = j0 + 16 * d;
-                if (js >= nj) break;
-                double an[4][2];
-#pragma unroll
-                for (int k = 0; k < 4; k++)
-#pragma unroll
-                    for (int rm = 0; rm < 2; rm++) an[k][rm] = a[d][k][rm];
-                if (js + 16 * D < nj) lda(js + 16 * D, a[d]);
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    double b[RN];
-#pragma unroll
-                    for (int nb = 0; nb < RN; nb++) b[nb] = G[nb * 8 * S + js + 4 * k];
-#pragma unroll
-                    for (int rm = 0; rm < 2; rm++)
-#pragma unroll
-                        for (int nb = 0; nb < RN; nb++) dmma8844(acc[rm][nb][0], acc[rm][nb][1], an[k][rm], b[nb]);
-                }
-            }
-        }
+        acp_wait<0>();
         __syncthreads();
     }
 #pragma unroll
@@ -259,7 +289,7 @@ __global__ void MMA_LB k_legendre_synthesis_mma(const double* __restrict__ plm,
         // table row of entry i: p + 2 (ic + i); rows past lmax read row lmax - |m|
         // (their staged spectra are zero)
         const int r0 = p + 2 * (ic + t);
-        constexpr int D = mma_depth_syn(RN);  // ring of D steps, as in the analysis
+        constexpr int D = mma_depth_syn(RN);  // register ring of D steps
         double a[D][4][2];
         auto lda = [&](int i0, double(&dst)[4][2]) {
 #pragma unroll
@@ -432,7 +462,7 @@ static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
     const int rn = mma_rn(batch), cn = 8 * rn;
-    const int kc = mma_chunk((sm.lmax + 2) / 2, cn);
+    const int kc = mma_chunk((sm.lmax + 2) / 2, cn, 0);
     // staged spectra, then the odd sums of the 4 warp pairs
     const size_t smem = (size_t)std::max(2 * cn * (kc + 4), 4 * 2 * rn * 2 * 32) * sizeof(double);
     const dim3 grid((h->nh + MNT / 4 - 1) / (MNT / 4), (2 * batch + cn - 1) / cn, nm);
@@ -452,8 +482,8 @@ static int launch_anal(const Handle* h, const double2* F, long long ldF, double2
     if (batch <= 0) return SPH_OK;
     const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
     const int rn = mma_rn(batch), cn = 8 * rn;
-    const int cj = mma_chunk(h->nh, cn);
-    const size_t smem = (size_t)2 * cn * (cj + 4) * sizeof(double);
+    const int cj = mma_chunk(h->nh, cn, RING_A);
+    const size_t smem = (size_t)(2 * cn * (cj + 4) + RING_A) * sizeof(double);
     const dim3 grid((sm.lmax + 1 + MNT / 2 - 1) / (MNT / 2), (2 * batch + cn - 1) / cn, nm);
 #define ANA_MMA(RN)                                                                                                  \
     k_legendre_analysis_mma<RN><<<grid, MNT, smem, s>>>(h->plm, h->poff, h->nh, h->nlat, wts, F, ldF, spec, sm, batch, \
