@@ -798,7 +798,8 @@ def profile_case(which="all"):
     one nonlinear RK4 step at T255 (advective and vorticity-divergence forms),
     one REXI step at T127 (M = 64) and one spectral operator pass.  which:
     "all", or one workload alone: "cfg1" (two steps of the transform
-    configuration in each form, built-in kernel variants), "rk4" (two
+    configuration in each form, built-in kernel variants), "specops" (the
+    spectral operators on 256 T255 spectra), "rk4" (two
     nonlinear RK4 steps at T255 in each form, tuned variants), "fp64x64" (two
     inverse + forward transforms of the 64 scalar T255 fields in the FP64
     form), "mixed64" (two inverse + forward transforms
@@ -825,6 +826,18 @@ def profile_case(which="all"):
                 s.vec_spat_to_SH(*s.vec_SH_to_spat(vort, div))
             capi.check(capi.lib().sph_sync(s.h, None))
             s.close()
+        print(json.dumps({"profile_case": which}))
+        return
+    if which == "specops":
+        # the spectral operators on 256 T255 spectra (135 MB, more than L2),
+        # one launch each
+        s = Sph(L_CFG1)
+        spec = torch.from_numpy(random_spec(L_CFG1, 4 * N_SCALAR, 1)).to(dev)
+        out = torch.empty_like(spec)
+        for op in ("diff_lon", "d1mu2", "mu", "mu2", "laplace", "helmholtz"):
+            s.spec_op(op, spec, a=1.0, b=2.0, out=out)
+        capi.check(capi.lib().sph_sync(s.h, None))
+        s.close()
         print(json.dumps({"profile_case": which}))
         return
     if which == "rk4":
@@ -964,7 +977,7 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel (default: the committed capture)")
     ap.add_argument("--profile-case", nargs="?", const="all", default=None,
-                    help="run one small instance of each workload (for ncu); optionally one of cfg1, rk4, fp64x64, mixed64, rexi, rexi_s0")
+                    help="run one small instance of each workload (for ncu); optionally one of cfg1, specops, rk4, fp64x64, mixed64, rexi, rexi_s0")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)
