@@ -19,37 +19,61 @@
 
 namespace sphgpu {
 
+// Thread layout of the two coefficient kernels below (packed layout of degree
+// K): block row y takes the orders y and K - y (K + 2 coefficients together;
+// for even K the middle order alone), so that rows are about equally long; a
+// thread takes one (n, m) of every field (fields blockIdx.z, + gridDim.z, ...)
+// and forms its recurrence coefficients once.  Returns false past the row.
+__device__ __forceinline__ bool vec_nm(int K, int& n, int& m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y, len0 = K + 1 - y;
+    if (i < len0) {
+        m = y;
+        n = y + i;
+    } else {
+        m = K - y;
+        if (m == y) return false;
+        n = m + (i - len0);
+    }
+    return n <= K;
+}
+
 // vort/div (degree L) -> [U, V] spectra of degree L+1
 __global__ void k_vec_prep(const double2* __restrict__ vort, const double2* __restrict__ div, long long ld,
-                           double2* __restrict__ X, int L, int nlmp) {
-    const int m = blockIdx.y;  // 0..L+1
-    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
+                           double2* __restrict__ X, int L, int nlmp, int batch) {
     const int Lp = L + 1;
-    if (n > Lp) return;
-    const int b = blockIdx.z;
-    double2* U = X + (size_t)b * 2 * nlmp;
-    double2* V = U + nlmp;
+    int n, m;
+    if (!vec_nm(Lp, n, m)) return;
     const int k = pidx(Lp, n, m);
-    if (m > L) {
-        U[k] = make_double2(0, 0);
-        V[k] = make_double2(0, 0);
-        return;
-    }
-    const double2* z = vort + (size_t)b * ld;
-    const double2* d = div + (size_t)b * ld;
-    auto inv = [&](const double2* x, int nn) -> double2 {  // lap^-1 on degree nn
-        if (nn < m || nn > L || nn == 0) return make_double2(0, 0);
-        const double s = -1.0 / ((double)nn * (nn + 1.0));
-        const double2 v = x[pidx(L, nn, m)];
-        return make_double2(v.x * s, v.y * s);
+    // lap^-1 factor of degree nn and the packed index of (nn, m) in degree L (-1: none)
+    auto slot = [&](int nn, double& sc) -> int {
+        if (m > L || nn < m || nn > L || nn == 0) {
+            sc = 0.0;
+            return -1;
+        }
+        sc = -1.0 / ((double)nn * (nn + 1.0));
+        return pidx(L, nn, m);
     };
+    double s0, sl, sh;
+    const int k0 = slot(n, s0), kl = slot(n - 1, sl), kh = slot(n + 1, sh);
     const double dn = n, dm = m;
-    const double cl = (-dn + 1.0) * idR(dn - 1, dm), ch = (dn + 2.0) * idS(dn + 1, dm);
-    const double2 psi = inv(z, n), chi = inv(d, n);
-    const double2 psl = inv(z, n - 1), psh = inv(z, n + 1), chl = inv(d, n - 1), chh = inv(d, n + 1);
-    // U = i m chi - Dex psi ; V = i m psi + Dex chi
-    U[k] = make_double2(-dm * chi.y - (cl * psl.x + ch * psh.x), dm * chi.x - (cl * psl.y + ch * psh.y));
-    V[k] = make_double2(-dm * psi.y + (cl * chl.x + ch * chh.x), dm * psi.x + (cl * chl.y + ch * chh.y));
+    const double cl = m > L ? 0.0 : (-dn + 1.0) * idR(dn - 1, dm), ch = m > L ? 0.0 : (dn + 2.0) * idS(dn + 1, dm);
+    auto ld2 = [](const double2* x, int q, double sc) -> double2 {
+        if (q < 0) return make_double2(0, 0);
+        const double2 v = x[q];
+        return make_double2(v.x * sc, v.y * sc);
+    };
+    for (int b = blockIdx.z; b < batch; b += gridDim.z) {
+        double2* U = X + (size_t)b * 2 * nlmp;
+        double2* V = U + nlmp;
+        const double2* z = vort + (size_t)b * ld;
+        const double2* d = div + (size_t)b * ld;
+        const double2 psi = ld2(z, k0, s0), chi = ld2(d, k0, s0);
+        const double2 psl = ld2(z, kl, sl), psh = ld2(z, kh, sh), chl = ld2(d, kl, sl), chh = ld2(d, kh, sh);
+        // U = i m chi - Dex psi ; V = i m psi + Dex chi (zero at m = L + 1)
+        U[k] = make_double2(-dm * chi.y - (cl * psl.x + ch * psh.x), dm * chi.x - (cl * psl.y + ch * psh.y));
+        V[k] = make_double2(-dm * psi.y + (cl * chl.x + ch * chh.x), dm * psi.x + (cl * chl.y + ch * chh.y));
+    }
 }
 
 // F[f][m][j] *= c_j^(-p)
@@ -68,25 +92,24 @@ __global__ void k_fourier_scale(double2* __restrict__ F, long long ldF, int mF, 
 
 // a(U'), a(V') of degree L+1 -> vort, div of degree L
 __global__ void k_vec_post(const double2* __restrict__ A, int nlmp, double2* __restrict__ vort, double2* __restrict__ div,
-                           long long ld, int L) {
-    const int m = blockIdx.y;
-    const int n = m + blockIdx.x * blockDim.x + threadIdx.x;
-    if (n > L) return;
-    const int b = blockIdx.z;
+                           long long ld, int L, int batch) {
+    int n, m;
+    if (!vec_nm(L, n, m)) return;
     const int Lp = L + 1;
-    const double2* aU = A + (size_t)b * 2 * nlmp;
-    const double2* aV = aU + nlmp;
-    auto at = [&](const double2* x, int nn) -> double2 {
-        if (nn < m || nn > Lp) return make_double2(0, 0);
-        return x[pidx(Lp, nn, m)];
-    };
+    auto slot = [&](int nn) -> int { return (nn < m || nn > Lp) ? -1 : pidx(Lp, nn, m); };
+    const int q0 = slot(n), ql = slot(n - 1), qh = slot(n + 1);
     const double dn = n, dm = m;
     const double el = (dn + 1.0) * idR(dn - 1, dm), eh = dn * idS(dn + 1, dm);
-    const double2 u0 = at(aU, n), ul = at(aU, n - 1), uh = at(aU, n + 1);
-    const double2 v0 = at(aV, n), vl = at(aV, n - 1), vh = at(aV, n + 1);
     const int k = pidx(L, n, m);
-    vort[(size_t)b * ld + k] = make_double2(-dm * v0.y + el * ul.x - eh * uh.x, dm * v0.x + el * ul.y - eh * uh.y);
-    div[(size_t)b * ld + k] = make_double2(-dm * u0.y - el * vl.x + eh * vh.x, dm * u0.x - el * vl.y + eh * vh.y);
+    auto at = [](const double2* x, int q) -> double2 { return q < 0 ? make_double2(0, 0) : x[q]; };
+    for (int b = blockIdx.z; b < batch; b += gridDim.z) {
+        const double2* aU = A + (size_t)b * 2 * nlmp;
+        const double2* aV = aU + nlmp;
+        const double2 u0 = at(aU, q0), ul = at(aU, ql), uh = at(aU, qh);
+        const double2 v0 = at(aV, q0), vl = at(aV, ql), vh = at(aV, qh);
+        vort[(size_t)b * ld + k] = make_double2(-dm * v0.y + el * ul.x - eh * uh.x, dm * v0.x + el * ul.y - eh * uh.y);
+        div[(size_t)b * ld + k] = make_double2(-dm * u0.y - el * vl.x + eh * vh.x, dm * u0.x - el * vl.y + eh * vh.y);
+    }
 }
 
 }  // namespace sphgpu
@@ -113,9 +136,8 @@ int sph_vec_SH_to_spat(sph_handle* hh, const double* vort, const double* div, do
     if (int rc = ensure_workspace(h, xbytes + fbytes)) return rc;
     double2* X = static_cast<double2*>(h->ws);
     double2* F = reinterpret_cast<double2*>(static_cast<char*>(h->ws) + xbytes);
-    k_vec_prep<<<dim3((Lp + 1 + 63) / 64, Lp + 1, batch), 64, 0, s>>>(reinterpret_cast<const double2*>(vort),
-                                                                     reinterpret_cast<const double2*>(div), h->nlm, X, L,
-                                                                     nlmp);
+    k_vec_prep<<<dim3((Lp + 2 + 63) / 64, (Lp + 2) / 2, std::min(batch, 16)), 64, 0, s>>>(
+        reinterpret_cast<const double2*>(vort), reinterpret_cast<const double2*>(div), h->nlm, X, L, nlmp, batch);
     SPH_CUDA_TRY(cudaGetLastError());
     if (int rc = legendre_synthesis_real(h, X, nlmp, Lp, F, ldF, 2 * batch, s, 1)) return rc;
     if (!robert) {
@@ -161,8 +183,8 @@ int sph_vec_spat_to_SH(sph_handle* hh, const double* u, const double* v, double*
         SPH_CUDA_TRY(cudaGetLastError());
     }
     if (int rc = legendre_analysis_real(h, F, ldF, A, nlmp, Lp, 2 * batch, s, 1)) return rc;
-    k_vec_post<<<dim3((L + 1 + 63) / 64, L + 1, batch), 64, 0, s>>>(A, nlmp, reinterpret_cast<double2*>(vort),
-                                                                   reinterpret_cast<double2*>(div), h->nlm, L);
+    k_vec_post<<<dim3((L + 2 + 63) / 64, (L + 2) / 2, std::min(batch, 16)), 64, 0, s>>>(
+        A, nlmp, reinterpret_cast<double2*>(vort), reinterpret_cast<double2*>(div), h->nlm, L, batch);
     SPH_CUDA_TRY(cudaGetLastError());
     return SPH_OK;
 }
