@@ -100,8 +100,11 @@ int ring_analysis_real(const Handle* h, const double* spat, long long ld_spat, d
 // period <= 16, batch a multiple of period): output k of member k/period reads
 // Fourier field (k/period)*src_stride + src[k%period], modified by mod[k%period]
 // (0 plain, 1 multiply by i*m, i.e. d/dlambda).  src = NULL: output k reads field k.
+// rowdiv (optional): ring j of every output is multiplied by 1 / rowdiv[j]
+// after the transform (the 1 / cos phi of velocities from U = u cos phi).
 int ring_synthesis_real(const Handle* h, const double2* F, long long ldF, int mF, double* spat, long long ld_spat,
-                        int batch, const int* src, const int* mod, int period, int src_stride, cudaStream_t s);
+                        int batch, const int* src, const int* mod, int period, int src_stride, cudaStream_t s,
+                        const double* rowdiv = nullptr);
 int ring_analysis_cplx(const Handle* h, const double2* spat, long long ld_spat, double2* F, long long ldF, int batch,
                        cudaStream_t s);
 int ring_synthesis_cplx(const Handle* h, const double2* F, long long ldF, double2* spat, long long ld_spat, int batch,

@@ -23,6 +23,7 @@ struct RingMap {
     int src_stride;  // Fourier fields per member
     int src[16];
     int mod[16];
+    const double* rowdiv;  // nullptr, or ring j's output times 1 / rowdiv[j] (e.g. cos phi)
 };
 
 }  // namespace sphgpu
@@ -208,7 +209,8 @@ __global__ void k_ring_synthesis_real(const double2* __restrict__ F, long long l
         const int j = j0 + jj;
         if (j >= nlat) continue;
         const double2 z = res[(jj >> 1) * n + i];
-        out[(long long)i * nlat + j] = (jj & 1) ? z.y : z.x;
+        const double v = (jj & 1) ? z.y : z.x;
+        out[(long long)i * nlat + j] = map.rowdiv ? v * (1.0 / map.rowdiv[j]) : v;
     }
 }
 
@@ -380,12 +382,14 @@ int ring_analysis_real(const Handle* h, const double* spat, long long ld_spat, d
 }
 
 int ring_synthesis_real(const Handle* h, const double2* F, long long ldF, int mF, double* spat, long long ld_spat,
-                        int batch, const int* src, const int* mod, int period, int src_stride, cudaStream_t s) {
+                        int batch, const int* src, const int* mod, int period, int src_stride, cudaStream_t s,
+                        const double* rowdiv) {
     if (batch <= 0) return SPH_OK;
     const int JT = ring_tile(h->nphi, 0);
     const size_t sm = (size_t)JT * h->nphi * sizeof(double2);
     dim3 grid((h->nlat + JT - 1) / JT, batch);
     RingMap map{};
+    map.rowdiv = rowdiv;
     if (src) {
         if (period <= 0 || period > 16 || batch % period) {
             set_error("ring synthesis: bad output map");

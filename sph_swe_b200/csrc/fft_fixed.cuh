@@ -423,6 +423,11 @@ __global__ void __launch_bounds__(fftx::nt<N, P>(), fftx::minb<N, P>()) k_ring_s
             const int t = base + u * NT;
             const int f = t % P, j = t / P, jr = j0 + 2 * f;
             if ((TOT % (U * NT) == 0 || t < TOT) && jr < nlat) {
+                if (map.rowdiv) {  // rings jr, jr + 1 times 1 / rowdiv
+                    const double s0 = 1.0 / map.rowdiv[jr], s1 = jr + 1 < nlat ? 1.0 / map.rowdiv[jr + 1] : 0.0;
+#pragma unroll
+                    for (int r = 0; r < 3; r++) x[u][r] = make_double2(x[u][r].x * s0, x[u][r].y * s1);
+                }
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
                     double* p = out + (long long)(j + r * N3) * nlat + jr;

@@ -140,14 +140,13 @@ int sph_vec_SH_to_spat(sph_handle* hh, const double* vort, const double* div, do
         reinterpret_cast<const double2*>(vort), reinterpret_cast<const double2*>(div), h->nlm, X, L, nlmp, batch);
     SPH_CUDA_TRY(cudaGetLastError());
     if (int rc = legendre_synthesis_real(h, X, nlmp, Lp, F, ldF, 2 * batch, s, 1)) return rc;
-    if (!robert) {
-        k_fourier_scale<<<dim3((unsigned)((ldF + 255) / 256), 2 * batch), 256, 0, s>>>(F, ldF, mF, h->nlat, h->cosphi, 1);
-        SPH_CUDA_TRY(cudaGetLastError());
-    }
-    // outputs: member b -> u (field 2b) and v (field 2b+1) written to separate arrays
+    // outputs: member b -> u (field 2b) and v (field 2b+1) written to separate
+    // arrays; velocities u = U / cos phi: the ring synthesis divides its
+    // output rings (Robert form: U, V as they are)
     for (int c = 0; c < 2; c++) {
         const int srcs[1] = {c};
-        if (int rc = ring_synthesis_real(h, F, ldF, mF, c == 0 ? u : v, h->nspat, batch, srcs, nullptr, 1, 2, s))
+        if (int rc = ring_synthesis_real(h, F, ldF, mF, c == 0 ? u : v, h->nspat, batch, srcs, nullptr, 1, 2, s,
+                                         robert ? nullptr : h->cosphi))
             return rc;
     }
     return SPH_OK;
