@@ -1484,7 +1484,7 @@ static int tcb_launch(const Handle* h, const MixedTables* Tc, bool syn, int lmax
 //   32        split-TF32, P streamed by TMA, B staged by producer warps
 //   8         split-TF32, both operands by TMA (B prepared once per call)
 //   4         split-TF32, P regenerated from recurrence checkpoints
-//   16        the FP64 CUDA-core kernel (legendre.cu)
+//   16        the FP64 tensor-core kernels of the plain form (legendre.cu)
 static bool use_i8(const MixedTables* T, int var) { return T->i8 && !(var & (4 | 8 | 16 | 32)); }
 
 

@@ -9,7 +9,7 @@
 //     m-to-CTA schedule), the split-TF32 kernels with P
 //     loaded by the TMA unit and B staged by producer warps, with both
 //     operands loaded by the TMA unit (B prepared once per call), or with P
-//     regenerated from recurrence checkpoints; and the FP64 CUDA-core kernel
+//     regenerated from recurrence checkpoints; and the FP64 tensor-core kernels
 //     of the plain form (variant 16);
 //   - the fixed-length ring FFTs (automatic grids): 2P rings per CTA with the
 //     default P, twice or half of it (fewer or more CTAs per SM);
@@ -107,7 +107,7 @@ static int autotune(Handle* h, int batch, int families, std::string& json, cudaS
             if (families & SPH_TUNE_TF32)
                 for (int src : {32, 8, 4})
                     for (int c = 1; c <= 3; c++) cand.push_back(src | c);
-            if (families & SPH_TUNE_FP64) cand.push_back(16);  // FP64 CUDA-core kernel
+            if (families & SPH_TUNE_FP64) cand.push_back(16);  // FP64 kernels of the plain form
             if (cand.empty()) continue;
         } else {
             if (!fixed_ring(h->nphi)) continue;

@@ -101,8 +101,9 @@ def test_batched_strides_and_large_batch(gpu, oracle_mod):
 
 @pytest.mark.parametrize("L,nb", [(31, 17), (127, 37), (255, 64)])
 def test_wide_batches_match_oracle(gpu, oracle_mod, L, nb):
-    """Batches above 16 fields take the wide-tile FP64 Legendre kernels (32
-    fields per CTA): ragged and full column tiles, real, complex and vector."""
+    """Batches above 16 fields take several 16-field column blocks of the FP64
+    tensor-core Legendre kernels: ragged and full column blocks, real, complex
+    and vector."""
     from sph_swe_b200.sph import Sph
 
     s, g = Sph(L), oracle_mod.Grid(L)
