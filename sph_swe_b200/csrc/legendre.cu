@@ -368,99 +368,14 @@ __global__ void k_zero_top(double2* spec, long long ld, int lmax, int batch) {
     if (f < batch) spec[(long long)f * ld + pidx(lmax, lmax, lmax)] = make_double2(0, 0);
 }
 
-// The orders m = 0 and 1 alone, FP64 (blockIdx.z = m): a CTA of 8 warps takes
-// 32 consecutive northern latitudes (one per lane: coalesced table reads) of
-// one field, each warp an eighth of the degrees; the partial even / odd sums
-// E = sum over l - m even, O = over l - m odd of P_l^m(mu_j) X_lm meet in shared
-// memory; north E + O, south E - O.  A few microseconds for any batch, where
-// the general kernel given two orders runs a handful of long CTAs.
-__global__ void __launch_bounds__(256) k_legendre_synthesis_m01(const double* __restrict__ plm,
-                                                                const long long* __restrict__ poff, int nh, int nlat,
-                                                                const double2* __restrict__ spec, long long ld_spec,
-                                                                int lmax, double2* __restrict__ F, long long ldF) {
-    __shared__ double2 part[8][2][32];
-    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    const int j = blockIdx.x * 32 + lane;
-    const int f = blockIdx.y, m = blockIdx.z;
-    const double* P = plm + poff[m];                                      // rows l - m
-    const double2* x = spec + (long long)f * ld_spec + pidx(lmax, m, m);  // degrees m..lmax
-    const int nk = lmax - m + 1;
-    const int per = ((nk + 15) / 16) * 2;  // degrees per warp, even
-    const int k0 = wp * per, k1 = min(nk, k0 + per);
-    double2 e = make_double2(0, 0), o = make_double2(0, 0);
-    if (j < nh) {
-#pragma unroll 4
-        for (int k = k0; k < k1; k += 2) {
-            const double p0 = P[(long long)k * nh + j];
-            const double2 x0 = __ldg(&x[k]);
-            e.x = fma(p0, x0.x, e.x);
-            e.y = fma(p0, x0.y, e.y);
-            if (k + 1 < k1) {
-                const double p1 = P[(long long)(k + 1) * nh + j];
-                const double2 x1 = __ldg(&x[k + 1]);
-                o.x = fma(p1, x1.x, o.x);
-                o.y = fma(p1, x1.y, o.y);
-            }
-        }
-    }
-    part[wp][0][lane] = e;
-    part[wp][1][lane] = o;
-    __syncthreads();
-    if (wp == 0 && j < nh) {
-        e = o = make_double2(0, 0);
-#pragma unroll
-        for (int w = 0; w < 8; w++) {
-            e.x += part[w][0][lane].x;
-            e.y += part[w][0][lane].y;
-            o.x += part[w][1][lane].x;
-            o.y += part[w][1][lane].y;
-        }
-        double2* out = F + (long long)f * ldF + (long long)m * nlat;
-        out[j] = make_double2(e.x + o.x, e.y + o.y);
-        out[nlat - 1 - j] = make_double2(e.x - o.x, e.y - o.y);
-    }
-}
-
-// The orders m = 0 and 1 of an analysis alone, FP64: one warp per (degree l,
-// order m, field), lanes over the northern latitudes, a_lm = sum_j w_j
-// P_l^m(mu_j) (F(j) + (-1)^(l-m) F(nlat-1-j)), reduced by shuffles.
-__global__ void __launch_bounds__(128) k_legendre_analysis_m01(const double* __restrict__ plm,
-                                                               const long long* __restrict__ poff, int nh, int nlat,
-                                                               const double* __restrict__ w,
-                                                               const double2* __restrict__ F, long long ldF,
-                                                               double2* __restrict__ spec, long long ld_spec, int lmax,
-                                                               int batch) {
-    const int lane = threadIdx.x & 31;
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int per = 2 * lmax + 1;  // (l, m) pairs: m = 0: l = 0..lmax, m = 1: l = 1..lmax
-    if (warp >= (long long)per * batch) return;
-    const int f = (int)(warp / per), q = (int)(warp % per);
-    const int m = q <= lmax ? 0 : 1, l = m == 0 ? q : q - lmax;
-    const double* P = plm + poff[m] + (long long)(l - m) * nh;
-    const double2* src = F + (long long)f * ldF + (long long)m * nlat;
-    const double sg = ((l - m) & 1) ? -1.0 : 1.0;
-    double2 acc = make_double2(0, 0);
-    for (int j = lane; j < nh; j += 32) {
-        const double pw = P[j] * w[j];
-        const double2 a = src[j], b = src[nlat - 1 - j];
-        acc.x = fma(pw, fma(sg, b.x, a.x), acc.x);
-        acc.y = fma(pw, fma(sg, b.y, a.y), acc.y);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-    }
-    if (lane == 0) spec[(long long)f * ld_spec + pidx(lmax, l, m)] = acc;
-}
-
 // column-block width of the tensor-core kernels for a batch: 4, 8 or 16 fields
 static int mma_rn(int batch) { return batch <= 4 ? 1 : batch <= 8 ? 2 : 4; }
 
+// morders > 0 (real layout): the orders m = 0 .. morders - 1 alone
 static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double2* F, long long ldF, int batch,
-                        cudaStream_t s) {
+                        cudaStream_t s, int morders = 0) {
     if (batch <= 0) return SPH_OK;
-    const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
+    const int nm = morders > 0 ? morders : sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
     const int rn = mma_rn(batch), cn = 8 * rn;
     const int kc = mma_chunk((sm.lmax + 2) / 2, cn, 0);
     // staged spectra, then the odd sums of the 4 warp pairs
@@ -477,10 +392,10 @@ static int launch_synth(const Handle* h, const double2* spec, SpecMap sm, double
 }
 
 static int launch_anal(const Handle* h, const double2* F, long long ldF, double2* spec, SpecMap sm, int batch,
-                       cudaStream_t s, const double* wts = nullptr) {
+                       cudaStream_t s, const double* wts = nullptr, int morders = 0) {
     if (!wts) wts = h->w;
     if (batch <= 0) return SPH_OK;
-    const int nm = sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
+    const int nm = morders > 0 ? morders : sm.cplx ? 2 * h->L + 1 : std::min(sm.lmax, h->L) + 1;
     const int rn = mma_rn(batch), cn = 8 * rn;
     const int cj = mma_chunk(h->nh, cn, RING_A);
     const size_t smem = (size_t)(2 * cn * (cj + 4) + RING_A) * sizeof(double);
@@ -516,8 +431,6 @@ int legendre_kernels_init() {
     SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_mma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
     SPH_CUDA_TRY(cudaFuncSetAttribute(k_legendre_analysis_mma<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, MSMEM));
     SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_zero_top));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_synthesis_m01));
-    SPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_legendre_analysis_m01));
     return SPH_OK;
 }
 
@@ -528,11 +441,8 @@ int legendre_synthesis_real(const Handle* h, const double2* spec, long long ld_s
     if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_SYNTHESIS, batch, 0) & 16)) {
         if (int rc = legendre_synthesis_tc(h, spec, ld_spec, lmax, F, ldF, batch, s, nobuf)) return rc;
         if (!exact_m0) return SPH_OK;
-        if (batch > 65535) { set_error("legendre synthesis: too many fields for one launch"); return SPH_ERR_ARG; }
-        k_legendre_synthesis_m01<<<dim3((h->nh + 31) / 32, batch, 2), 256, 0, s>>>(h->plm, h->poff, h->nh, h->nlat,
-                                                                                   spec, ld_spec, lmax, F, ldF);
-        SPH_CUDA_TRY(cudaGetLastError());
-        return SPH_OK;
+        // the orders m = 0, 1 again, in FP64 (the plain form's kernels), over the mixed result
+        return launch_synth(h, spec, sm, F, ldF, batch, s, 2);
     }
     return launch_synth(h, spec, sm, F, ldF, batch, s);
 }
@@ -542,11 +452,10 @@ int legendre_analysis_real(const Handle* h, const double2* F, long long ldF, dou
     if ((h->flags & SPH_PREC_MIXED) && !(tune_get(h, TUNE_TC_ANALYSIS, batch, 0) & 16)) {
         if (int rc = legendre_analysis_tc(h, F, ldF, spec, ld_spec, lmax, batch, s, wmode)) return rc;
         if (wmode) {
-            // integrands of velocity-derived fields: the orders m = 0, 1 in FP64
-            const long long warps = (long long)(2 * lmax + 1) * batch;
-            k_legendre_analysis_m01<<<(unsigned)((warps + 3) / 4), 128, 0, s>>>(h->plm, h->poff, h->nh, h->nlat, h->wc, F,
-                                                                               ldF, spec, ld_spec, lmax, batch);
-            SPH_CUDA_TRY(cudaGetLastError());
+            // integrands of velocity-derived fields: the orders m = 0, 1 again in
+            // FP64 (the plain form's kernels), over the mixed result
+            SpecMap sm{0, lmax, h->L, ld_spec};
+            if (int rc = launch_anal(h, F, ldF, spec, sm, batch, s, h->wc, 2)) return rc;
         }
         if (lmax > h->L) {
             k_zero_top<<<(batch + 127) / 128, 128, 0, s>>>(spec, ld_spec, lmax, batch);
