@@ -57,10 +57,7 @@ constexpr int MNT = 256;                  // threads (8 warps)
 constexpr int MRING = 3;                  // ring slots of table tiles per warp (steps in flight)
 constexpr int ASA = 20;                   // analysis tile row: 16 latitudes + 4 (two-wavefront fragment loads)
 constexpr int RING_A = 8 * MRING * 16 * ASA;  // doubles of the analysis rings of a CTA
-#ifndef SPH_MSMEM
-#define SPH_MSMEM 115712
-#endif
-constexpr int MSMEM = SPH_MSMEM;          // dynamic shared memory per CTA at most (2 CTAs per SM)
+constexpr int MSMEM = 115712;             // dynamic shared memory per CTA at most (2 CTAs per SM)
 constexpr int MCHUNK = 192;               // most entries staged per column and parity
 // entries staged per column and parity: the whole range where it fits (up to
 // MCHUNK) next to the rings of `ring` doubles, else the largest multiple of 16
@@ -93,11 +90,6 @@ __device__ __forceinline__ void acp_wait() { asm volatile("cp.async.wait_group %
 // leaves less for the staged spectra, which then take more chunks.)
 constexpr int mma_depth_syn(int rn) { return rn == 4 ? 2 : 1; }
 
-#ifdef SPH_MMA_MINB
-#define MMA_LB __launch_bounds__(MNT, SPH_MMA_MINB)
-#else
-#define MMA_LB __launch_bounds__(MNT)
-#endif
 
 __device__ __forceinline__ void dmma8844(double& c0, double& c1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -106,7 +98,7 @@ __device__ __forceinline__ void dmma8844(double& c0, double& c1, double a, doubl
 }
 
 template <int RN>
-__global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
+__global__ void __launch_bounds__(MNT) k_legendre_analysis_mma(const double* __restrict__ plm,
                                                const long long* __restrict__ poff, int nh, int nlat,
                                                const double* __restrict__ w, const double2* __restrict__ F,
                                                long long ldF, double2* __restrict__ spec, SpecMap sm, int batch,
@@ -234,7 +226,7 @@ __global__ void MMA_LB k_legendre_analysis_mma(const double* __restrict__ plm,
 }
 
 template <int RN>
-__global__ void MMA_LB k_legendre_synthesis_mma(const double* __restrict__ plm,
+__global__ void __launch_bounds__(MNT) k_legendre_synthesis_mma(const double* __restrict__ plm,
                                                                 const long long* __restrict__ poff, int nh, int nlat,
                                                                 const double2* __restrict__ spec, SpecMap sm,
                                                                 double2* __restrict__ F, long long ldF, int batch,
