@@ -4,7 +4,8 @@
 
 Headline workload (one "step"), run in the mixed-precision form (Legendre
 stage on tcgen05 kind::i8, integer split with exact int32 sums) with the FP64
-form measured beside it: the
+form (Legendre stage on the FP64 tensor cores, mma.sync m8n8k4 f64) measured
+beside it: the
 transform-throughput configuration,
 T255 on the 384 x 768 Gauss grid, 64 scalar fields plus 32 vorticity/divergence
 pairs, inverse and forward transform of every field.  Metric: SHT GFLOP/s with
@@ -16,8 +17,11 @@ Inputs are synthetic (seeded complex N(0,1) spectra scaled by (l+1)^-1.5,
 Im = 0 at m = 0) and larger than L2 (>= 270 MB per step), so no L2 flush is
 needed between steps.  Also reported (not the headline): the FP64 form of the
 same step, the per-field relative L2 of the mixed form against the FP64 path,
-nonlinear RK4 steps/s at T255 and T63 (plain-method configuration) in both
-forms, and REXI steps/s at T127 (M = 256, 535 poles, FP64 direct solves).
+the Legendre stages alone (64 fields, and 1-8 fields as in the RK4 steps),
+nonlinear RK4 steps/s at T255 (advective and vorticity-divergence forms) and
+T63 (plain-method configuration) in both forms, REXI steps/s at T127 (M =
+256, 535 poles; FP64 with stored factors, and the mixed form), the 256-member
+uneven ensemble and T1023, each with its relative L2 against the FP64 form.
 
 End to end (`e2e`): the same step through the public transform calls with
 the input spectra in pinned host memory and the output spectra copied back to
